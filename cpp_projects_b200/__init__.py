@@ -1,0 +1,18 @@
+"""B200-native FRB / pulsar search core.
+
+Host-side mirror (Python) of the reference's C++ entry points on the search
+hot path, calling hand-written sm_100a CUDA through the C ABI in
+``include/bfs.h``:
+
+* :class:`CFdmtGpu` — FDMT (``CFdmtGpu::process_image``)
+* :mod:`.search` — boxcar detection (``clusterization::gather_candidates_*``),
+  per-row normalisation
+* :mod:`.cluster` — ``clusterization::complete_clusterization`` /
+  ``clusterization_main``, ``select_delegates``
+* :mod:`.preproc` — ``statistical_preprocessing::calc_fdmt_inputs``,
+  ``fdmt_normalization``
+"""
+from ._capi import BfsError, lib  # noqa: F401
+from .fdmt import CFdmtGpu  # noqa: F401
+
+__all__ = ["CFdmtGpu", "BfsError", "lib"]

@@ -1,0 +1,106 @@
+"""ctypes binding of the C ABI declared in include/bfs.h.
+
+The shared library is built in-tree (``python -m cpp_projects_b200.build``)
+and loaded from ``cpp_projects_b200/lib``.  There is no fallback: if the
+library is missing, importing a compute entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libbfs_b200.so"
+
+BFS_OK, BFS_ERR_ARG, BFS_ERR_CUDA, BFS_ERR_OVERFLOW, BFS_ERR_TIMEOUT, BFS_ERR_ALLOC, \
+    BFS_ERR_UNSUPPORTED = range(7)
+STATUS_NAMES = {0: "BFS_OK", 1: "BFS_ERR_ARG", 2: "BFS_ERR_CUDA", 3: "BFS_ERR_OVERFLOW",
+                4: "BFS_ERR_TIMEOUT", 5: "BFS_ERR_ALLOC", 6: "BFS_ERR_UNSUPPORTED"}
+BFS_WIDTHS_POW2, BFS_WIDTHS_ALL = 0, 1
+
+
+class BfsError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class FdmtDesc(ctypes.Structure):
+    _fields_ = [("fmin", ctypes.c_float), ("fmax", ctypes.c_float), ("nchan", ctypes.c_int),
+                ("ncols", ctypes.c_int), ("max_dt", ctypes.c_int), ("plan_kind", ctypes.c_int),
+                ("precision", ctypes.c_int), ("fuse_depth", ctypes.c_int),
+                ("reserved", ctypes.c_int * 8)]
+
+
+class FdmtInfo(ctypes.Structure):
+    _fields_ = [("niter", ctypes.c_int), ("rows_level0", ctypes.c_int),
+                ("fuse_depth", ctypes.c_int), ("rows_total", ctypes.c_int64),
+                ("workspace_bytes", ctypes.c_size_t), ("alg_bytes", ctypes.c_double)]
+
+
+class Cand(ctypes.Structure):
+    _fields_ = [("mt", ctypes.c_int), ("mdt", ctypes.c_int), ("mwidth", ctypes.c_int),
+                ("msnr", ctypes.c_float)]
+
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_U32 = ctypes.c_uint32
+_I64 = ctypes.c_int64
+_F = ctypes.c_float
+
+# name -> (restype, argtypes)
+_SIGNATURES = {
+    "bfs_last_error": (ctypes.c_char_p, []),
+    "bfs_version": (ctypes.c_char_p, []),
+    "bfs_fdmt_plan_create": (_I, [ctypes.POINTER(FdmtDesc), ctypes.POINTER(_P)]),
+    "bfs_fdmt_plan_create_host": (_I, [ctypes.POINTER(FdmtDesc), ctypes.POINTER(_P)]),
+    "bfs_fdmt_plan_destroy": (_I, [_P]),
+    "bfs_fdmt_plan_info": (_I, [_P, ctypes.POINTER(FdmtInfo)]),
+    "bfs_fdmt_plan_rows": (_I, [_P, _P, _I]),
+    "bfs_fdmt_plan_tables": (_I, [_P, _I, _P, _P, _P, _I]),
+    "bfs_fdmt_execute": (_I, [_P, _P, _P, _I, _P]),
+    "bfs_preproc_calc_fdmt_inputs": (_I, [_P, _I, _I, _P, _P, _P]),
+    "bfs_fdmt_normalize": (_I, [_P, _P, _I64, _P, _P]),
+    "bfs_norm_rows": (_I, [_P, _P, _I, _I, _P, _P]),
+    "bfs_row_stats": (_I, [_P, _I, _I, _P, _P]),
+    "bfs_boxcar_gather": (_I, [_P, _I, _I, _P, _F, _P, _I, _I, _I, _P, _U32,
+                               ctypes.POINTER(_U32), _P]),
+    "bfs_cluster": (_I, [_P, _U32, _P, _P, _P, _P, ctypes.POINTER(_U32), _P]),
+    "bfs_select_delegates": (_I, [_P, _P, _U32, _P, _U32, _P, _P]),
+}
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load (once) and return the native library; raise if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"native library {LIB_PATH} is missing: run "
+                          "`python -m cpp_projects_b200.build` (there is no CPU fallback)")
+    l = ctypes.CDLL(str(LIB_PATH), mode=os.RTLD_NOW | os.RTLD_LOCAL)
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(l, name, None)
+        if fn is None:
+            continue
+        fn.restype = res
+        fn.argtypes = args
+    _lib = l
+    return l
+
+
+def declared_symbols() -> list[str]:
+    return [n for n in _SIGNATURES]
+
+
+def check(status: int) -> None:
+    if status != BFS_OK:
+        msg = lib().bfs_last_error()
+        raise BfsError(status, msg.decode() if msg else "")
+
+
+def call(name: str, *args) -> None:
+    check(getattr(lib(), name)(*args))

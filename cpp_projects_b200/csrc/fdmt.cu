@@ -1,0 +1,241 @@
+// FDMT on sm_100a.
+//
+// Reference semantics (L/FDMT/FdmtCpu.cpp:197-367, L/FDMT/FdmtGpu.cu:273-448):
+//   level 0  row r of channel c at sample t is the running mean
+//            v_r = (v_{r-1} * r + x[c][t-r]) / (r+1), v_0 = x[c][t], and 0 for t < r;
+//   level l  out[g][t] = in[a_g][t] + (t >= s_g ? in[b_g][t - s_g] : 0), or a
+//            copy of in[a_g] for the carried-over sub-band of an odd count.
+// The products, sums and quotients use explicitly round-to-nearest intrinsics
+// (no FMA contraction), so the result is bit-identical to the reference's CPU
+// class run on one thread.
+//
+// Layout in HBM: every plane is row-major [row][ncols] float32, rows of a
+// level concatenated sub-band by sub-band in frequency order (the reference's
+// layout).  The plan owns two ping-pong planes sized for the largest even and
+// odd level; the last level is written straight into the caller's output.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+
+#include "internal.h"
+
+struct bfs_fdmt_plan {
+    bfs::FdmtPlanHost host;
+    int device = -1;
+    bool host_only = false;
+    int fuse_depth = 0;
+    int4* d_tab = nullptr;             // per level, per output row: {a, b, shift, 0}
+    std::vector<size_t> tab_off;       // offset of each level's table in d_tab
+    float* d_buf[2] = {nullptr, nullptr};
+    size_t buf_rows[2] = {0, 0};
+    size_t ws_bytes = 0;
+};
+
+namespace bfs {
+namespace {
+
+constexpr int kInitThreads = 256;
+constexpr int kInitCols = 4;        // columns per thread (strided by the block)
+constexpr int kLevelThreads = 256;
+constexpr int kLevelCols = 8;       // columns per thread (strided by the block)
+
+// Level 0.  grid: (ceil(ncols / (256*4)), nchan).
+__global__ void __launch_bounds__(kInitThreads)
+k_fdmt_init(const float* __restrict__ x, float* __restrict__ out, int ncols, int rows_per_chan,
+            int ones) {
+    const int c = blockIdx.y;
+    const float* xr = x + static_cast<size_t>(c) * ncols;
+    float* o = out + static_cast<size_t>(c) * rows_per_chan * ncols;
+    const int base = blockIdx.x * (kInitThreads * kInitCols) + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < kInitCols; ++k) {
+        const int t = base + k * kInitThreads;
+        if (t >= ncols) break;
+        float v = ones ? 1.0f : __ldg(xr + t);
+        o[t] = v;
+        for (int r = 1; r < rows_per_chan; ++r) {
+            float w = 0.0f;
+            if (t >= r) {
+                const float xv = ones ? 1.0f : __ldg(xr + t - r);
+                v = __fdiv_rn(__fadd_rn(__fmul_rn(v, static_cast<float>(r)), xv),
+                              static_cast<float>(r + 1));
+                w = v;
+            }
+            o[static_cast<size_t>(r) * ncols + t] = w;
+        }
+    }
+}
+
+// One merge level.  grid: (rows, ceil(ncols / (256*8))).
+__global__ void __launch_bounds__(kLevelThreads)
+k_fdmt_level(const float* __restrict__ in, float* __restrict__ out, const int4* __restrict__ tab,
+             int ncols) {
+    const int g = blockIdx.x;
+    const int4 e = __ldg(tab + g);
+    const float* ra = in + static_cast<size_t>(e.x) * ncols;
+    const float* rb = in + static_cast<size_t>(e.y < 0 ? e.x : e.y) * ncols;
+    float* ro = out + static_cast<size_t>(g) * ncols;
+    const int s = e.z;
+    const bool has_b = e.y >= 0;
+    const int base = blockIdx.y * (kLevelThreads * kLevelCols) + threadIdx.x;
+    float va[kLevelCols], vb[kLevelCols];
+#pragma unroll
+    for (int k = 0; k < kLevelCols; ++k) {
+        const int t = base + k * kLevelThreads;
+        va[k] = (t < ncols) ? __ldg(ra + t) : 0.0f;
+        vb[k] = (has_b && t < ncols && t >= s) ? __ldg(rb + t - s) : 0.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < kLevelCols; ++k) {
+        const int t = base + k * kLevelThreads;
+        if (t < ncols) ro[t] = (has_b && t >= s) ? __fadd_rn(va[k], vb[k]) : va[k];
+    }
+}
+
+}  // namespace
+}  // namespace bfs
+
+using namespace bfs;
+
+static bfs_status plan_host_part(const bfs_fdmt_desc* desc, std::unique_ptr<bfs_fdmt_plan>& p) {
+    BFS_ARG(desc != nullptr, "null argument");
+    BFS_ARG(desc->plan_kind == BFS_PLAN_KEITH, "unsupported plan_kind %d", desc->plan_kind);
+    BFS_ARG(desc->precision == BFS_PREC_F32, "unsupported precision %d", desc->precision);
+    p.reset(new bfs_fdmt_plan);
+    p->host_only = true;
+    return build_fdmt_plan(desc->fmin, desc->fmax, desc->nchan, desc->ncols, desc->max_dt,
+                           &p->host);
+}
+
+extern "C" bfs_status bfs_fdmt_plan_create_host(const bfs_fdmt_desc* desc, bfs_fdmt_plan** plan) {
+    BFS_ARG(plan != nullptr, "null argument");
+    *plan = nullptr;
+    std::unique_ptr<bfs_fdmt_plan> p;
+    bfs_status st = plan_host_part(desc, p);
+    if (st != BFS_OK) return st;
+    *plan = p.release();
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc, bfs_fdmt_plan** plan) {
+    BFS_ARG(plan != nullptr, "null argument");
+    *plan = nullptr;
+    std::unique_ptr<bfs_fdmt_plan> p;
+    bfs_status st = plan_host_part(desc, p);
+    if (st != BFS_OK) return st;
+    p->host_only = false;
+    BFS_CUDA(cudaGetDevice(&p->device));
+    const FdmtPlanHost& h = p->host;
+    p->fuse_depth = 0;
+
+    // device row tables
+    std::vector<int4> tab;
+    p->tab_off.assign(h.niter + 1, 0);
+    for (int l = 1; l <= h.niter; ++l) {
+        p->tab_off[l] = tab.size();
+        const FdmtLevel& L = h.lv[l];
+        for (int g = 0; g < L.total_rows(); ++g)
+            tab.push_back(make_int4(L.a_row[g], L.b_row[g], L.shift[g], 0));
+    }
+    if (!tab.empty()) {
+        BFS_CUDA(cudaMalloc(&p->d_tab, tab.size() * sizeof(int4)));
+        BFS_CUDA(cudaMemcpy(p->d_tab, tab.data(), tab.size() * sizeof(int4),
+                            cudaMemcpyHostToDevice));
+    }
+    // ping-pong planes: level l lives in buffer l & 1; the last level goes to the output
+    for (int l = 0; l < h.niter; ++l)
+        p->buf_rows[l & 1] = std::max(p->buf_rows[l & 1], static_cast<size_t>(h.lv[l].total_rows()));
+    for (int b = 0; b < 2; ++b) {
+        if (p->buf_rows[b] == 0) continue;
+        const size_t bytes = p->buf_rows[b] * static_cast<size_t>(h.ncols) * sizeof(float);
+        cudaError_t e = cudaMalloc(&p->d_buf[b], bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            if (p->d_buf[0]) cudaFree(p->d_buf[0]);
+            if (p->d_tab) cudaFree(p->d_tab);
+            return fail(BFS_ERR_ALLOC, "cudaMalloc(%zu) for an FDMT plane failed: %s", bytes,
+                        cudaGetErrorString(e));
+        }
+        p->ws_bytes += bytes;
+    }
+    *plan = p.release();
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_fdmt_plan_destroy(bfs_fdmt_plan* plan) {
+    if (!plan) return BFS_OK;
+    if (plan->d_tab) cudaFree(plan->d_tab);
+    for (float* b : plan->d_buf)
+        if (b) cudaFree(b);
+    delete plan;
+    return BFS_OK;
+}
+
+static double fdmt_alg_bytes(const FdmtPlanHost& h) {
+    double rows = h.nchan + h.lv[0].total_rows();
+    for (int l = 1; l <= h.niter; ++l) rows += 3.0 * h.lv[l].total_rows();
+    return 4.0 * rows * h.ncols;
+}
+
+extern "C" bfs_status bfs_fdmt_plan_info(const bfs_fdmt_plan* plan, bfs_fdmt_info* info) {
+    BFS_ARG(plan != nullptr && info != nullptr, "null argument");
+    const FdmtPlanHost& h = plan->host;
+    info->niter = h.niter;
+    info->rows_level0 = h.lv[0].total_rows();
+    info->fuse_depth = plan->fuse_depth;
+    int64_t tot = 0;
+    for (const auto& L : h.lv) tot += L.total_rows();
+    info->rows_total = tot;
+    info->workspace_bytes = plan->ws_bytes;
+    info->alg_bytes = fdmt_alg_bytes(h);
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_fdmt_plan_rows(const bfs_fdmt_plan* plan, int* rows, int cap) {
+    BFS_ARG(plan != nullptr && rows != nullptr, "null argument");
+    BFS_ARG(cap >= plan->host.niter + 1, "need %d entries", plan->host.niter + 1);
+    for (int l = 0; l <= plan->host.niter; ++l) rows[l] = plan->host.lv[l].total_rows();
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_fdmt_plan_tables(const bfs_fdmt_plan* plan, int level, int* a_row,
+                                           int* b_row, int* shift, int cap) {
+    BFS_ARG(plan != nullptr && a_row && b_row && shift, "null argument");
+    BFS_ARG(level >= 1 && level <= plan->host.niter, "level %d out of range", level);
+    const FdmtLevel& L = plan->host.lv[level];
+    BFS_ARG(cap >= L.total_rows(), "need %d entries", L.total_rows());
+    std::memcpy(a_row, L.a_row.data(), sizeof(int) * L.total_rows());
+    std::memcpy(b_row, L.b_row.data(), sizeof(int) * L.total_rows());
+    std::memcpy(shift, L.shift.data(), sizeof(int) * L.total_rows());
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_fdmt_execute(bfs_fdmt_plan* plan, const float* d_in, float* d_out,
+                                       int b_ones, void* stream) {
+    BFS_ARG(plan != nullptr && d_out != nullptr, "null argument");
+    BFS_ARG(!plan->host_only, "plan was created with bfs_fdmt_plan_create_host");
+    BFS_ARG(b_ones || d_in != nullptr, "d_in is null");
+    const FdmtPlanHost& h = plan->host;
+    cudaStream_t s = as_stream(stream);
+    const int T = h.ncols;
+    {
+        dim3 grid((T + kInitThreads * kInitCols - 1) / (kInitThreads * kInitCols), h.nchan);
+        BFS_ARG(grid.y <= 65535, "nchan too large for this build");
+        k_fdmt_init<<<grid, kInitThreads, 0, s>>>(d_in, plan->d_buf[0], T, h.rows_per_chan0,
+                                                  b_ones ? 1 : 0);
+        BFS_LAUNCH_CHECK("k_fdmt_init");
+    }
+    const int chunk = kLevelThreads * kLevelCols;
+    for (int l = 1; l <= h.niter; ++l) {
+        const float* src = plan->d_buf[(l - 1) & 1];
+        float* dst = (l == h.niter) ? d_out : plan->d_buf[l & 1];
+        dim3 grid(h.lv[l].total_rows(), (T + chunk - 1) / chunk);
+        BFS_ARG(grid.y <= 65535, "ncols too large for this build");
+        k_fdmt_level<<<grid, kLevelThreads, 0, s>>>(src, dst, plan->d_tab + plan->tab_off[l], T);
+        BFS_LAUNCH_CHECK("k_fdmt_level");
+    }
+    return BFS_OK;
+}

@@ -1,0 +1,70 @@
+// Internal helpers shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "bfs.h"
+
+namespace bfs {
+
+// Thread-local last-error message (bfs_last_error()).
+void set_error(const char* fmt, ...);
+bfs_status fail(bfs_status st, const char* fmt, ...);
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+#define BFS_CUDA(call)                                                                     \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return ::bfs::fail(BFS_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call,     \
+                               cudaGetErrorString(e_));                                    \
+    } while (0)
+
+#define BFS_LAUNCH_CHECK(what)                                                             \
+    do {                                                                                   \
+        cudaError_t e_ = cudaGetLastError();                                               \
+        if (e_ != cudaSuccess)                                                             \
+            return ::bfs::fail(BFS_ERR_CUDA, "launch of %s failed: %s", what,              \
+                               cudaGetErrorString(e_));                                    \
+    } while (0)
+
+#define BFS_ARG(cond, ...)                                                                 \
+    do {                                                                                   \
+        if (!(cond)) return ::bfs::fail(BFS_ERR_ARG, __VA_ARGS__);                         \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// FDMT plan (host side).  Built once per (fmin, fmax, nchan, ncols, max_dt).
+// ---------------------------------------------------------------------------
+struct FdmtLevel {
+    int nsub = 0;                 // sub-bands at this level
+    std::vector<int> rows;        // rows per sub-band
+    std::vector<int> cum;         // nsub + 1 cumulative rows
+    std::vector<float> freq;      // nsub + 1 sub-band edges (MHz)
+    // level >= 1: one entry per output row (global indices in the previous plane)
+    std::vector<int> a_row, b_row, shift;
+    // maximum look-back (samples) of any row of this level, counting level 0
+    std::vector<int> lookback;    // per row
+    int total_rows() const { return cum.empty() ? 0 : cum[nsub]; }
+};
+
+struct FdmtPlanHost {
+    float fmin = 0, fmax = 0;
+    int nchan = 0, ncols = 0, max_dt = 0;
+    int niter = 0;
+    int rows_per_chan0 = 0;  // level-0 rows of every channel (d0 + 1)
+    std::vector<FdmtLevel> lv;  // niter + 1 levels
+};
+
+// Builds the plan exactly as the reference's CFdmtB/CFdmtCpu do.  Returns
+// BFS_OK or BFS_ERR_ARG (with the message set).
+bfs_status build_fdmt_plan(float fmin, float fmax, int nchan, int ncols, int max_dt,
+                           FdmtPlanHost* out);
+
+}  // namespace bfs

@@ -1,0 +1,159 @@
+// FDMT plan builder (host).
+//
+// Restates the reference's plan so the device tables index exactly the rows
+// the reference reads:
+//   sub-band delay rows   CFdmtB::calc_deltaT            L/FDMT/FdmtB.cpp:201-204
+//   level-to-level state  CFdmtB::calcNextStateConfig    L/FDMT/FdmtB.cpp:206-227
+//   row cumsums           CFdmtB::calcCumSum_            L/FDMT/FdmtB.cpp:238-245
+//   level-0 set-up        CFdmtCpu::create_config        L/FDMT/FdmtCpu.cpp:143-194
+//   merge coefficients    CFdmtCpu::fncFdmtIterationC    L/FDMT/FdmtCpu.cpp:286-296
+//                         and fnc_delay_h                L/FDMT/FdmtCpu.cpp:369-372
+// The arithmetic keeps the reference's types: band edges are float, squared in
+// float, reciprocals and differences in double, the merge coefficients are
+// float quotients of float delays and the row offsets are float products
+// truncated to int.  This file must be compiled with -ffp-contract=off so no
+// multiply-add is fused.  The reference GPU class computes the same offsets on
+// the device with the approximate __fdividef (L/FDMT/FdmtGpu.cu:372-373); the
+// CPU class (the parity oracle) uses exact division, which is what is
+// reproduced here, once, on the host.
+#include <cmath>
+#include <cstring>
+
+#include "internal.h"
+
+namespace bfs {
+namespace {
+
+struct DeltaT {
+    float fmin, fmax;
+    int max_dt;
+    int operator()(float f0, float f1) const {
+        const float f0sq = f0 * f0, f1sq = f1 * f1;
+        const float lo = fmin * fmin, hi = fmax * fmax;
+        const double span = 1.0 / static_cast<double>(f0sq) - 1.0 / static_cast<double>(f1sq);
+        const double full = 1.0 / static_cast<double>(lo) - 1.0 / static_cast<double>(hi);
+        return static_cast<int>(std::ceil(span / full * (static_cast<double>(max_dt) - 1.0)));
+    }
+};
+
+// Dispersion delay factor between two band edges, rounded to float.
+float edge_delay(float flo, float fhi) {
+    const float a = flo * flo, b = fhi * fhi;
+    return static_cast<float>(1.0 / static_cast<double>(a) - 1.0 / static_cast<double>(b));
+}
+
+}  // namespace
+
+bfs_status build_fdmt_plan(float fmin, float fmax, int nchan, int ncols, int max_dt,
+                           FdmtPlanHost* out) {
+    BFS_ARG(out != nullptr, "plan output is null");
+    BFS_ARG(nchan >= 2, "nchan must be >= 2 (got %d)", nchan);
+    BFS_ARG(ncols >= 1, "ncols must be >= 1 (got %d)", ncols);
+    BFS_ARG(max_dt >= 1, "max_dt must be >= 1 (got %d)", max_dt);
+    BFS_ARG(std::isfinite(fmin) && std::isfinite(fmax) && fmin > 0.0f && fmax > fmin,
+            "need 0 < fmin < fmax (got %g, %g)", fmin, fmax);
+
+    FdmtPlanHost& p = *out;
+    p = FdmtPlanHost{};
+    p.fmin = fmin; p.fmax = fmax; p.nchan = nchan; p.ncols = ncols; p.max_dt = max_dt;
+    const DeltaT delta{fmin, fmax, max_dt};
+
+    int q = nchan, n = 0;
+    while (q > 1) { q = (q & 1) ? q / 2 + 1 : q / 2; ++n; }
+    p.niter = n;
+    p.lv.resize(n + 1);
+
+    // level 0
+    {
+        FdmtLevel& L = p.lv[0];
+        const float bw = fmax - fmin;
+        const int d0 = delta(fmin, fmin + bw / static_cast<float>(nchan));
+        BFS_ARG(d0 >= 0, "negative level-0 delay span");
+        p.rows_per_chan0 = d0 + 1;
+        L.nsub = nchan;
+        L.rows.assign(nchan, d0 + 1);
+        L.freq.resize(nchan + 1);
+        for (int i = 0; i < nchan; ++i) {
+            const float v = static_cast<float>(i) * bw;
+            L.freq[i] = fmin + v / static_cast<float>(nchan);
+        }
+        L.freq[nchan] = fmax;
+    }
+    // levels 1..n: sub-band bookkeeping
+    for (int l = 1; l <= n; ++l) {
+        const FdmtLevel& P = p.lv[l - 1];
+        FdmtLevel& L = p.lv[l];
+        const int qin = P.nsub, half = qin / 2;
+        const int qout = (qin & 1) ? half + 1 : half;
+        L.nsub = qout;
+        L.rows.resize(qout);
+        L.freq.resize(qout + 1);
+        for (int i = 0; i < half; ++i) {
+            L.rows[i] = delta(P.freq[2 * i], P.freq[2 * i + 2]) + 1;
+            L.freq[i] = P.freq[2 * i];
+        }
+        if (qin & 1) {
+            L.freq[qout - 1] = P.freq[qin - 1];
+            L.rows[qout - 1] = P.rows[qin - 1];
+        }
+        L.freq[qout] = fmax;
+    }
+    for (auto& L : p.lv) {
+        L.cum.assign(L.nsub + 1, 0);
+        for (int i = 0; i < L.nsub; ++i) L.cum[i + 1] = L.cum[i] + L.rows[i];
+    }
+    BFS_ARG(p.lv[n].total_rows() == max_dt,
+            "plan's last level has %d rows, expected max_dt=%d", p.lv[n].total_rows(), max_dt);
+
+    // level 0 look-back: row r of a channel averages x[t-r..t]
+    {
+        FdmtLevel& L = p.lv[0];
+        L.lookback.resize(L.total_rows());
+        for (int c = 0; c < nchan; ++c)
+            for (int r = 0; r < p.rows_per_chan0; ++r) L.lookback[c * p.rows_per_chan0 + r] = r;
+    }
+    // merge tables
+    for (int l = 1; l <= n; ++l) {
+        const FdmtLevel& P = p.lv[l - 1];
+        FdmtLevel& L = p.lv[l];
+        const int R = L.total_rows(), Rin = P.total_rows();
+        L.a_row.resize(R); L.b_row.resize(R); L.shift.resize(R); L.lookback.resize(R);
+        for (int i = 0; i < L.nsub; ++i) {
+            const int r0 = L.cum[i], nr = L.rows[i];
+            if (2 * i + 1 >= P.nsub) {  // odd sub-band count: last one carried over
+                for (int j = 0; j < nr; ++j) {
+                    L.a_row[r0 + j] = P.cum[2 * i] + j;
+                    L.b_row[r0 + j] = -1;
+                    L.shift[r0 + j] = 0;
+                }
+                continue;
+            }
+            const float all = edge_delay(P.freq[2 * i], P.freq[2 * i + 2]);
+            const float c0 = edge_delay(P.freq[2 * i], P.freq[2 * i + 1]) / all;
+            const float c1 = edge_delay(P.freq[2 * i + 1], P.freq[2 * i + 2]) / all;
+            for (int j = 0; j < nr; ++j) {
+                const float fj = static_cast<float>(j);
+                const int j0 = static_cast<int>(c0 * fj);
+                const int j1 = static_cast<int>(c1 * fj);
+                L.a_row[r0 + j] = P.cum[2 * i] + j0;
+                L.b_row[r0 + j] = P.cum[2 * i + 1] + j1;
+                L.shift[r0 + j] = j0;
+            }
+        }
+        for (int g = 0; g < R; ++g) {
+            // The reference indexes the previous plane without bounds checks; a
+            // row outside it would be undefined behaviour there, so reject it.
+            BFS_ARG(L.a_row[g] >= 0 && L.a_row[g] < Rin && L.b_row[g] < Rin && L.shift[g] >= 0,
+                    "level %d row %d references a row outside the previous plane", l, g);
+            int lb = P.lookback[L.a_row[g]];
+            if (L.b_row[g] >= 0) {
+                const int hb = L.shift[g] + P.lookback[L.b_row[g]];
+                if (hb > lb) lb = hb;
+            }
+            L.lookback[g] = lb;
+        }
+    }
+    return BFS_OK;
+}
+
+}  // namespace bfs

@@ -1,0 +1,86 @@
+"""FDMT host interface mirroring the reference's ``CFdmtGpu`` class.
+
+Reference: ``CFdmtGpu(Fmin, Fmax, nchan, cols, imaxDt)`` and
+``process_image(d_in, d_out, b_ones)`` (MyVSLib_C++/FDMT/FdmtGpu.cuh:12-53).
+Inputs and outputs are caller-owned device buffers (here: CUDA torch tensors,
+float32, contiguous): ``d_in`` is ``nchan x cols`` with row 0 the lowest
+frequency channel, ``d_out`` is ``imaxDt x cols``.  The work is enqueued on
+the current torch stream.  Unlike the reference (which prints to stderr and
+returns), errors raise :class:`BfsError`.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _capi
+from ._tensors import dev_ptr, stream_handle
+
+
+class CFdmtGpu:
+    def __init__(self, Fmin: float, Fmax: float, nchan: int, cols: int, imaxDt: int,
+                 fuse_depth: int = -1):
+        self.m_Fmin = float(Fmin)
+        self.m_Fmax = float(Fmax)
+        self.m_nchan = int(nchan)
+        self.m_cols = int(cols)
+        self.m_imaxDt = int(imaxDt)
+        desc = _capi.FdmtDesc(fmin=self.m_Fmin, fmax=self.m_Fmax, nchan=self.m_nchan,
+                              ncols=self.m_cols, max_dt=self.m_imaxDt, plan_kind=0,
+                              precision=0, fuse_depth=int(fuse_depth))
+        self._plan = ctypes.c_void_p()
+        _capi.call("bfs_fdmt_plan_create", ctypes.byref(desc), ctypes.byref(self._plan))
+        info = _capi.FdmtInfo()
+        _capi.call("bfs_fdmt_plan_info", self._plan, ctypes.byref(info))
+        self.info = info
+        self.m_iNumIter = info.niter
+
+    def __del__(self):
+        p = getattr(self, "_plan", None)
+        if p is not None and p.value:
+            try:
+                _capi.lib().bfs_fdmt_plan_destroy(p)
+            except Exception:
+                pass
+            self._plan = None
+
+    # --- reference API ---------------------------------------------------
+    def process_image(self, d_in: torch.Tensor | None, d_out: torch.Tensor, b_ones: bool = False,
+                      stream: torch.cuda.Stream | None = None) -> None:
+        if d_out.numel() != self.m_imaxDt * self.m_cols:
+            raise ValueError(f"d_out must hold {self.m_imaxDt}x{self.m_cols} floats")
+        pin = None
+        if not b_ones:
+            if d_in is None or d_in.numel() != self.m_nchan * self.m_cols:
+                raise ValueError(f"d_in must hold {self.m_nchan}x{self.m_cols} floats")
+            pin = dev_ptr(d_in, torch.float32, "d_in")
+        _capi.call("bfs_fdmt_execute", self._plan, pin, dev_ptr(d_out, torch.float32, "d_out"),
+                   1 if b_ones else 0, stream_handle(stream))
+
+    # --- plan introspection ------------------------------------------------
+    def rows_per_level(self) -> np.ndarray:
+        rows = np.zeros(self.m_iNumIter + 1, np.int32)
+        _capi.call("bfs_fdmt_plan_rows", self._plan, rows.ctypes.data_as(ctypes.c_void_p),
+                   rows.size)
+        return rows
+
+    def tables(self, level: int):
+        n = int(self.rows_per_level()[level])
+        a = np.zeros(n, np.int32); b = np.zeros(n, np.int32); s = np.zeros(n, np.int32)
+        P = ctypes.c_void_p
+        _capi.call("bfs_fdmt_plan_tables", self._plan, level, a.ctypes.data_as(P),
+                   b.ctypes.data_as(P), s.ctypes.data_as(P), n)
+        return a, b, s
+
+    @property
+    def alg_bytes(self) -> float:
+        """Level-by-level algorithmic bytes of one call (input read, level-0
+        plane write, each level's tail + head read and output write)."""
+        return float(self.info.alg_bytes)
+
+    def __call__(self, d_in: torch.Tensor, b_ones: bool = False) -> torch.Tensor:
+        out = torch.empty((self.m_imaxDt, self.m_cols), dtype=torch.float32, device=d_in.device)
+        self.process_image(d_in, out, b_ones)
+        return out

@@ -1,0 +1,98 @@
+"""Seeded synthetic filterbanks for the search path's test and bench shapes.
+
+No observational data ships with the repository, so every workload is
+generated: i.i.d. N(0,1) float32 noise from ``numpy.random.default_rng(seed)``
+plus pulses injected along the cold-plasma dispersion track
+``t(f) = t0 + span * (f^-2 - fmax^-2) / (fmin^-2 - fmax^-2)``: a pulse starts
+at sample ``t0`` in the highest channel and arrives ``span`` samples later in
+the lowest one (the FDMT's delay convention: output row ``d`` sums channel
+``c`` at sample ``t - delay_c(d)`` with delay 0 at ``fmin``).  Channel centres
+are uniform: ``fmin + (c + 0.5) * (fmax - fmin) / nchan``.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Pulse:
+    t0: int            # arrival sample in the highest-frequency channel
+    span: float        # delay (samples) between the highest and lowest channel
+    width: int         # samples
+    amp: float         # added to every channel over the width
+
+
+@dataclass
+class Beam:
+    nchan: int
+    nsamp: int
+    fmin: float
+    fmax: float
+    max_dt: int
+    seed: int
+    pulses: list = field(default_factory=list)
+    gain: np.ndarray | None = None   # optional per-channel bandpass gain
+
+
+def channel_centres(nchan: int, fmin: float, fmax: float) -> np.ndarray:
+    return fmin + (np.arange(nchan) + 0.5) * (fmax - fmin) / nchan
+
+
+def track(nchan, fmin, fmax, t0, span) -> np.ndarray:
+    f = channel_centres(nchan, fmin, fmax)
+    frac = (f ** -2 - fmax ** -2) / (fmin ** -2 - fmax ** -2)
+    return t0 + np.rint(span * frac).astype(np.int64)
+
+
+def filterbank(beam: Beam) -> np.ndarray:
+    rng = np.random.default_rng(beam.seed)
+    x = rng.standard_normal((beam.nchan, beam.nsamp), dtype=np.float32)
+    if beam.gain is not None:
+        x *= beam.gain[:, None].astype(np.float32)
+    for p in beam.pulses:
+        tt = track(beam.nchan, beam.fmin, beam.fmax, p.t0, p.span)
+        for c in range(beam.nchan):
+            a, b = int(tt[c]), int(tt[c]) + int(p.width)
+            a, b = max(a, 0), min(b, beam.nsamp)
+            if a < b:
+                x[c, a:b] += np.float32(p.amp)
+    return x
+
+
+# ---- named workloads ---------------------------------------------------------
+def config0(seed: int = 1) -> Beam:
+    """512 ch x 32768 samples, 1200-1600 MHz, max delay 512, one pulse of width
+    4 and amplitude 2.0 starting at sample 10000, track spanning 256 samples."""
+    return Beam(512, 32768, 1200.0, 1600.0, 512, seed, [Pulse(10000, 256.0, 4, 2.0)])
+
+
+CONFIG0_SEARCH = dict(widths_mode=0, param=5, thr=7.0, metrics=(16, 8, 1 << 30))
+
+
+def config2(seed: int = 2, nbeams: int = 48, max_nchan: int = 4096) -> list[Beam]:
+    """48 beams of uneven shapes: nchan from {256, 512, 1024, 4096}, lengths
+    uniform in 2^14..2^17, max delay = nchan, band 1200-1600 MHz, 0-3 pulses
+    of width 1-32, amplitude 1.5-4, delay span 10-90 % of the max delay."""
+    rng = np.random.default_rng(seed)
+    choices = [c for c in (256, 512, 1024, 4096) if c <= max_nchan]
+    beams = []
+    for b in range(nbeams):
+        nchan = int(rng.choice(choices))
+        nsamp = int(rng.integers(1 << 14, (1 << 17) + 1))
+        npulse = int(rng.integers(0, 4))
+        pulses = []
+        for _ in range(npulse):
+            span = float(rng.uniform(0.1, 0.9) * (nchan - 1))
+            width = int(rng.integers(1, 33))
+            amp = float(rng.uniform(1.5, 4.0))
+            t0 = int(rng.integers(0, max(1, nsamp - int(span) - width)))
+            pulses.append(Pulse(t0, span, width, amp))
+        beams.append(Beam(nchan, nsamp, 1200.0, 1600.0, nchan, int(seed * 1000 + b), pulses))
+    return beams
+
+
+def manifest(beams: list[Beam]) -> list[dict]:
+    return [dict(nchan=b.nchan, nsamp=b.nsamp, max_dt=b.max_dt, seed=b.seed,
+                 pulses=[p.__dict__ for p in b.pulses]) for b in beams]

@@ -1,0 +1,173 @@
+/* bfs.h — C ABI of the B200-native FRB / pulsar search core.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, returns a
+ * bfs_status and never throws.  Unless stated otherwise, pointers named d_*
+ * are DEVICE pointers owned by the caller, `stream` is a cudaStream_t passed
+ * as void* (NULL = legacy default stream), and work is enqueued
+ * asynchronously on that stream.  A plan object is not thread-safe: use one
+ * plan per host thread / stream.  bfs_last_error() returns a message for the
+ * last failing call on the calling thread.
+ *
+ * Each declaration names the reference interface it replaces
+ * (Iourick/cpp_projects, paths relative to its root, MyVSLib_C++ = "L/").
+ */
+#ifndef BFS_H
+#define BFS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum bfs_status {
+    BFS_OK = 0,
+    BFS_ERR_ARG = 1,         /* invalid argument / size mismatch                */
+    BFS_ERR_CUDA = 2,        /* a CUDA runtime or library call failed           */
+    BFS_ERR_OVERFLOW = 3,    /* output capacity exceeded (count still reported) */
+    BFS_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up              */
+    BFS_ERR_ALLOC = 5,       /* device or host allocation failed                */
+    BFS_ERR_UNSUPPORTED = 6  /* valid request this build does not implement     */
+} bfs_status;
+
+/* Candidate record, byte-compatible with the reference's Cand / SCand
+ * (L/Clusterization/Candidate.cuh:4-10): 16 bytes. */
+typedef struct bfs_cand {
+    int mt;      /* start sample of the window          */
+    int mdt;     /* row of the DM-time plane (delay)     */
+    int mwidth;  /* width code (log2 w or w, see below)  */
+    float msnr;  /* window sum / sqrt(w)                 */
+} bfs_cand;
+
+const char* bfs_last_error(void);
+const char* bfs_version(void);
+
+/* ------------------------------------------------------------------------
+ * FDMT
+ * Replaces CFdmtGpu(Fmin, Fmax, nchan, cols, imaxDt) + process_image
+ * (L/FDMT/FdmtGpu.cuh:12-53, L/FDMT/FdmtGpu.cu:230-348) whose plan is
+ * CFdmtB/CFdmtCpu::create_config (L/FDMT/FdmtB.cpp:141-245,
+ * L/FDMT/FdmtCpu.cpp:143-194).
+ * Input: nchan x ncols float32, row 0 = fmin channel.  Output: max_dt x ncols,
+ * row d = delay d samples across the band.
+ * ---------------------------------------------------------------------- */
+enum { BFS_PLAN_KEITH = 0 };
+enum { BFS_PREC_F32 = 0 };
+
+typedef struct bfs_fdmt_desc {
+    float fmin;        /* MHz, lower band edge                          */
+    float fmax;        /* MHz, upper band edge                          */
+    int nchan;         /* input rows (>= 2)                             */
+    int ncols;         /* time samples per row (>= 1)                   */
+    int max_dt;        /* output rows (>= 1)                            */
+    int plan_kind;     /* BFS_PLAN_KEITH                                */
+    int precision;     /* BFS_PREC_F32                                  */
+    int fuse_depth;    /* -1 = autotuned; 0 = level-by-level; k = fuse levels 0..k in one kernel */
+    int reserved[8];
+} bfs_fdmt_desc;
+
+typedef struct bfs_fdmt_plan bfs_fdmt_plan;
+
+typedef struct bfs_fdmt_info {
+    int niter;              /* number of merge levels (ceil(log2 nchan))      */
+    int rows_level0;        /* rows of the level-0 plane                      */
+    int fuse_depth;         /* fused levels actually used                     */
+    int64_t rows_total;     /* sum of rows over levels 0..niter               */
+    size_t workspace_bytes; /* device scratch the plan owns                   */
+    double alg_bytes;       /* level-by-level algorithmic bytes of one call   */
+} bfs_fdmt_info;
+
+bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc, bfs_fdmt_plan** plan);
+/* Same plan without device resources (introspection only; execute fails). */
+bfs_status bfs_fdmt_plan_create_host(const bfs_fdmt_desc* desc, bfs_fdmt_plan** plan);
+bfs_status bfs_fdmt_plan_destroy(bfs_fdmt_plan* plan);
+bfs_status bfs_fdmt_plan_info(const bfs_fdmt_plan* plan, bfs_fdmt_info* info);
+/* rows_per_level[0..niter] (cap entries at most); returns BFS_ERR_ARG if cap too small */
+bfs_status bfs_fdmt_plan_rows(const bfs_fdmt_plan* plan, int* rows_per_level, int cap);
+/* Host copies of level `level`'s (>= 1) row tables: tail row, head row (-1 = copied row), head shift. */
+bfs_status bfs_fdmt_plan_tables(const bfs_fdmt_plan* plan, int level, int* a_row, int* b_row,
+                                int* shift, int cap);
+/* d_in: nchan*ncols floats (ignored when b_ones != 0: an all-ones image is used,
+ * the reference's normalisation mode), d_out: max_dt*ncols floats. */
+bfs_status bfs_fdmt_execute(bfs_fdmt_plan* plan, const float* d_in, float* d_out, int b_ones,
+                            void* stream);
+
+/* ------------------------------------------------------------------------
+ * Statistical preprocessing of the FDMT input.
+ * Replaces statistical_preprocessing::calc_fdmt_inputs
+ * (L/CDMT/Statistical_preprocessing.cuh:9-10, .cu:15-88): per-row mean and
+ * variance, global mean/std, rows whose variance is > 4 sigma from the mean
+ * variance are zeroed (mask 0), the rest become (x - mean)/std (mask 1).
+ * d_buff: 4 + 2*nrows floats, same layout as the reference:
+ * [row mean][row variance][mean][std][variance mean][variance std].
+ * ---------------------------------------------------------------------- */
+bfs_status bfs_preproc_calc_fdmt_inputs(float* d_inout, int nrows, int ncols, float* d_buff,
+                                        float* d_norm_input, void* stream);
+/* Replaces fdmt_normalization (L/CDMT/Chunk_gpu.cu:842-852):
+ * d_out[i] = d_fdmt[i] / sqrtf(d_norm[i] + 1e-8).  d_out may alias d_fdmt. */
+bfs_status bfs_fdmt_normalize(const float* d_fdmt, const float* d_norm, int64_t n, float* d_out,
+                              void* stream);
+
+/* ------------------------------------------------------------------------
+ * Per-delay-row normalisation of a DM-time plane: out = (x - mean_r)/std_r
+ * with FP64 row statistics (population std).  d_stats (optional, 2*rows
+ * floats) receives [mean_r][std_r].  No reference counterpart: the
+ * reference normalises the FDMT input instead (calc_fdmt_inputs above).
+ * ---------------------------------------------------------------------- */
+bfs_status bfs_norm_rows(const float* d_in, float* d_out, int rows, int cols, float* d_stats,
+                         void* stream);
+/* Only the statistics (2*rows floats: mean then std). */
+bfs_status bfs_row_stats(const float* d_in, int rows, int cols, float* d_stats, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Boxcar detection + candidate compaction.
+ * widths_mode BFS_WIDTHS_POW2, param Q: widths 1,2,4..2^Q, mwidth = log2 w —
+ *   replaces clusterization::gather_candidates_in_dynamicalArray
+ *   (L/Clusterization/Clusterization.cu:56-89, :420-455).
+ * widths_mode BFS_WIDTHS_ALL, param W: widths 1..W, mwidth = w —
+ *   replaces gather_candidates_in_heap_with_plan (Clusterization.cu:169-202,
+ *   :592-671).
+ * The window sum is accumulated sequentially from the start sample (the
+ * reference's order); only complete windows are tested; S/N = sum/sqrtf(w)
+ * with an IEEE divide (snr_fast != 0 uses the reference GPU's __fdividef).
+ * A candidate is emitted when S/N > thr; thr is read from d_thr (device) when
+ * non-NULL, else from `thr`.  d_stats (optional, from bfs_row_stats) makes the
+ * kernel normalise each sample as (x - mean_r)/std_r before summing.
+ * Candidates are returned in canonical row-major order (mdt, mt, width) —
+ * the reference's heap order; the reference's atomic (dynamic) order is not
+ * reproducible.  *h_count receives the total number found; if it exceeds
+ * capacity only `capacity` are written and BFS_ERR_OVERFLOW is returned.
+ * Synchronises `stream` (the count is returned to the host).
+ * ---------------------------------------------------------------------- */
+enum { BFS_WIDTHS_POW2 = 0, BFS_WIDTHS_ALL = 1 };
+bfs_status bfs_boxcar_gather(const float* d_plane, int rows, int cols, const float* d_stats,
+                             float thr, const float* d_thr, int widths_mode, int param,
+                             int snr_fast, bfs_cand* d_out, uint32_t capacity,
+                             uint32_t* h_count, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Clustering + delegates.
+ * Replaces clusterization::complete_clusterization (Clusterization.cu:92-166):
+ * three passes over (mt, mdt, mwidth) — sort inside each group, split where
+ * consecutive keys differ by more than metrics[k] — then per-group argmax of
+ * msnr (select_delegates_kernel, L/Clusterization/select_delegates.cu:63-125,
+ * 64 lanes) and delegates sorted by mt (Clusterization.cu:147-149).  Ties are
+ * broken by candidate index (canonical order).
+ * Outputs (device, capacity n): d_perm (n) = members in group order,
+ * d_offsets (n+1) = group starts, d_delegates (n) = delegate candidate index
+ * per group sorted by (mt, group).  *h_ngroups receives the group count.
+ * Synchronises `stream`.
+ * ---------------------------------------------------------------------- */
+bfs_status bfs_cluster(const bfs_cand* d_cands, uint32_t n, const int* metrics /* host, 3 */,
+                       int* d_perm, int* d_offsets, int* d_delegates, uint32_t* h_ngroups,
+                       void* stream);
+/* The reference's per-group argmax on its own (select_delegates_kernel). */
+bfs_status bfs_select_delegates(const bfs_cand* d_cands, const int* d_perm, uint32_t n,
+                                const int* d_offsets, uint32_t ngroups, int* d_delegates,
+                                void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BFS_H */

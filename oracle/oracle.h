@@ -1,0 +1,54 @@
+/* ORACLE — test infrastructure only.
+ *
+ * CPU restatement of the reference's algorithms on the FDMT + search hot path.
+ * Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use
+ * it, and only as the checker.  The product (cpp_projects_b200/) never links
+ * or calls anything here.
+ *
+ * Parity pinning: the FDMT restatement is checked bit-for-bit against the
+ * reference's own CFdmtCpu compiled from its sources (oracle/_ref, built by
+ * oracle/Makefile) and the search restatement against the reference's golden
+ * CSVs (clusterization_forpravir/Candidates{1,2}.csv, copied as fixtures under
+ * tests/golden/).
+ */
+#ifndef BFS_ORACLE_H
+#define BFS_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same 16-byte layout as the reference's Cand (Clusterization/Candidate.cuh:4-10). */
+typedef struct orc_cand { int mt; int mdt; int mwidth; float msnr; } orc_cand;
+
+/* --- FDMT (reference: MyVSLib_C++/FDMT/FdmtB.cpp, FdmtCpu.cpp) --------- */
+int orc_fdmt_niter(int nchan);
+/* rows_per_level[0..niter] = total rows of each level's plane; returns niter or <0 */
+int orc_fdmt_rows(float fmin, float fmax, int nchan, int max_dt, int* rows_per_level, int cap);
+/* Row tables of level `level` (>=1): for each output row, the tail row, the
+ * head row (-1 for a copied row) and the head shift.  Returns the row count. */
+int orc_fdmt_tables(float fmin, float fmax, int nchan, int max_dt, int level,
+                    int* a_row, int* b_row, int* shift, int cap);
+int orc_fdmt_run_f32(float fmin, float fmax, int nchan, int cols, int max_dt,
+                     const float* in, float* out, int b_ones);
+int orc_fdmt_run_f64(float fmin, float fmax, int nchan, int cols, int max_dt,
+                     const double* in, double* out, int b_ones);
+
+/* --- search (reference: MyVSLib_C++/Clusterization/*.cu) ---------------- */
+int64_t orc_boxcar(const float* plane, int rows, int cols, float thr, int mode,
+                   int param, orc_cand* out, int64_t cap);
+void orc_norm_rows(const float* in, float* out, int rows, int cols,
+                   float* mean_out, float* std_out);
+int orc_select_delegates(const orc_cand* c, const int* perm, const int* offsets,
+                         int ngroups, int block, int* delegates);
+int orc_cluster(const orc_cand* c, int n, const int* metrics, int* perm_out,
+                int* offsets_out, int* delegates_out);
+void orc_calc_fdmt_inputs(float* inout, int rows, int cols, float* norm_input,
+                          float* stats_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,165 @@
+"""ORACLE — test infrastructure only.
+
+ctypes wrapper over ``oracle/liboracle.so`` (the C restatement in
+``fdmt_oracle.c`` / ``search_oracle.c``) and, when it has been built,
+``oracle/_ref/libref_fdmt.so`` (the reference's own ``CFdmtCpu`` compiled from
+its sources by ``oracle/Makefile``).  Only tests/, ``__graft_entry__.smoke()``
+and bench.py's CPU-baseline leg may use this module, and only as the checker.
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_P = ctypes.c_void_p
+_F = ctypes.c_float
+
+CAND_DTYPE = np.dtype([("mt", "<i4"), ("mdt", "<i4"), ("mwidth", "<i4"), ("msnr", "<f4")])
+
+_lib = None
+_ref = None
+
+
+def build() -> None:
+    """Compile the oracle (and the reference shim when the sources exist)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True, capture_output=True)
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        path = HERE / "liboracle.so"
+        if not path.exists():
+            build()
+        _lib = ctypes.CDLL(str(path))
+        _lib.orc_boxcar.restype = ctypes.c_int64
+        _lib.orc_boxcar.argtypes = [_P, ctypes.c_int, ctypes.c_int, _F, ctypes.c_int,
+                                    ctypes.c_int, _P, ctypes.c_int64]
+        for n in ("orc_fdmt_rows", "orc_fdmt_tables", "orc_fdmt_run_f32", "orc_fdmt_run_f64"):
+            getattr(_lib, n).restype = ctypes.c_int
+    return _lib
+
+
+def ref_lib() -> ctypes.CDLL | None:
+    """The reference's CFdmtCpu (oracle/_ref), or None when it was not built."""
+    global _ref
+    if _ref is None:
+        path = HERE / "_ref" / "libref_fdmt.so"
+        if not path.exists():
+            return None
+        _ref = ctypes.CDLL(str(path))
+    return _ref
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_P)
+
+
+# ---- FDMT -------------------------------------------------------------------
+def fdmt_rows(fmin, fmax, nchan, max_dt) -> np.ndarray:
+    rows = np.zeros(64, np.int32)
+    n = lib().orc_fdmt_rows(_F(fmin), _F(fmax), nchan, max_dt, _ptr(rows), rows.size)
+    if n < 0:
+        raise ValueError("bad FDMT parameters")
+    return rows[: n + 1].copy()
+
+
+def fdmt_tables(fmin, fmax, nchan, max_dt, level):
+    n = int(fdmt_rows(fmin, fmax, nchan, max_dt)[level])
+    a = np.zeros(n, np.int32); b = np.zeros(n, np.int32); s = np.zeros(n, np.int32)
+    lib().orc_fdmt_tables(_F(fmin), _F(fmax), nchan, max_dt, level, _ptr(a), _ptr(b), _ptr(s), n)
+    return a, b, s
+
+
+def fdmt_f32(fmin, fmax, x: np.ndarray | None, nchan, ncols, max_dt, b_ones=False) -> np.ndarray:
+    out = np.zeros((max_dt, ncols), np.float32)
+    xin = np.zeros(1, np.float32) if b_ones else np.ascontiguousarray(x, np.float32)
+    rc = lib().orc_fdmt_run_f32(_F(fmin), _F(fmax), nchan, ncols, max_dt, _ptr(xin), _ptr(out),
+                                1 if b_ones else 0)
+    if rc != 0:
+        raise ValueError(f"oracle FDMT failed ({rc})")
+    return out
+
+
+def fdmt_f64(fmin, fmax, x: np.ndarray | None, nchan, ncols, max_dt, b_ones=False) -> np.ndarray:
+    out = np.zeros((max_dt, ncols), np.float64)
+    xin = np.zeros(1, np.float64) if b_ones else np.ascontiguousarray(x, np.float64)
+    rc = lib().orc_fdmt_run_f64(_F(fmin), _F(fmax), nchan, ncols, max_dt, _ptr(xin), _ptr(out),
+                                1 if b_ones else 0)
+    if rc != 0:
+        raise ValueError(f"oracle FDMT failed ({rc})")
+    return out
+
+
+def ref_fdmt_cpu(fmin, fmax, x: np.ndarray | None, nchan, ncols, max_dt, b_ones=False,
+                 threads=1) -> np.ndarray | None:
+    """Runs the reference's CFdmtCpu::process_image (None if not built)."""
+    r = ref_lib()
+    if r is None:
+        return None
+    out = np.zeros((max_dt, ncols), np.float32)
+    xin = np.ones((nchan, ncols), np.float32) if b_ones else np.ascontiguousarray(x, np.float32)
+    r.ref_fdmt_cpu_process(_F(fmin), _F(fmax), nchan, ncols, max_dt, _ptr(xin), _ptr(out),
+                           1 if b_ones else 0, threads)
+    return out
+
+
+# ---- search -----------------------------------------------------------------
+def boxcar(plane: np.ndarray, thr: float, mode: int, param: int, cap: int = 1 << 22) -> np.ndarray:
+    plane = np.ascontiguousarray(plane, np.float32)
+    rows, cols = plane.shape
+    out = np.zeros(cap, CAND_DTYPE)
+    n = lib().orc_boxcar(_ptr(plane), rows, cols, _F(thr), mode, param, _ptr(out), cap)
+    if n > cap:
+        raise ValueError(f"oracle boxcar capacity {cap} exceeded ({n})")
+    return out[:n].copy()
+
+
+def norm_rows(plane: np.ndarray):
+    plane = np.ascontiguousarray(plane, np.float32)
+    rows, cols = plane.shape
+    out = np.zeros_like(plane)
+    mean = np.zeros(rows, np.float32); std = np.zeros(rows, np.float32)
+    lib().orc_norm_rows(_ptr(plane), _ptr(out), rows, cols, _ptr(mean), _ptr(std))
+    return out, mean, std
+
+
+def cluster(cands: np.ndarray, metrics):
+    cands = np.ascontiguousarray(cands, CAND_DTYPE)
+    n = len(cands)
+    perm = np.zeros(max(n, 1), np.int32)
+    offs = np.zeros(n + 1, np.int32)
+    dl = np.zeros(max(n, 1), np.int32)
+    m = np.asarray(metrics, np.int32)
+    g = lib().orc_cluster(_ptr(cands), n, _ptr(m), _ptr(perm), _ptr(offs), _ptr(dl))
+    return perm[:n].copy(), offs[: g + 1].copy(), dl[:g].copy()
+
+
+def select_delegates(cands, perm, offsets, block=64):
+    cands = np.ascontiguousarray(cands, CAND_DTYPE)
+    perm = np.ascontiguousarray(perm, np.int32)
+    offsets = np.ascontiguousarray(offsets, np.int32)
+    g = len(offsets) - 1
+    out = np.zeros(max(g, 1), np.int32)
+    lib().orc_select_delegates(_ptr(cands), _ptr(perm), _ptr(offsets), g, block, _ptr(out))
+    return out[:g].copy()
+
+
+def calc_fdmt_inputs(x: np.ndarray):
+    x = np.array(x, np.float32, copy=True, order="C")
+    rows, cols = x.shape
+    mask = np.zeros_like(x)
+    stats = np.zeros(2 * rows + 4, np.float32)
+    lib().orc_calc_fdmt_inputs(_ptr(x), rows, cols, _ptr(mask), _ptr(stats))
+    return x, mask, stats
+
+
+def fdmt_normalize(fdmt: np.ndarray, norm: np.ndarray) -> np.ndarray:
+    """fdmt / sqrtf(norm + 1e-8): the double-literal sum rounded to float first
+    (L/CDMT/Chunk_gpu.cu:842-852)."""
+    den = np.sqrt((norm.astype(np.float64) + 1e-8).astype(np.float32))
+    return (fdmt.astype(np.float32) / den).astype(np.float32)

@@ -1,0 +1,88 @@
+"""GPU parity of the FDMT (through the C ABI) against the oracle, which is
+itself bit-exact against the reference's CFdmtCpu.  Integer row tables plus
+round-to-nearest float arithmetic make the GPU result bit-identical."""
+import numpy as np
+import pytest
+import torch
+
+from cpp_projects_b200 import CFdmtGpu, synth
+from oracle import pyoracle
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    (1200.0, 1600.0, 64, 1024, 64),
+    (1200.0, 1600.0, 512, 4096, 512),
+    (1100.0, 1500.0, 100, 2048, 77),
+    (1200.0, 1600.0, 48, 2000, 48),
+    (1200.0, 1328.0, 1024, 3000, 1024),
+    (1200.0, 1600.0, 3, 64, 5),
+    (1200.0, 1600.0, 2, 33, 3),
+    (1200.0, 1600.0, 256, 1, 256),     # a single time sample
+    (1200.0, 1600.0, 300, 4097, 300),  # ragged length
+]
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("fuse", [0, -1])
+def test_fdmt_bit_exact_vs_oracle(cuda, case, fuse):
+    fmin, fmax, nchan, ncols, max_dt = case
+    x = np.random.default_rng(11).standard_normal((nchan, ncols)).astype(np.float32)
+    f = CFdmtGpu(fmin, fmax, nchan, ncols, max_dt, fuse_depth=fuse)
+    d_in = torch.from_numpy(x).to(cuda)
+    d_out = torch.full((max_dt, ncols), float("nan"), device=cuda)
+    f.process_image(d_in, d_out, False)
+    got = d_out.cpu().numpy()
+    want = pyoracle.fdmt_f32(fmin, fmax, x, nchan, ncols, max_dt)
+    assert np.array_equal(_bits(got), _bits(want))
+
+
+@pytest.mark.parametrize("fuse", [0, -1])
+def test_fdmt_ones_mode(cuda, fuse):
+    fmin, fmax, nchan, ncols, max_dt = 1200.0, 1600.0, 512, 2048, 512
+    f = CFdmtGpu(fmin, fmax, nchan, ncols, max_dt, fuse_depth=fuse)
+    d_out = torch.zeros((max_dt, ncols), device=cuda)
+    f.process_image(None, d_out, True)
+    want = pyoracle.fdmt_f32(fmin, fmax, None, nchan, ncols, max_dt, b_ones=True)
+    assert np.array_equal(d_out.cpu().numpy(), want)
+
+
+def test_fdmt_config0_full_size_bit_exact_and_fp64_error(cuda):
+    beam = synth.config0()
+    x = synth.filterbank(beam)
+    f = CFdmtGpu(beam.fmin, beam.fmax, beam.nchan, beam.nsamp, beam.max_dt)
+    d_out = torch.empty((beam.max_dt, beam.nsamp), device=cuda)
+    f.process_image(torch.from_numpy(x).to(cuda), d_out)
+    got = d_out.cpu().numpy()
+    want = pyoracle.fdmt_f32(beam.fmin, beam.fmax, x, beam.nchan, beam.nsamp, beam.max_dt)
+    assert np.array_equal(_bits(got), _bits(want))
+    f64 = pyoracle.fdmt_f64(beam.fmin, beam.fmax, x.astype(np.float64), beam.nchan,
+                            beam.nsamp, beam.max_dt)
+    rel = np.abs(got - f64).max() / np.abs(f64).max()
+    print(f"config0 FDMT max error vs FP64, relative to max |out|: {rel:.3e}")
+    assert rel < 1e-5
+
+
+def test_fdmt_deterministic_and_stream_ordered(cuda):
+    fmin, fmax, nchan, ncols, max_dt = 1200.0, 1600.0, 1024, 8192, 1024
+    x = torch.randn((nchan, ncols), device=cuda, generator=torch.Generator(cuda).manual_seed(3))
+    f = CFdmtGpu(fmin, fmax, nchan, ncols, max_dt)
+    s = torch.cuda.Stream()
+    outs = []
+    with torch.cuda.stream(s):
+        for _ in range(2):
+            o = torch.empty((max_dt, ncols), device=cuda)
+            f.process_image(x, o)
+            outs.append(o)
+    s.synchronize()
+    assert torch.equal(outs[0], outs[1])
+
+
+def test_fdmt_rejects_bad_sizes(cuda):
+    f = CFdmtGpu(1200.0, 1600.0, 64, 128, 64)
+    with pytest.raises(ValueError):
+        f.process_image(torch.zeros(10, device=cuda), torch.zeros((64, 128), device=cuda))
