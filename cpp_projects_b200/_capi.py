@@ -17,6 +17,7 @@ BFS_OK, BFS_ERR_ARG, BFS_ERR_CUDA, BFS_ERR_OVERFLOW, BFS_ERR_TIMEOUT, BFS_ERR_AL
 STATUS_NAMES = {0: "BFS_OK", 1: "BFS_ERR_ARG", 2: "BFS_ERR_CUDA", 3: "BFS_ERR_OVERFLOW",
                 4: "BFS_ERR_TIMEOUT", 5: "BFS_ERR_ALLOC", 6: "BFS_ERR_UNSUPPORTED"}
 BFS_WIDTHS_POW2, BFS_WIDTHS_ALL = 0, 1
+BFS_FDMT_EXTERNAL_WS = 1
 
 
 class BfsError(RuntimeError):
@@ -29,7 +30,7 @@ class FdmtDesc(ctypes.Structure):
     _fields_ = [("fmin", ctypes.c_float), ("fmax", ctypes.c_float), ("nchan", ctypes.c_int),
                 ("ncols", ctypes.c_int), ("max_dt", ctypes.c_int), ("plan_kind", ctypes.c_int),
                 ("precision", ctypes.c_int), ("fuse_depth", ctypes.c_int),
-                ("reserved", ctypes.c_int * 8)]
+                ("flags", ctypes.c_int), ("reserved", ctypes.c_int * 7)]
 
 
 class FdmtInfo(ctypes.Structure):
@@ -59,7 +60,10 @@ _SIGNATURES = {
     "bfs_fdmt_plan_info": (_I, [_P, ctypes.POINTER(FdmtInfo)]),
     "bfs_fdmt_plan_rows": (_I, [_P, _P, _I]),
     "bfs_fdmt_plan_tables": (_I, [_P, _I, _P, _P, _P, _I]),
+    "bfs_fdmt_plan_head": (_I, [_P, _P, _P, _I, _P, _I]),
     "bfs_fdmt_execute": (_I, [_P, _P, _P, _I, _P]),
+    "bfs_fdmt_workspace_size": (_I, [_P, ctypes.POINTER(ctypes.c_size_t)]),
+    "bfs_fdmt_execute_ws": (_I, [_P, _P, _P, _I, _P, ctypes.c_size_t, _P]),
     "bfs_preproc_calc_fdmt_inputs": (_I, [_P, _I, _I, _P, _P, _P]),
     "bfs_fdmt_normalize": (_I, [_P, _P, _I64, _P, _P]),
     "bfs_norm_rows": (_I, [_P, _P, _I, _I, _P, _P]),

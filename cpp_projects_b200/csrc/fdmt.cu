@@ -26,12 +26,23 @@ struct bfs_fdmt_plan {
     bfs::FdmtPlanHost host;
     int device = -1;
     bool host_only = false;
+    bool external_ws = false;
     int fuse_depth = 0;
     int4* d_tab = nullptr;             // per level, per output row: {a, b, shift, 0}
     std::vector<size_t> tab_off;       // offset of each level's table in d_tab
     float* d_buf[2] = {nullptr, nullptr};
     size_t buf_rows[2] = {0, 0};
     size_t ws_bytes = 0;
+    bfs::HeadPlan head;                     // fused levels 0..k (depth 0 = not used)
+    bfs::HeadGroup* d_head_groups = nullptr;
+    int* d_head_tab = nullptr;
+    ~bfs_fdmt_plan() {
+        if (d_tab) cudaFree(d_tab);
+        if (d_head_groups) cudaFree(d_head_groups);
+        if (d_head_tab) cudaFree(d_head_tab);
+        for (float* b : d_buf)
+            if (b) cudaFree(b);
+    }
 };
 
 namespace bfs {
@@ -95,6 +106,81 @@ k_fdmt_level(const float* __restrict__ in, float* __restrict__ out, const int4* 
     }
 }
 
+// Fused levels 0..depth for one group of `group` adjacent channels and one
+// tile of `tile` output samples.  blockDim.x = the tile plus the group's
+// look-back (rounded to a warp): thread u owns sample t = tile0 - halo + u of
+// every row.  Level 0 goes to shared buffer A, level 1 to B, level 2 to A, ...
+// and the last level straight to the level-`depth` plane in HBM.  Only
+// samples u >= halo are written; the plan's look-back guarantees that every
+// value they depend on was computed from in-tile samples (u - shift >= 0), so
+// the halo columns may hold partial values.  Samples t < 0 are the zeros the
+// reference's planes hold there.
+// grid: (ceil(ncols / tile), nchan / group)
+__global__ void __launch_bounds__(1024)
+k_fdmt_head(const float* __restrict__ x, float* __restrict__ out,
+            const HeadGroup* __restrict__ groups, const int4* __restrict__ tab, int ncols,
+            int depth, int group, int rows_per_chan, int tile, int rows_a, int ones) {
+    extern __shared__ float sm[];
+    const int W = blockDim.x;
+    const int u = threadIdx.x;
+    const HeadGroup* hg = groups + blockIdx.y;
+    const int halo = __ldg(&hg->halo);
+    const int t = blockIdx.x * tile - halo + u;
+    float* bufa = sm;
+    float* bufb = sm + rows_a * W;
+
+    const int c0 = blockIdx.y * group;
+    for (int c = 0; c < group; ++c) {
+        const float* xr = x + static_cast<size_t>(c0 + c) * ncols;
+        float* dst = bufa + c * rows_per_chan * W + u;
+        float v = 0.0f;
+        if (t >= 0) v = ones ? 1.0f : (t < ncols ? __ldg(xr + t) : 0.0f);
+        dst[0] = v;
+        for (int r = 1; r < rows_per_chan; ++r) {
+            float w = 0.0f;
+            if (t >= r) {
+                const int tt = t - r;
+                const float xv = ones ? 1.0f : (tt < ncols ? __ldg(xr + tt) : 0.0f);
+                v = __fdiv_rn(__fadd_rn(__fmul_rn(v, static_cast<float>(r)), xv),
+                              static_cast<float>(r + 1));
+                w = v;
+            }
+            dst[r * W] = w;
+        }
+    }
+    __syncthreads();
+
+    float* src = bufa;
+    float* dst = bufb;
+    const bool writer = (u >= halo) && (u < halo + tile) && (t < ncols);
+    for (int l = 1; l <= depth; ++l) {
+        const int rows = __ldg(&hg->rows[l]);
+        const int4* tb = tab + __ldg(&hg->tab_off[l]);
+        if (l < depth) {
+            for (int j = 0; j < rows; ++j) {
+                const int4 e = __ldg(tb + j);
+                float v = src[e.x * W + u];
+                if (t >= e.z && u >= e.z) v = __fadd_rn(v, src[e.y * W + u - e.z]);
+                dst[j * W + u] = v;
+            }
+            __syncthreads();
+            float* tmp = src; src = dst; dst = tmp;
+        } else {
+            float* o = out + static_cast<size_t>(__ldg(&hg->out_row0)) * ncols + t;
+            for (int j = 0; j < rows; ++j) {
+                const int4 e = __ldg(tb + j);
+                float v = src[e.x * W + u];
+                if (t >= e.z && u >= e.z) v = __fadd_rn(v, src[e.y * W + u - e.z]);
+                if (writer) o[static_cast<size_t>(j) * ncols] = v;
+            }
+        }
+    }
+}
+
+constexpr int kHeadTile = 256;
+constexpr size_t kHeadSmemTwoPerSm = 113 * 1024;  // two CTAs per SM
+constexpr size_t kHeadSmemMax = 227 * 1024;
+
 }  // namespace
 }  // namespace bfs
 
@@ -106,8 +192,27 @@ static bfs_status plan_host_part(const bfs_fdmt_desc* desc, std::unique_ptr<bfs_
     BFS_ARG(desc->precision == BFS_PREC_F32, "unsupported precision %d", desc->precision);
     p.reset(new bfs_fdmt_plan);
     p->host_only = true;
-    return build_fdmt_plan(desc->fmin, desc->fmax, desc->nchan, desc->ncols, desc->max_dt,
-                           &p->host);
+    bfs_status st = build_fdmt_plan(desc->fmin, desc->fmax, desc->nchan, desc->ncols,
+                                    desc->max_dt, &p->host);
+    if (st != BFS_OK) return st;
+    const FdmtPlanHost& h = p->host;
+    // fused head: explicit depth, or the deepest one that keeps two CTAs per SM
+    if (desc->fuse_depth != 0) {
+        const int want = desc->fuse_depth < 0 ? kHeadMaxDepth : desc->fuse_depth;
+        const size_t limit = desc->fuse_depth < 0 ? kHeadSmemTwoPerSm : kHeadSmemMax;
+        for (int k = std::min(want, h.niter); k >= 1; --k) {
+            HeadPlan hp;
+            if (build_head_plan(h, k, kHeadTile, limit, &hp)) {
+                p->head = std::move(hp);
+                break;
+            }
+            if (desc->fuse_depth > 0) break;  // an explicit depth is not lowered silently
+        }
+        BFS_ARG(desc->fuse_depth <= 0 || p->head.depth == desc->fuse_depth,
+                "fuse_depth %d is not usable for this plan", desc->fuse_depth);
+    }
+    p->fuse_depth = p->head.depth;
+    return BFS_OK;
 }
 
 extern "C" bfs_status bfs_fdmt_plan_create_host(const bfs_fdmt_desc* desc, bfs_fdmt_plan** plan) {
@@ -129,7 +234,18 @@ extern "C" bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc, bfs_fdmt_p
     p->host_only = false;
     BFS_CUDA(cudaGetDevice(&p->device));
     const FdmtPlanHost& h = p->host;
-    p->fuse_depth = 0;
+    if (p->head.depth > 0) {
+        const HeadPlan& hp = p->head;
+        BFS_CUDA(cudaMalloc(&p->d_head_groups, hp.groups.size() * sizeof(HeadGroup)));
+        BFS_CUDA(cudaMemcpy(p->d_head_groups, hp.groups.data(),
+                            hp.groups.size() * sizeof(HeadGroup), cudaMemcpyHostToDevice));
+        BFS_CUDA(cudaMalloc(&p->d_head_tab, hp.tab.size() * sizeof(int)));
+        BFS_CUDA(cudaMemcpy(p->d_head_tab, hp.tab.data(), hp.tab.size() * sizeof(int),
+                            cudaMemcpyHostToDevice));
+        if (hp.smem_bytes > 48 * 1024)
+            BFS_CUDA(cudaFuncSetAttribute(k_fdmt_head, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(hp.smem_bytes)));
+    }
 
     // device row tables
     std::vector<int4> tab;
@@ -145,17 +261,18 @@ extern "C" bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc, bfs_fdmt_p
         BFS_CUDA(cudaMemcpy(p->d_tab, tab.data(), tab.size() * sizeof(int4),
                             cudaMemcpyHostToDevice));
     }
-    // ping-pong planes: level l lives in buffer l & 1; the last level goes to the output
-    for (int l = 0; l < h.niter; ++l)
+    // ping-pong planes: level l lives in buffer l & 1; the last level goes to the
+    // output; levels inside the fused head never reach HBM
+    for (int l = p->head.depth; l < h.niter; ++l)
         p->buf_rows[l & 1] = std::max(p->buf_rows[l & 1], static_cast<size_t>(h.lv[l].total_rows()));
-    for (int b = 0; b < 2; ++b) {
+    p->external_ws = (desc->flags & BFS_FDMT_EXTERNAL_WS) != 0;
+    for (int b = 0; b < 2 && !p->external_ws; ++b) {
         if (p->buf_rows[b] == 0) continue;
         const size_t bytes = p->buf_rows[b] * static_cast<size_t>(h.ncols) * sizeof(float);
         cudaError_t e = cudaMalloc(&p->d_buf[b], bytes);
         if (e != cudaSuccess) {
             cudaGetLastError();
-            if (p->d_buf[0]) cudaFree(p->d_buf[0]);
-            if (p->d_tab) cudaFree(p->d_tab);
+            p->d_buf[b] = nullptr;
             return fail(BFS_ERR_ALLOC, "cudaMalloc(%zu) for an FDMT plane failed: %s", bytes,
                         cudaGetErrorString(e));
         }
@@ -166,11 +283,26 @@ extern "C" bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc, bfs_fdmt_p
 }
 
 extern "C" bfs_status bfs_fdmt_plan_destroy(bfs_fdmt_plan* plan) {
-    if (!plan) return BFS_OK;
-    if (plan->d_tab) cudaFree(plan->d_tab);
-    for (float* b : plan->d_buf)
-        if (b) cudaFree(b);
     delete plan;
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_fdmt_plan_head(const bfs_fdmt_plan* plan, int* params, int* groups,
+                                         int group_cap, int* tab, int tab_cap) {
+    BFS_ARG(plan != nullptr && params != nullptr, "null argument");
+    const HeadPlan& hp = plan->head;
+    params[0] = hp.depth; params[1] = hp.group; params[2] = hp.tile; params[3] = hp.width;
+    params[4] = hp.rows_a; params[5] = hp.rows_b; params[6] = static_cast<int>(hp.smem_bytes);
+    params[7] = static_cast<int>(hp.groups.size()); params[8] = static_cast<int>(hp.tab.size() / 4);
+    const int gi = static_cast<int>(sizeof(HeadGroup) / sizeof(int));
+    if (groups) {
+        BFS_ARG(group_cap >= params[7] * gi, "groups needs %d ints", params[7] * gi);
+        std::memcpy(groups, hp.groups.data(), hp.groups.size() * sizeof(HeadGroup));
+    }
+    if (tab) {
+        BFS_ARG(tab_cap >= static_cast<int>(hp.tab.size()), "tab needs %zu ints", hp.tab.size());
+        std::memcpy(tab, hp.tab.data(), hp.tab.size() * sizeof(int));
+    }
     return BFS_OK;
 }
 
@@ -213,29 +345,71 @@ extern "C" bfs_status bfs_fdmt_plan_tables(const bfs_fdmt_plan* plan, int level,
     return BFS_OK;
 }
 
-extern "C" bfs_status bfs_fdmt_execute(bfs_fdmt_plan* plan, const float* d_in, float* d_out,
-                                       int b_ones, void* stream) {
-    BFS_ARG(plan != nullptr && d_out != nullptr, "null argument");
-    BFS_ARG(!plan->host_only, "plan was created with bfs_fdmt_plan_create_host");
-    BFS_ARG(b_ones || d_in != nullptr, "d_in is null");
+static size_t plane_bytes(const bfs_fdmt_plan* p, int b) {
+    const size_t raw = p->buf_rows[b] * static_cast<size_t>(p->host.ncols) * sizeof(float);
+    return (raw + 255) & ~static_cast<size_t>(255);
+}
+
+extern "C" bfs_status bfs_fdmt_workspace_size(const bfs_fdmt_plan* plan, size_t* bytes) {
+    BFS_ARG(plan != nullptr && bytes != nullptr, "null argument");
+    *bytes = plane_bytes(plan, 0) + plane_bytes(plan, 1);
+    return BFS_OK;
+}
+
+static bfs_status fdmt_run(bfs_fdmt_plan* plan, const float* d_in, float* d_out, int b_ones,
+                           float* buf0, float* buf1, cudaStream_t s) {
     const FdmtPlanHost& h = plan->host;
-    cudaStream_t s = as_stream(stream);
     const int T = h.ncols;
-    {
+    float* bufs[2] = {buf0, buf1};
+    const int k = plan->head.depth;
+    if (k > 0) {
+        const HeadPlan& hp = plan->head;
+        dim3 grid((T + hp.tile - 1) / hp.tile, h.nchan / hp.group);
+        BFS_ARG(grid.y <= 65535, "nchan too large for this build");
+        float* dst = (k == h.niter) ? d_out : bufs[k & 1];
+        k_fdmt_head<<<grid, hp.width, hp.smem_bytes, s>>>(
+            d_in, dst, plan->d_head_groups, reinterpret_cast<const int4*>(plan->d_head_tab), T, k,
+            hp.group, h.rows_per_chan0, hp.tile, hp.rows_a, b_ones ? 1 : 0);
+        BFS_LAUNCH_CHECK("k_fdmt_head");
+    } else {
         dim3 grid((T + kInitThreads * kInitCols - 1) / (kInitThreads * kInitCols), h.nchan);
         BFS_ARG(grid.y <= 65535, "nchan too large for this build");
-        k_fdmt_init<<<grid, kInitThreads, 0, s>>>(d_in, plan->d_buf[0], T, h.rows_per_chan0,
+        k_fdmt_init<<<grid, kInitThreads, 0, s>>>(d_in, bufs[0], T, h.rows_per_chan0,
                                                   b_ones ? 1 : 0);
         BFS_LAUNCH_CHECK("k_fdmt_init");
     }
     const int chunk = kLevelThreads * kLevelCols;
-    for (int l = 1; l <= h.niter; ++l) {
-        const float* src = plan->d_buf[(l - 1) & 1];
-        float* dst = (l == h.niter) ? d_out : plan->d_buf[l & 1];
+    for (int l = k + 1; l <= h.niter; ++l) {
+        const float* src = bufs[(l - 1) & 1];
+        float* dst = (l == h.niter) ? d_out : bufs[l & 1];
         dim3 grid(h.lv[l].total_rows(), (T + chunk - 1) / chunk);
         BFS_ARG(grid.y <= 65535, "ncols too large for this build");
         k_fdmt_level<<<grid, kLevelThreads, 0, s>>>(src, dst, plan->d_tab + plan->tab_off[l], T);
         BFS_LAUNCH_CHECK("k_fdmt_level");
     }
     return BFS_OK;
+}
+
+extern "C" bfs_status bfs_fdmt_execute(bfs_fdmt_plan* plan, const float* d_in, float* d_out,
+                                       int b_ones, void* stream) {
+    BFS_ARG(plan != nullptr && d_out != nullptr, "null argument");
+    BFS_ARG(!plan->host_only, "plan was created with bfs_fdmt_plan_create_host");
+    BFS_ARG(!plan->external_ws, "plan has no planes of its own: use bfs_fdmt_execute_ws");
+    BFS_ARG(b_ones || d_in != nullptr, "d_in is null");
+    return fdmt_run(plan, d_in, d_out, b_ones, plan->d_buf[0], plan->d_buf[1], as_stream(stream));
+}
+
+extern "C" bfs_status bfs_fdmt_execute_ws(bfs_fdmt_plan* plan, const float* d_in, float* d_out,
+                                          int b_ones, void* d_workspace, size_t workspace_bytes,
+                                          void* stream) {
+    BFS_ARG(plan != nullptr && d_out != nullptr, "null argument");
+    BFS_ARG(!plan->host_only, "plan was created with bfs_fdmt_plan_create_host");
+    BFS_ARG(b_ones || d_in != nullptr, "d_in is null");
+    const size_t need = plane_bytes(plan, 0) + plane_bytes(plan, 1);
+    BFS_ARG(d_workspace != nullptr && workspace_bytes >= need,
+            "workspace of %zu bytes is smaller than the %zu needed", workspace_bytes, need);
+    BFS_ARG((reinterpret_cast<uintptr_t>(d_workspace) & 255) == 0, "workspace must be 256-byte aligned");
+    char* w = static_cast<char*>(d_workspace);
+    return fdmt_run(plan, d_in, d_out, b_ones, reinterpret_cast<float*>(w),
+                    reinterpret_cast<float*>(w + plane_bytes(plan, 0)), as_stream(stream));
 }

@@ -67,4 +67,34 @@ struct FdmtPlanHost {
 bfs_status build_fdmt_plan(float fmin, float fmax, int nchan, int ncols, int max_dt,
                            FdmtPlanHost* out);
 
+// ---------------------------------------------------------------------------
+// Fused "head" of the FDMT: levels 0..k of one group of 2^k adjacent channels
+// computed by one CTA over a time tile, all intermediate levels in shared
+// memory.  Tables index rows local to the group's shared-memory planes.
+// ---------------------------------------------------------------------------
+constexpr int kHeadMaxDepth = 8;
+
+struct HeadGroup {                  // device-side, one per channel group
+    int halo;                       // samples of look-back of the group's level-k rows
+    int out_row0;                   // first row of the group's sub-band in the level-k plane
+    int rows[kHeadMaxDepth + 1];    // rows of the group at levels 0..k
+    int tab_off[kHeadMaxDepth + 1]; // offset of level l's table (l >= 1)
+};
+
+struct HeadPlan {
+    int depth = 0;          // k (0 = no fused head)
+    int group = 1;          // 2^k channels per CTA
+    int tile = 0;           // output samples per CTA
+    int width = 0;          // tile + max halo, rounded to a warp: threads per CTA
+    int rows_a = 0;         // shared rows of the even-level buffer (level 0, 2, ...)
+    int rows_b = 0;         // shared rows of the odd-level buffer
+    size_t smem_bytes = 0;
+    std::vector<HeadGroup> groups;
+    std::vector<int> tab;   // 4 ints per row: {a_local, b_local, shift, 0}
+};
+
+// Head plan for depth k and tile width; returns false when k is not usable
+// (k > trailing zero bits of nchan, k > niter, or too much shared memory).
+bool build_head_plan(const FdmtPlanHost& p, int k, int tile, size_t smem_limit, HeadPlan* out);
+
 }  // namespace bfs

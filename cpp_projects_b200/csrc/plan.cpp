@@ -16,6 +16,7 @@
 // the device with the approximate __fdividef (L/FDMT/FdmtGpu.cu:372-373); the
 // CPU class (the parity oracle) uses exact division, which is what is
 // reproduced here, once, on the host.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -154,6 +155,61 @@ bfs_status build_fdmt_plan(float fmin, float fmax, int nchan, int ncols, int max
         }
     }
     return BFS_OK;
+}
+
+bool build_head_plan(const FdmtPlanHost& p, int k, int tile, size_t smem_limit, HeadPlan* out) {
+    if (k < 1 || k > kHeadMaxDepth || k > p.niter || tile < 32) return false;
+    const int G = 1 << k;
+    if (p.nchan % G != 0) return false;  // every level <= k must pair sub-bands evenly
+    for (int l = 1; l <= k; ++l)
+        if (p.lv[l].nsub * (1 << l) != p.nchan) return false;
+    HeadPlan h;
+    h.depth = k;
+    h.group = G;
+    h.tile = tile;
+    const int ngroups = p.nchan / G;
+    int max_halo = 0;
+    for (int g = 0; g < ngroups; ++g) {
+        HeadGroup hg{};
+        hg.rows[0] = G * p.rows_per_chan0;
+        int rows_a = hg.rows[0], rows_b = 0;
+        for (int l = 1; l <= k; ++l) {
+            const FdmtLevel& L = p.lv[l];
+            const FdmtLevel& P = p.lv[l - 1];
+            const int sub_per_group = G >> l;        // sub-bands of this group at level l
+            const int s0 = g * sub_per_group;
+            const int row0 = L.cum[s0], row1 = L.cum[s0 + sub_per_group];
+            const int in0 = P.cum[g * (sub_per_group * 2)];
+            hg.rows[l] = row1 - row0;
+            hg.tab_off[l] = static_cast<int>(h.tab.size() / 4);
+            for (int r = row0; r < row1; ++r) {
+                if (L.b_row[r] < 0) return false;    // no carried-over rows inside a group
+                h.tab.push_back(L.a_row[r] - in0);
+                h.tab.push_back(L.b_row[r] - in0);
+                h.tab.push_back(L.shift[r]);
+                h.tab.push_back(0);
+            }
+            if (l < k) {
+                if (l & 1) rows_b = std::max(rows_b, hg.rows[l]);
+                else rows_a = std::max(rows_a, hg.rows[l]);
+            } else {
+                hg.out_row0 = row0;
+                int lb = 0;
+                for (int r = row0; r < row1; ++r) lb = std::max(lb, L.lookback[r]);
+                hg.halo = lb;
+            }
+        }
+        h.rows_a = std::max(h.rows_a, rows_a);
+        h.rows_b = std::max(h.rows_b, rows_b);
+        max_halo = std::max(max_halo, hg.halo);
+        h.groups.push_back(hg);
+    }
+    h.width = ((tile + max_halo) + 31) / 32 * 32;
+    if (h.width > 1024) return false;
+    h.smem_bytes = static_cast<size_t>(h.rows_a + h.rows_b) * h.width * sizeof(float);
+    if (h.smem_bytes > smem_limit) return false;
+    *out = std::move(h);
+    return true;
 }
 
 }  // namespace bfs

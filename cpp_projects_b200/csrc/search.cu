@@ -1,0 +1,292 @@
+// Search stage on sm_100a: per-row statistics, per-row normalisation and the
+// fused normalise + boxcar + candidate-compaction kernel.
+//
+// Boxcar semantics (reference L/Clusterization/Clusterization.cu):
+//   POW2 mode  gather_candidates_in_dynamicalArray_kernel (:420-455): for each
+//              start sample t a running sum x[t] + x[t+1] + ... is tested at
+//              w = 1, 2, 4, .., 2^Q; mwidth = log2 w;
+//   ALL mode   do_plan_kernel / gather_candidates_in_heap_kernel (:592-671):
+//              every w = 1..W, mwidth = w (the same running sum, since the
+//              reference re-adds x[t..t+w-1] from x[t] in order);
+//   a window is only tested when it lies inside the row; S/N = sum / sqrtf(w)
+//   and a candidate is emitted when S/N > thr.
+// The running sum is sequential from the start sample, as in the reference
+// (a prefix-sum difference rounds differently and would flip candidates at
+// the threshold).
+//
+// Compaction: lanes that pass a test are appended with one atomicAdd per warp
+// (ballot + popc); the set of candidates is deterministic, their order is not,
+// so the list is then sorted by the canonical key (mdt, mt, width) — the
+// reference's heap order — with a stable device radix sort.
+#include <cub/device/device_radix_sort.cuh>
+
+#include "internal.h"
+#include "search_common.cuh"
+
+namespace bfs {
+namespace {
+
+constexpr int kBoxThreads = 256;
+constexpr int kBoxTile = 1024;  // start samples per CTA
+constexpr int kMaxPow2Q = 16;
+constexpr int kMaxAllW = 4096;
+constexpr int kWidthBits = 12;
+
+// stats[r] = mean, stats[rows + r] = std (mode 0) or population variance (mode 1)
+__global__ void __cluster_dims__(kStatCluster, 1, 1) __launch_bounds__(kStatThreads)
+k_row_stats(const float* __restrict__ plane, int rows, int cols, float* __restrict__ stats,
+            int mode) {
+    const int row = blockIdx.y;
+    double s, q;
+    cluster_row_moments(plane + static_cast<size_t>(row) * cols, cols, s, q);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const double mean = s / cols;
+        double var = q / cols - mean * mean;
+        if (mode == 0) {
+            if (var < 0.0) var = 0.0;
+            stats[row] = static_cast<float>(mean);
+            stats[rows + row] = static_cast<float>(sqrt(var));
+        } else {
+            stats[row] = static_cast<float>(mean);
+            stats[rows + row] = static_cast<float>(var);
+        }
+    }
+}
+
+__device__ __forceinline__ float norm_sample(float v, float m, float s) {
+    return s > 0.0f ? __fdiv_rn(__fsub_rn(v, m), s) : 0.0f;
+}
+
+__global__ void k_norm_rows(const float* __restrict__ in, float* __restrict__ out, int rows,
+                            int cols, const float* __restrict__ stats) {
+    const int row = blockIdx.y;
+    const float m = stats[row], s = stats[rows + row];
+    const size_t base = static_cast<size_t>(row) * cols;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cols; t += gridDim.x * blockDim.x)
+        out[base + t] = norm_sample(__ldg(in + base + t), m, s);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kBoxThreads)
+k_boxcar(const float* __restrict__ plane, int rows, int cols, const float* __restrict__ stats,
+         const float* __restrict__ d_thr, float thr_host, int wmax, int snr_fast,
+         bfs_cand* __restrict__ out, unsigned capacity, unsigned* __restrict__ d_count) {
+    extern __shared__ float tile[];
+    const int row = blockIdx.y;
+    const int t0 = blockIdx.x * kBoxTile;
+    const float* x = plane + static_cast<size_t>(row) * cols;
+    const int span = kBoxTile + wmax - 1;
+    float m = 0.0f, sd = 0.0f;
+    if (stats) { m = stats[row]; sd = stats[rows + row]; }
+    for (int i = threadIdx.x; i < span; i += kBoxThreads) {
+        const int t = t0 + i;
+        float v = (t < cols) ? __ldg(x + t) : 0.0f;
+        if (stats) v = norm_sample(v, m, sd);
+        tile[i] = v;
+    }
+    __syncthreads();
+    const float thr = d_thr ? __ldg(d_thr) : thr_host;
+    const int lane = threadIdx.x & 31;
+#pragma unroll 1
+    for (int k = 0; k < kBoxTile / kBoxThreads; ++k) {
+        const int i = threadIdx.x + k * kBoxThreads;
+        const int t = t0 + i;
+        float sum = 0.0f;
+        int next = 1, pw = 0;
+#pragma unroll 1
+        for (int w = 1; w <= wmax; ++w) {
+            const bool inside = (t + w - 1) < cols;
+            if (inside) sum = __fadd_rn(sum, tile[i + w - 1]);
+            bool test;
+            int code;
+            if (MODE == 0) {
+                test = (w == next);
+                code = pw;
+                if (test) { next <<= 1; ++pw; }
+                if (!test) continue;  // warp-uniform: w and next are the same in every lane
+            } else {
+                test = true;
+                code = w;
+            }
+            const float rw = __fsqrt_rn(static_cast<float>(w));
+            const float snr = snr_fast ? __fdividef(sum, rw) : __fdiv_rn(sum, rw);
+            const bool pass = inside && test && (snr > thr);
+            const unsigned ballot = __ballot_sync(0xffffffffu, pass);
+            if (ballot) {
+                const int leader = __ffs(ballot) - 1;
+                unsigned base = 0;
+                if (lane == leader) base = atomicAdd(d_count, static_cast<unsigned>(__popc(ballot)));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (pass) {
+                    const unsigned idx = base + __popc(ballot & ((1u << lane) - 1u));
+                    if (idx < capacity) {
+                        bfs_cand c;
+                        c.mt = t; c.mdt = row; c.mwidth = code; c.msnr = snr;
+                        out[idx] = c;
+                    }
+                }
+            }
+        }
+    }
+}
+
+__global__ void k_cand_keys(const bfs_cand* __restrict__ c, unsigned n, int cols, int mode,
+                            unsigned long long* __restrict__ keys, unsigned* __restrict__ vals) {
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bfs_cand v = c[i];
+    const unsigned long long wcode =
+        static_cast<unsigned long long>(mode == 0 ? v.mwidth : v.mwidth - 1);
+    keys[i] = ((static_cast<unsigned long long>(v.mdt) * cols + v.mt) << kWidthBits) | wcode;
+    vals[i] = i;
+}
+
+__global__ void k_gather_cands(const bfs_cand* __restrict__ src, const unsigned* __restrict__ idx,
+                               unsigned n, bfs_cand* __restrict__ dst) {
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[idx[i]];
+}
+
+int bits_for(unsigned long long v) {
+    int b = 0;
+    while (b < 64 && (v >> b) != 0ull) ++b;
+    return b;
+}
+
+}  // namespace
+
+// Sorts n candidates of a rows x cols plane into the canonical order in place.
+// Scratch comes from the stream-ordered pool allocator.
+bfs_status sort_candidates_canonical(bfs_cand* d_c, unsigned n, int rows, int cols, int mode,
+                                     cudaStream_t s) {
+    if (n < 2) return BFS_OK;
+    unsigned long long *k_in = nullptr, *k_out = nullptr;
+    unsigned *v_in = nullptr, *v_out = nullptr;
+    bfs_cand* tmp = nullptr;
+    void* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+    const int end_bit =
+        bits_for((static_cast<unsigned long long>(rows) * cols) << kWidthBits);
+    BFS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, k_in, k_out, v_in, v_out,
+                                             static_cast<int>(n), 0, end_bit, s));
+    BFS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&k_in), n * sizeof(unsigned long long) * 2, s));
+    k_out = k_in + n;
+    BFS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&v_in), n * sizeof(unsigned) * 2, s));
+    v_out = v_in + n;
+    BFS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&tmp), n * sizeof(bfs_cand), s));
+    BFS_CUDA(cudaMallocAsync(&cub_tmp, cub_bytes ? cub_bytes : 16, s));
+    const int th = 256, bl = static_cast<int>((n + th - 1) / th);
+    k_cand_keys<<<bl, th, 0, s>>>(d_c, n, cols, mode, k_in, v_in);
+    BFS_LAUNCH_CHECK("k_cand_keys");
+    BFS_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp, cub_bytes, k_in, k_out, v_in, v_out,
+                                             static_cast<int>(n), 0, end_bit, s));
+    k_gather_cands<<<bl, th, 0, s>>>(d_c, v_out, n, tmp);
+    BFS_LAUNCH_CHECK("k_gather_cands");
+    BFS_CUDA(cudaMemcpyAsync(d_c, tmp, n * sizeof(bfs_cand), cudaMemcpyDeviceToDevice, s));
+    BFS_CUDA(cudaFreeAsync(k_in, s));
+    BFS_CUDA(cudaFreeAsync(v_in, s));
+    BFS_CUDA(cudaFreeAsync(tmp, s));
+    BFS_CUDA(cudaFreeAsync(cub_tmp, s));
+    return BFS_OK;
+}
+
+bfs_status launch_row_stats(const float* d_in, int rows, int cols, float* d_stats, int mode,
+                            cudaStream_t s) {
+    BFS_ARG(d_in && d_stats, "null argument");
+    BFS_ARG(rows >= 1 && cols >= 1, "bad shape %dx%d", rows, cols);
+    BFS_ARG(rows <= 65535, "rows > 65535 not supported");
+    dim3 grid(kStatCluster, rows);
+    k_row_stats<<<grid, kStatThreads, 0, s>>>(d_in, rows, cols, d_stats, mode);
+    BFS_LAUNCH_CHECK("k_row_stats");
+    return BFS_OK;
+}
+
+bfs_status launch_boxcar(const float* d_plane, int rows, int cols, const float* d_stats,
+                         float thr, const float* d_thr, int mode, int param, int snr_fast,
+                         bfs_cand* d_out, unsigned capacity, unsigned* d_count, cudaStream_t s) {
+    BFS_ARG(d_plane && d_count, "null argument");
+    BFS_ARG(rows >= 1 && cols >= 1 && rows <= 65535, "bad shape %dx%d", rows, cols);
+    BFS_ARG(capacity == 0 || d_out, "d_out is null");
+    int wmax;
+    if (mode == BFS_WIDTHS_POW2) {
+        BFS_ARG(param >= 0 && param <= kMaxPow2Q, "Q must be in [0, %d]", kMaxPow2Q);
+        wmax = 1 << param;
+    } else if (mode == BFS_WIDTHS_ALL) {
+        BFS_ARG(param >= 1 && param <= kMaxAllW, "W must be in [1, %d]", kMaxAllW);
+        wmax = param;
+    } else {
+        return fail(BFS_ERR_ARG, "unknown widths_mode %d", mode);
+    }
+    dim3 grid((cols + kBoxTile - 1) / kBoxTile, rows);
+    const size_t smem = sizeof(float) * (kBoxTile + wmax - 1);
+    if (mode == BFS_WIDTHS_POW2) {
+        if (smem > 48 * 1024)
+            BFS_CUDA(cudaFuncSetAttribute(k_boxcar<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(smem)));
+        k_boxcar<0><<<grid, kBoxThreads, smem, s>>>(d_plane, rows, cols, d_stats, d_thr, thr, wmax,
+                                                    snr_fast, d_out, capacity, d_count);
+    } else {
+        if (smem > 48 * 1024)
+            BFS_CUDA(cudaFuncSetAttribute(k_boxcar<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(smem)));
+        k_boxcar<1><<<grid, kBoxThreads, smem, s>>>(d_plane, rows, cols, d_stats, d_thr, thr, wmax,
+                                                    snr_fast, d_out, capacity, d_count);
+    }
+    BFS_LAUNCH_CHECK("k_boxcar");
+    return BFS_OK;
+}
+
+}  // namespace bfs
+
+using namespace bfs;
+
+extern "C" bfs_status bfs_row_stats(const float* d_in, int rows, int cols, float* d_stats,
+                                    void* stream) {
+    return launch_row_stats(d_in, rows, cols, d_stats, 0, as_stream(stream));
+}
+
+extern "C" bfs_status bfs_norm_rows(const float* d_in, float* d_out, int rows, int cols,
+                                    float* d_stats, void* stream) {
+    BFS_ARG(d_in && d_out, "null argument");
+    cudaStream_t s = as_stream(stream);
+    float* stats = d_stats;
+    if (!stats) BFS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&stats), sizeof(float) * 2 * rows, s));
+    bfs_status st = launch_row_stats(d_in, rows, cols, stats, 0, s);
+    if (st == BFS_OK) {
+        dim3 grid(std::min((cols + 255) / 256, 64), rows);
+        k_norm_rows<<<grid, 256, 0, s>>>(d_in, d_out, rows, cols, stats);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) st = fail(BFS_ERR_CUDA, "k_norm_rows: %s", cudaGetErrorString(e));
+    }
+    if (!d_stats) cudaFreeAsync(stats, s);
+    return st;
+}
+
+extern "C" bfs_status bfs_boxcar_gather(const float* d_plane, int rows, int cols,
+                                        const float* d_stats, float thr, const float* d_thr,
+                                        int widths_mode, int param, int snr_fast, bfs_cand* d_out,
+                                        uint32_t capacity, uint32_t* h_count, void* stream) {
+    BFS_ARG(h_count != nullptr, "h_count is null");
+    cudaStream_t s = as_stream(stream);
+    unsigned* d_count = nullptr;
+    BFS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_count), sizeof(unsigned), s));
+    BFS_CUDA(cudaMemsetAsync(d_count, 0, sizeof(unsigned), s));
+    bfs_status st = launch_boxcar(d_plane, rows, cols, d_stats, thr, d_thr, widths_mode, param,
+                                  snr_fast, d_out, capacity, d_count, s);
+    unsigned count = 0;
+    if (st == BFS_OK) {
+        cudaError_t e = cudaMemcpyAsync(&count, d_count, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = fail(BFS_ERR_CUDA, "reading the candidate count: %s",
+                                        cudaGetErrorString(e));
+    }
+    cudaFreeAsync(d_count, s);
+    if (st != BFS_OK) return st;
+    *h_count = count;
+    const unsigned n = count < capacity ? count : capacity;
+    st = sort_candidates_canonical(d_out, n, rows, cols, widths_mode, s);
+    if (st != BFS_OK) return st;
+    if (count > capacity)
+        return fail(BFS_ERR_OVERFLOW, "%u candidates found, capacity %u", count, capacity);
+    return BFS_OK;
+}

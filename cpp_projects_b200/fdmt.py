@@ -21,7 +21,7 @@ from ._tensors import dev_ptr, stream_handle
 
 class CFdmtGpu:
     def __init__(self, Fmin: float, Fmax: float, nchan: int, cols: int, imaxDt: int,
-                 fuse_depth: int = -1):
+                 fuse_depth: int = -1, external_ws: bool = False):
         self.m_Fmin = float(Fmin)
         self.m_Fmax = float(Fmax)
         self.m_nchan = int(nchan)
@@ -29,7 +29,8 @@ class CFdmtGpu:
         self.m_imaxDt = int(imaxDt)
         desc = _capi.FdmtDesc(fmin=self.m_Fmin, fmax=self.m_Fmax, nchan=self.m_nchan,
                               ncols=self.m_cols, max_dt=self.m_imaxDt, plan_kind=0,
-                              precision=0, fuse_depth=int(fuse_depth))
+                              precision=0, fuse_depth=int(fuse_depth),
+                              flags=_capi.BFS_FDMT_EXTERNAL_WS if external_ws else 0)
         self._plan = ctypes.c_void_p()
         _capi.call("bfs_fdmt_plan_create", ctypes.byref(desc), ctypes.byref(self._plan))
         info = _capi.FdmtInfo()
@@ -58,6 +59,21 @@ class CFdmtGpu:
             pin = dev_ptr(d_in, torch.float32, "d_in")
         _capi.call("bfs_fdmt_execute", self._plan, pin, dev_ptr(d_out, torch.float32, "d_out"),
                    1 if b_ones else 0, stream_handle(stream))
+
+    def workspace_size(self) -> int:
+        n = ctypes.c_size_t(0)
+        _capi.call("bfs_fdmt_workspace_size", self._plan, ctypes.byref(n))
+        return int(n.value)
+
+    def process_image_ws(self, d_in: torch.Tensor | None, d_out: torch.Tensor, b_ones: bool,
+                         workspace: torch.Tensor, stream: torch.cuda.Stream | None = None) -> None:
+        """process_image with caller-provided scratch (a uint8 CUDA tensor of at
+        least workspace_size() bytes, 256-byte aligned)."""
+        pin = None if b_ones else dev_ptr(d_in, torch.float32, "d_in")
+        _capi.call("bfs_fdmt_execute_ws", self._plan, pin, dev_ptr(d_out, torch.float32, "d_out"),
+                   1 if b_ones else 0, dev_ptr(workspace, None, "workspace"),
+                   ctypes.c_size_t(workspace.numel() * workspace.element_size()),
+                   stream_handle(stream))
 
     # --- plan introspection ------------------------------------------------
     def rows_per_level(self) -> np.ndarray:

@@ -54,6 +54,7 @@ const char* bfs_version(void);
  * ---------------------------------------------------------------------- */
 enum { BFS_PLAN_KEITH = 0 };
 enum { BFS_PREC_F32 = 0 };
+enum { BFS_FDMT_EXTERNAL_WS = 1 };
 
 typedef struct bfs_fdmt_desc {
     float fmin;        /* MHz, lower band edge                          */
@@ -64,7 +65,8 @@ typedef struct bfs_fdmt_desc {
     int plan_kind;     /* BFS_PLAN_KEITH                                */
     int precision;     /* BFS_PREC_F32                                  */
     int fuse_depth;    /* -1 = autotuned; 0 = level-by-level; k = fuse levels 0..k in one kernel */
-    int reserved[8];
+    int flags;         /* BFS_FDMT_EXTERNAL_WS: the plan allocates no planes; use _execute_ws */
+    int reserved[7];
 } bfs_fdmt_desc;
 
 typedef struct bfs_fdmt_plan bfs_fdmt_plan;
@@ -88,10 +90,23 @@ bfs_status bfs_fdmt_plan_rows(const bfs_fdmt_plan* plan, int* rows_per_level, in
 /* Host copies of level `level`'s (>= 1) row tables: tail row, head row (-1 = copied row), head shift. */
 bfs_status bfs_fdmt_plan_tables(const bfs_fdmt_plan* plan, int level, int* a_row, int* b_row,
                                 int* shift, int cap);
+/* Fused-head layout (no reference counterpart; introspection for tests and
+ * tuning): params[0..8] = depth, channels per group, tile, threads per CTA,
+ * shared rows A, shared rows B, shared bytes, groups, table rows.  groups
+ * (optional) receives per group {halo, out_row0, rows[9], tab_off[9]}; tab
+ * (optional) receives 4 ints per row {tail, head, shift, 0} local to a group. */
+bfs_status bfs_fdmt_plan_head(const bfs_fdmt_plan* plan, int* params, int* groups, int group_cap,
+                              int* tab, int tab_cap);
 /* d_in: nchan*ncols floats (ignored when b_ones != 0: an all-ones image is used,
  * the reference's normalisation mode), d_out: max_dt*ncols floats. */
 bfs_status bfs_fdmt_execute(bfs_fdmt_plan* plan, const float* d_in, float* d_out, int b_ones,
                             void* stream);
+/* Bytes of device scratch one call needs (the two ping-pong planes). */
+bfs_status bfs_fdmt_workspace_size(const bfs_fdmt_plan* plan, size_t* bytes);
+/* As bfs_fdmt_execute, with caller-provided scratch (>= workspace_size bytes,
+ * 256-byte aligned).  Several plans may share one workspace on one stream. */
+bfs_status bfs_fdmt_execute_ws(bfs_fdmt_plan* plan, const float* d_in, float* d_out, int b_ones,
+                               void* d_workspace, size_t workspace_bytes, void* stream);
 
 /* ------------------------------------------------------------------------
  * Statistical preprocessing of the FDMT input.

@@ -36,9 +36,11 @@ int orc_fdmt_run_f32(float fmin, float fmax, int nchan, int cols, int max_dt,
 int orc_fdmt_run_f64(float fmin, float fmax, int nchan, int cols, int max_dt,
                      const double* in, double* out, int b_ones);
 
-/* --- search (reference: MyVSLib_C++/Clusterization/*.cu) ---------------- */
+/* --- search (reference: MyVSLib_C++/Clusterization/ sources) --------------- */
 int64_t orc_boxcar(const float* plane, int rows, int cols, float thr, int mode,
                    int param, orc_cand* out, int64_t cap);
+int64_t orc_boxcar_mt(const float* plane, int rows, int cols, float thr, int mode,
+                      int param, orc_cand* out, int64_t cap);
 void orc_norm_rows(const float* in, float* out, int rows, int cols,
                    float* mean_out, float* std_out);
 int orc_select_delegates(const orc_cand* c, const int* perm, const int* offsets,

@@ -39,6 +39,8 @@ def lib() -> ctypes.CDLL:
         _lib.orc_boxcar.restype = ctypes.c_int64
         _lib.orc_boxcar.argtypes = [_P, ctypes.c_int, ctypes.c_int, _F, ctypes.c_int,
                                     ctypes.c_int, _P, ctypes.c_int64]
+        _lib.orc_boxcar_mt.restype = ctypes.c_int64
+        _lib.orc_boxcar_mt.argtypes = _lib.orc_boxcar.argtypes
         for n in ("orc_fdmt_rows", "orc_fdmt_tables", "orc_fdmt_run_f32", "orc_fdmt_run_f64"):
             getattr(_lib, n).restype = ctypes.c_int
     return _lib
@@ -114,6 +116,16 @@ def boxcar(plane: np.ndarray, thr: float, mode: int, param: int, cap: int = 1 <<
     rows, cols = plane.shape
     out = np.zeros(cap, CAND_DTYPE)
     n = lib().orc_boxcar(_ptr(plane), rows, cols, _F(thr), mode, param, _ptr(out), cap)
+    if n > cap:
+        raise ValueError(f"oracle boxcar capacity {cap} exceeded ({n})")
+    return out[:n].copy()
+
+
+def boxcar_mt(plane: np.ndarray, thr: float, mode: int, param: int, cap: int = 1 << 22):
+    plane = np.ascontiguousarray(plane, np.float32)
+    rows, cols = plane.shape
+    out = np.zeros(cap, CAND_DTYPE)
+    n = lib().orc_boxcar_mt(_ptr(plane), rows, cols, _F(thr), mode, param, _ptr(out), cap)
     if n > cap:
         raise ValueError(f"oracle boxcar capacity {cap} exceeded ({n})")
     return out[:n].copy()

@@ -62,6 +62,28 @@ int64_t orc_boxcar(const float* plane, int rows, int cols, float thr, int mode,
     return n;
 }
 
+/* Same result as orc_boxcar (row-major order), rows split across OpenMP
+ * threads; used to time the CPU baseline on many cores. */
+int64_t orc_boxcar_mt(const float* plane, int rows, int cols, float thr, int mode,
+                      int param, orc_cand* out, int64_t cap) {
+    int64_t* cnt = (int64_t*)calloc((size_t)rows + 1, sizeof(int64_t));
+    #pragma omp parallel for schedule(dynamic, 4)
+    for (int r = 0; r < rows; ++r)
+        cnt[r + 1] = orc_boxcar(plane + (size_t)r * cols, 1, cols, thr, mode, param, NULL, 0);
+    for (int r = 0; r < rows; ++r) cnt[r + 1] += cnt[r];
+    int64_t total = cnt[rows];
+    if (total <= cap) {
+        #pragma omp parallel for schedule(dynamic, 4)
+        for (int r = 0; r < rows; ++r) {
+            orc_cand* o = out + cnt[r];
+            int64_t n = orc_boxcar(plane + (size_t)r * cols, 1, cols, thr, mode, param, o, cnt[r + 1] - cnt[r]);
+            for (int64_t i = 0; i < n; ++i) o[i].mdt = r;
+        }
+    }
+    free(cnt);
+    return total;
+}
+
 void orc_norm_rows(const float* in, float* out, int rows, int cols, float* mean_out, float* std_out) {
     for (int r = 0; r < rows; ++r) {
         const float* x = in + (size_t)r * cols;
@@ -100,24 +122,30 @@ static int cmp_pass(const void* pa, const void* pb) {
 
 int orc_select_delegates(const orc_cand* c, const int* perm, const int* offsets,
                          int ngroups, int block, int* delegates) {
+    float* v = (float*)malloc(sizeof(float) * (size_t)block);
+    int* id = (int*)malloc(sizeof(int) * (size_t)block);
     for (int g = 0; g < ngroups; ++g) {
         int beg = offsets[g], len = offsets[g + 1] - offsets[g];
-        float best = -FLT_MAX;
-        int best_idx = -1;
         for (int lane = 0; lane < block; ++lane) {
-            float v = -FLT_MAX;
-            int idx = lane;  /* reference sets the lane id for idle lanes */
+            v[lane] = -FLT_MAX;
+            id[lane] = lane;  /* the reference stores the lane id for idle lanes */
             if (lane < len) {
-                idx = -1;
+                id[lane] = -1;
                 for (int i = lane; i < len; i += block) {
                     int k = perm[beg + i];
-                    if (c[k].msnr > v) { v = c[k].msnr; idx = k; }
+                    if (c[k].msnr > v[lane]) { v[lane] = c[k].msnr; id[lane] = k; }
                 }
             }
-            if (lane == 0 || v > best) { best = v; best_idx = idx; }
         }
-        delegates[g] = best_idx;
+        /* the reference's tree reduction: lane l takes lane l+s only if strictly
+         * greater; on ties the winner follows the tree, not the lowest lane */
+        for (int s = block / 2; s > 0; s >>= 1)
+            for (int lane = 0; lane < s; ++lane)
+                if (v[lane + s] > v[lane]) { v[lane] = v[lane + s]; id[lane] = id[lane + s]; }
+        delegates[g] = id[0];
     }
+    free(v);
+    free(id);
     return ngroups;
 }
 
@@ -184,9 +212,13 @@ void orc_calc_fdmt_inputs(float* x, int rows, int cols, float* norm_input, float
         double m = s / cols, d = q / cols - m * m;
         rmean[r] = (float)m;
         rdisp[r] = (float)d;
-        sm += m; s2 += d + m * m;
     }
-    for (int r = 0; r < rows; ++r) { dsum += rdisp[r]; dsq += (double)rdisp[r] * rdisp[r]; }
+    /* global moments from the stored float row values, as the reference does */
+    for (int r = 0; r < rows; ++r) {
+        double m = rmean[r], d = rdisp[r];
+        sm += m; s2 += d + m * m;
+        dsum += d; dsq += d * d;
+    }
     double mean = sm / rows, var = s2 / rows - mean * mean;
     double dmean = dsum / rows, dvar = dsq / rows - dmean * dmean;
     float mf = (float)mean, sf = (float)sqrt(var > 0 ? var : 0);
