@@ -64,6 +64,9 @@ _SIGNATURES = {
     "bfs_fdmt_execute": (_I, [_P, _P, _P, _I, _P]),
     "bfs_fdmt_workspace_size": (_I, [_P, ctypes.POINTER(ctypes.c_size_t)]),
     "bfs_fdmt_execute_ws": (_I, [_P, _P, _P, _I, _P, ctypes.c_size_t, _P]),
+    "bfs_fdmt_execute_noalloc": (_I, [_P, _P, _P, _I, _P]),
+    "bfs_fdmt_noalloc_scratch_bytes": (_I, [_P, ctypes.POINTER(ctypes.c_size_t),
+                                            ctypes.POINTER(ctypes.c_size_t)]),
     "bfs_preproc_calc_fdmt_inputs": (_I, [_P, _I, _I, _P, _P, _P]),
     "bfs_fdmt_normalize": (_I, [_P, _P, _I64, _P, _P]),
     "bfs_norm_rows": (_I, [_P, _P, _I, _I, _P, _P]),

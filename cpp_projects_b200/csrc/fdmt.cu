@@ -413,3 +413,185 @@ extern "C" bfs_status bfs_fdmt_execute_ws(bfs_fdmt_plan* plan, const float* d_in
     return fdmt_run(plan, d_in, d_out, b_ones, reinterpret_cast<float*>(w),
                     reinterpret_cast<float*>(w + plane_bytes(plan, 0)), as_stream(stream));
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free FDMT.
+//
+// Some callers cannot allocate device memory when they need the transform: a
+// real-time receiver that reserves all of its GPU memory at start-up and may
+// not risk an allocation failure (or an allocator stall) mid-observation, a
+// host framework that owns the device allocator and forbids side
+// allocations, or a plain C caller linked against this library without its
+// own CUDA allocation code.  bfs_fdmt_execute_noalloc serves them.  It takes
+// a host-only plan (bfs_fdmt_plan_create_host: host memory only) and runs the
+// same kernels as bfs_fdmt_execute, with every piece of scratch — the row
+// tables and the two ping-pong planes — carved out of g_fdmt_static_scratch,
+// a file-scope device array of kNoAllocScratchBytes (256 MiB) that every GPU
+// which loads this library holds until the process exits.
+//
+// In host code the array's name is only a host-side stand-in, not a device
+// address, so the device address is looked up with cudaGetSymbolAddress once
+// per device (with that device current) on the first call made on it; that
+// first call should therefore come before any stream capture.  All calls
+// share the one array and it keeps the previous call's contents: every byte a
+// call reads is written by that call first (tables copied in, planes fully
+// overwritten), so nothing needs clearing, but calls whose executions
+// overlap on the GPU (other streams, other host threads) race on it.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace bfs {
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = static_cast<size_t>(256) << 20;
+constexpr int kNoAllocMaxDevices = 64;
+
+__device__ __align__(256) unsigned char g_fdmt_static_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+bfs_status noalloc_scratch(void** out) {
+    int dev = -1;
+    BFS_CUDA(cudaGetDevice(&dev));
+    BFS_ARG(dev >= 0 && dev < kNoAllocMaxDevices, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (g_noalloc_ptr[dev] == nullptr) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_fdmt_static_scratch);
+        if (e != cudaSuccess || p == nullptr)
+            return fail(BFS_ERR_CUDA, "cudaGetSymbolAddress(static FDMT scratch) on device %d: %s",
+                        dev, cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return BFS_OK;
+}
+
+size_t align256(size_t v) { return (v + 255) & ~static_cast<size_t>(255); }
+
+// Packs the three per-row int arrays staged in the scratch into int4 rows.
+__global__ void k_pack_rows(const int* __restrict__ a, const int* __restrict__ b,
+                            const int* __restrict__ s, int n, int4* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = make_int4(a[i], b[i], s[i], 0);
+}
+
+}  // namespace
+}  // namespace bfs
+
+extern "C" bfs_status bfs_fdmt_noalloc_scratch_bytes(const bfs_fdmt_plan* plan, size_t* need,
+                                                     size_t* capacity) {
+    BFS_ARG(plan != nullptr, "null argument");
+    const FdmtPlanHost& h = plan->host;
+    const int k = plan->head.depth;
+    size_t rows = 0, prow[2] = {0, 0};
+    for (int l = k + 1; l <= h.niter; ++l) rows += static_cast<size_t>(h.lv[l].total_rows());
+    for (int l = k; l < h.niter; ++l)
+        prow[l & 1] = std::max(prow[l & 1], static_cast<size_t>(h.lv[l].total_rows()));
+    size_t total = align256(rows * sizeof(int4)) + align256(rows * 3 * sizeof(int));
+    if (k > 0)
+        total += align256(plan->head.groups.size() * sizeof(HeadGroup)) +
+                 align256(plan->head.tab.size() * sizeof(int));
+    total += align256(prow[0] * h.ncols * sizeof(float)) + align256(prow[1] * h.ncols * sizeof(float));
+    if (need) *need = total;
+    if (capacity) *capacity = kNoAllocScratchBytes;
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_fdmt_execute_noalloc(const bfs_fdmt_plan* plan, const float* d_in,
+                                               float* d_out, int b_ones, void* stream) {
+    BFS_ARG(plan != nullptr && d_out != nullptr, "null argument");
+    BFS_ARG(b_ones || d_in != nullptr, "d_in is null");
+    size_t need = 0;
+    bfs_status st = bfs_fdmt_noalloc_scratch_bytes(plan, &need, nullptr);
+    if (st != BFS_OK) return st;
+    BFS_ARG(need <= kNoAllocScratchBytes,
+            "this FDMT needs %zu bytes of scratch; the allocation-free entry point has a fixed "
+            "%zu-byte (256 MiB) static scratch: use bfs_fdmt_execute or bfs_fdmt_execute_ws",
+            need, kNoAllocScratchBytes);
+    void* base = nullptr;
+    st = noalloc_scratch(&base);
+    if (st != BFS_OK) return st;
+    cudaStream_t s = as_stream(stream);
+    const FdmtPlanHost& h = plan->host;
+    const HeadPlan& hp = plan->head;
+    const int k = hp.depth;
+    const int T = h.ncols;
+
+    // carve the scratch: packed tables | staged int tables | head groups | head table | planes
+    char* p = static_cast<char*>(base);
+    size_t rows = 0, prow[2] = {0, 0};
+    for (int l = k + 1; l <= h.niter; ++l) rows += static_cast<size_t>(h.lv[l].total_rows());
+    for (int l = k; l < h.niter; ++l)
+        prow[l & 1] = std::max(prow[l & 1], static_cast<size_t>(h.lv[l].total_rows()));
+    int4* tab = reinterpret_cast<int4*>(p);
+    p += align256(rows * sizeof(int4));
+    int* staged = reinterpret_cast<int*>(p);
+    p += align256(rows * 3 * sizeof(int));
+    HeadGroup* groups = nullptr;
+    int* head_tab = nullptr;
+    if (k > 0) {
+        groups = reinterpret_cast<HeadGroup*>(p);
+        p += align256(hp.groups.size() * sizeof(HeadGroup));
+        head_tab = reinterpret_cast<int*>(p);
+        p += align256(hp.tab.size() * sizeof(int));
+    }
+    float* bufs[2];
+    bufs[0] = reinterpret_cast<float*>(p);
+    p += align256(prow[0] * T * sizeof(float));
+    bufs[1] = reinterpret_cast<float*>(p);
+
+    // tables: host vectors -> staged ints -> packed int4 rows
+    size_t off[64] = {};  // per level; niter <= 31 for any int channel count
+    BFS_ARG(h.niter < 64, "too many levels");
+    size_t pos = 0;
+    for (int l = k + 1; l <= h.niter; ++l) {
+        const FdmtLevel& L = h.lv[l];
+        const size_t n = static_cast<size_t>(L.total_rows());
+        off[l] = pos;
+        BFS_CUDA(cudaMemcpyAsync(staged + pos, L.a_row.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
+        BFS_CUDA(cudaMemcpyAsync(staged + rows + pos, L.b_row.data(), n * sizeof(int),
+                                 cudaMemcpyHostToDevice, s));
+        BFS_CUDA(cudaMemcpyAsync(staged + 2 * rows + pos, L.shift.data(), n * sizeof(int),
+                                 cudaMemcpyHostToDevice, s));
+        pos += n;
+    }
+    if (rows > 0) {
+        const int n = static_cast<int>(rows);
+        k_pack_rows<<<(n + 255) / 256, 256, 0, s>>>(staged, staged + rows, staged + 2 * rows, n, tab);
+        BFS_LAUNCH_CHECK("k_pack_rows");
+    }
+    if (k > 0) {
+        BFS_CUDA(cudaMemcpyAsync(groups, hp.groups.data(), hp.groups.size() * sizeof(HeadGroup),
+                                 cudaMemcpyHostToDevice, s));
+        BFS_CUDA(cudaMemcpyAsync(head_tab, hp.tab.data(), hp.tab.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice, s));
+        if (hp.smem_bytes > 48 * 1024)
+            BFS_CUDA(cudaFuncSetAttribute(k_fdmt_head, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(hp.smem_bytes)));
+        dim3 grid((T + hp.tile - 1) / hp.tile, h.nchan / hp.group);
+        BFS_ARG(grid.y <= 65535, "nchan too large for this build");
+        float* dst = (k == h.niter) ? d_out : bufs[k & 1];
+        k_fdmt_head<<<grid, hp.width, hp.smem_bytes, s>>>(
+            d_in, dst, groups, reinterpret_cast<const int4*>(head_tab), T, k, hp.group,
+            h.rows_per_chan0, hp.tile, hp.rows_a, b_ones ? 1 : 0);
+        BFS_LAUNCH_CHECK("k_fdmt_head");
+    } else {
+        dim3 grid((T + kInitThreads * kInitCols - 1) / (kInitThreads * kInitCols), h.nchan);
+        BFS_ARG(grid.y <= 65535, "nchan too large for this build");
+        k_fdmt_init<<<grid, kInitThreads, 0, s>>>(d_in, bufs[0], T, h.rows_per_chan0,
+                                                  b_ones ? 1 : 0);
+        BFS_LAUNCH_CHECK("k_fdmt_init");
+    }
+    const int chunk = kLevelThreads * kLevelCols;
+    for (int l = k + 1; l <= h.niter; ++l) {
+        const float* src = bufs[(l - 1) & 1];
+        float* dst = (l == h.niter) ? d_out : bufs[l & 1];
+        dim3 grid(h.lv[l].total_rows(), (T + chunk - 1) / chunk);
+        BFS_ARG(grid.y <= 65535, "ncols too large for this build");
+        k_fdmt_level<<<grid, kLevelThreads, 0, s>>>(src, dst, tab + off[l], T);
+        BFS_LAUNCH_CHECK("k_fdmt_level");
+    }
+    return BFS_OK;
+}

@@ -108,6 +108,24 @@ bfs_status bfs_fdmt_workspace_size(const bfs_fdmt_plan* plan, size_t* bytes);
 bfs_status bfs_fdmt_execute_ws(bfs_fdmt_plan* plan, const float* d_in, float* d_out, int b_ones,
                                void* d_workspace, size_t workspace_bytes, void* stream);
 
+/* Allocation-free FDMT.  No counterpart in the reference: it exists for
+ * callers that cannot allocate device memory where they run the transform
+ * (a real-time receiver whose GPU memory is all reserved at start-up, a
+ * framework that owns the device allocator, a C caller with no CUDA
+ * allocation code of its own).  `plan` may be host-only
+ * (bfs_fdmt_plan_create_host).  The call allocates nothing: the row tables
+ * and both ping-pong planes live in one 256 MiB static device array built
+ * into the library (held by every GPU that loads it, until exit); a problem
+ * needing more returns BFS_ERR_ARG.  The first call on each device looks the
+ * array's device address up (cudaGetSymbolAddress), so make it before any
+ * stream capture.  Calls share the array: calls that overlap on the GPU
+ * race.  Same output as bfs_fdmt_execute. */
+bfs_status bfs_fdmt_execute_noalloc(const bfs_fdmt_plan* plan, const float* d_in, float* d_out,
+                                    int b_ones, void* stream);
+/* Scratch bytes bfs_fdmt_execute_noalloc needs for `plan`, and the static capacity. */
+bfs_status bfs_fdmt_noalloc_scratch_bytes(const bfs_fdmt_plan* plan, size_t* need,
+                                          size_t* capacity);
+
 /* ------------------------------------------------------------------------
  * Statistical preprocessing of the FDMT input.
  * Replaces statistical_preprocessing::calc_fdmt_inputs
