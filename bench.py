@@ -11,7 +11,8 @@ data generated on the device.  A step is one pass of the whole path over all
 48 beams: FDMT -> per-row statistics -> fused normalise + boxcar (widths
 1..32, S/N > 7) + compaction -> 3-pass clustering (+-16 samples, +-8 rows,
 any width) -> delegates copied to the host.  ``config0`` is the single
-512 x 32768 beam of the reference's CPU-runnable case.
+512 x 32768 beam of the reference's CPU-runnable case; ``config4fwd`` one
+1024 x 65536 beam (used for profiling: its input exceeds L2).
 
 Metric: channel*samples per second over the whole job (all ranks).
 ``value`` is device-timed with inputs already in HBM (the working set of
@@ -50,7 +51,7 @@ def parse_args(argv=None):
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["config2", "config0"], default="config2")
+    ap.add_argument("--workload", choices=["config2", "config0", "config4fwd"], default="config2")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args(argv)
@@ -68,6 +69,8 @@ def beams_for(workload: str, rank: int):
     from cpp_projects_b200 import synth
     if workload == "config0":
         return [synth.config0(seed=1 + rank)]
+    if workload == "config4fwd":
+        return [synth.config4(seed=4 + rank)]
     return synth.config2(seed=2 + 1000 * rank)
 
 
@@ -207,8 +210,10 @@ def run_ours(args):
 
     beams = beams_for(args.workload, rank)
     shapes = [BeamShape(b.nchan, b.nsamp, b.fmin, b.fmax, b.max_dt) for b in beams]
+    capacity = (1 << 26) if args.workload == "config2" else (1 << 24)
     pipe = SearchPipeline(shapes, widths_mode=SEARCH["widths_mode"], param=SEARCH["param"],
-                          thr=SEARCH["thr"], metrics=SEARCH["metrics"], device=dev)
+                          thr=SEARCH["thr"], metrics=SEARCH["metrics"], capacity=capacity,
+                          device=dev)
     inputs = [device_filterbank(b.nchan, b.nsamp, b.fmin, b.fmax, b.seed, b.pulses, dev)
               for b in beams]
     torch.cuda.synchronize()

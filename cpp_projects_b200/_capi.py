@@ -54,6 +54,7 @@ _F = ctypes.c_float
 _SIGNATURES = {
     "bfs_last_error": (ctypes.c_char_p, []),
     "bfs_version": (ctypes.c_char_p, []),
+    "bfs_trim_scratch": (_I, []),
     "bfs_fdmt_plan_create": (_I, [ctypes.POINTER(FdmtDesc), ctypes.POINTER(_P)]),
     "bfs_fdmt_plan_create_host": (_I, [ctypes.POINTER(FdmtDesc), ctypes.POINTER(_P)]),
     "bfs_fdmt_plan_destroy": (_I, [_P]),

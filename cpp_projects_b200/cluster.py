@@ -11,7 +11,7 @@ import torch
 
 from . import _capi
 from ._tensors import dev_ptr, stream_handle
-from .search import cands_to_numpy, gather_candidates_in_heap_with_plan
+from .search import CAND_DTYPE, cands_to_numpy, gather_candidates_in_heap_with_plan
 
 
 class Clusters:
@@ -25,8 +25,10 @@ class Clusters:
         self.ngroups = ngroups
 
     def delegate_records(self) -> np.ndarray:
-        c = cands_to_numpy(self.cands)
-        return c[self.delegates.cpu().numpy()]
+        """Delegate Cand records (gathered on the device; only they cross PCIe)."""
+        if self.ngroups == 0:
+            return np.zeros(0, CAND_DTYPE)
+        return cands_to_numpy(self.cands.index_select(0, self.delegates.long()))
 
     def group_sizes(self) -> np.ndarray:
         o = self.offsets.cpu().numpy()
@@ -71,11 +73,11 @@ def write_log(cl: Clusters, filename: str, delt_bin: float, t_chunkBegin: float,
     columns N, t bin, t sec, dedisp, width, SNR, num, each setw(10).
     The reference pairs the i-th delegate (sorted by mt) with the i-th group's
     size in group order; that quirk is kept unless num_from_delegate_group."""
-    c = cands_to_numpy(cl.cands)
+    drec = cl.delegate_records()
     dl = cl.delegates.cpu().numpy()
     sizes = cl.group_sizes()
     if num_from_delegate_group:
-        gid = np.empty(len(c), np.int64)
+        gid = np.empty(int(cl.cands.shape[0]), np.int64)
         perm = cl.perm.cpu().numpy()
         offs = cl.offsets.cpu().numpy()
         for g in range(cl.ngroups):
@@ -84,7 +86,7 @@ def write_log(cl: Clusters, filename: str, delt_bin: float, t_chunkBegin: float,
         f.write("".join(s.rjust(10) for s in ("N", "t, bin", "t, sec", "dedisp", "width", "SNR",
                                                 "num")) + "\n")
         for i, j in enumerate(dl):
-            r = c[j]
+            r = drec[i]
             num = sizes[gid[j]] if num_from_delegate_group else sizes[i]
             t_sec = np.float32(t_chunkBegin) + np.float32(r["mt"]) * np.float32(delt_bin)
             cols = [str(i + 1), str(int(r["mt"])), _fmt_g(float(t_sec)), str(int(r["mdt"])),

@@ -12,7 +12,9 @@
 // Layout in HBM: every plane is row-major [row][ncols] float32, rows of a
 // level concatenated sub-band by sub-band in frequency order (the reference's
 // layout).  The plan owns two ping-pong planes sized for the largest even and
-// odd level; the last level is written straight into the caller's output.
+// odd level that reaches HBM, with rows padded to a 128-byte pitch so every
+// merge level moves float4s whatever ncols is; the last level is written
+// straight into the caller's output (pitch ncols).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -51,15 +53,14 @@ namespace {
 constexpr int kInitThreads = 256;
 constexpr int kInitCols = 4;        // columns per thread (strided by the block)
 constexpr int kLevelThreads = 256;
-constexpr int kLevelCols = 8;       // columns per thread (strided by the block)
 
 // Level 0.  grid: (ceil(ncols / (256*4)), nchan).
 __global__ void __launch_bounds__(kInitThreads)
-k_fdmt_init(const float* __restrict__ x, float* __restrict__ out, int ncols, int rows_per_chan,
-            int ones) {
+k_fdmt_init(const float* __restrict__ x, float* __restrict__ out, int ncols, int out_pitch,
+            int rows_per_chan, int ones) {
     const int c = blockIdx.y;
     const float* xr = x + static_cast<size_t>(c) * ncols;
-    float* o = out + static_cast<size_t>(c) * rows_per_chan * ncols;
+    float* o = out + static_cast<size_t>(c) * rows_per_chan * out_pitch;
     const int base = blockIdx.x * (kInitThreads * kInitCols) + threadIdx.x;
 #pragma unroll
     for (int k = 0; k < kInitCols; ++k) {
@@ -75,34 +76,65 @@ k_fdmt_init(const float* __restrict__ x, float* __restrict__ out, int ncols, int
                               static_cast<float>(r + 1));
                 w = v;
             }
-            o[static_cast<size_t>(r) * ncols + t] = w;
+            o[static_cast<size_t>(r) * out_pitch + t] = w;
         }
     }
 }
 
-// One merge level.  grid: (rows, ceil(ncols / (256*8))).
+// One merge level.  The input plane is always a workspace plane (128-byte
+// row pitch), so the tail row moves as float4; the shifted head row moves as
+// 4 scalar loads (its alignment depends on the row's shift); the output is
+// stored as float4 when its pitch and base allow (VOUT), else as scalars (the
+// caller's plane with an odd ncols).  Each thread owns kLevelVecs column
+// groups of 4 strided by the block.
+// grid: (rows, ceil(ncols / (256*4*kLevelVecs)))
+constexpr int kLevelVecs = 4;
+
+template <bool VOUT>
 __global__ void __launch_bounds__(kLevelThreads)
 k_fdmt_level(const float* __restrict__ in, float* __restrict__ out, const int4* __restrict__ tab,
-             int ncols) {
+             int ncols, int in_pitch, int out_pitch) {
     const int g = blockIdx.x;
     const int4 e = __ldg(tab + g);
-    const float* ra = in + static_cast<size_t>(e.x) * ncols;
-    const float* rb = in + static_cast<size_t>(e.y < 0 ? e.x : e.y) * ncols;
-    float* ro = out + static_cast<size_t>(g) * ncols;
+    const float4* ra = reinterpret_cast<const float4*>(in + static_cast<size_t>(e.x) * in_pitch);
+    const float* rb = in + static_cast<size_t>(e.y < 0 ? e.x : e.y) * in_pitch;
+    float* ro = out + static_cast<size_t>(g) * out_pitch;
     const int s = e.z;
     const bool has_b = e.y >= 0;
-    const int base = blockIdx.y * (kLevelThreads * kLevelCols) + threadIdx.x;
-    float va[kLevelCols], vb[kLevelCols];
+    const int nv = (ncols + 3) >> 2;
+    const int base = blockIdx.y * (kLevelThreads * kLevelVecs) + threadIdx.x;
+    float4 va[kLevelVecs];
+    float vb[kLevelVecs][4];
 #pragma unroll
-    for (int k = 0; k < kLevelCols; ++k) {
-        const int t = base + k * kLevelThreads;
-        va[k] = (t < ncols) ? __ldg(ra + t) : 0.0f;
-        vb[k] = (has_b && t < ncols && t >= s) ? __ldg(rb + t - s) : 0.0f;
+    for (int k = 0; k < kLevelVecs; ++k) {
+        const int q = base + k * kLevelThreads;
+        va[k] = (q < nv) ? __ldg(ra + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int t = 4 * q + i;
+            vb[k][i] = (has_b && t < ncols && t >= s) ? __ldg(rb + t - s) : 0.0f;
+        }
     }
 #pragma unroll
-    for (int k = 0; k < kLevelCols; ++k) {
-        const int t = base + k * kLevelThreads;
-        if (t < ncols) ro[t] = (has_b && t >= s) ? __fadd_rn(va[k], vb[k]) : va[k];
+    for (int k = 0; k < kLevelVecs; ++k) {
+        const int q = base + k * kLevelThreads;
+        if (q >= nv) continue;
+        const int t = 4 * q;
+        float4 o = va[k];
+        if (has_b) {
+            if (t >= s) o.x = __fadd_rn(o.x, vb[k][0]);
+            if (t + 1 >= s) o.y = __fadd_rn(o.y, vb[k][1]);
+            if (t + 2 >= s) o.z = __fadd_rn(o.z, vb[k][2]);
+            if (t + 3 >= s) o.w = __fadd_rn(o.w, vb[k][3]);
+        }
+        if (VOUT) {
+            reinterpret_cast<float4*>(ro)[q] = o;
+        } else {
+            if (t < ncols) ro[t] = o.x;
+            if (t + 1 < ncols) ro[t + 1] = o.y;
+            if (t + 2 < ncols) ro[t + 2] = o.z;
+            if (t + 3 < ncols) ro[t + 3] = o.w;
+        }
     }
 }
 
@@ -114,12 +146,65 @@ k_fdmt_level(const float* __restrict__ in, float* __restrict__ out, const int4* 
 // samples u >= halo are written; the plan's look-back guarantees that every
 // value they depend on was computed from in-tile samples (u - shift >= 0), so
 // the halo columns may hold partial values.  Samples t < 0 are the zeros the
-// reference's planes hold there.
+// reference's planes hold there.  The group's row tables are staged in shared
+// memory (after the two planes) and merge rows are processed four at a time
+// with all loads issued before the stores.  R0C = level-0 rows per channel
+// (0: runtime value rows_per_chan).
 // grid: (ceil(ncols / tile), nchan / group)
+template <int R0C>
+__device__ __forceinline__ void head_level0(const float* __restrict__ x, float* __restrict__ bufa,
+                                            int c0, int group, int rows_per_chan, int ncols, int t,
+                                            int u, int W, int ones) {
+    const int r0c = R0C > 0 ? R0C : rows_per_chan;
+#pragma unroll 2
+    for (int c = 0; c < group; ++c) {
+        const float* xr = x + static_cast<size_t>(c0 + c) * ncols;
+        float* dst = bufa + c * r0c * W + u;
+        float v = 0.0f;
+        if (t >= 0) v = ones ? 1.0f : (t < ncols ? __ldg(xr + t) : 0.0f);
+        dst[0] = v;
+        if constexpr (R0C > 0) {
+#pragma unroll
+            for (int r = 1; r < R0C; ++r) {
+                float w = 0.0f;
+                if (t >= r) {
+                    const int tt = t - r;
+                    const float xv = ones ? 1.0f : (tt < ncols ? __ldg(xr + tt) : 0.0f);
+                    v = __fdiv_rn(__fadd_rn(__fmul_rn(v, static_cast<float>(r)), xv),
+                                  static_cast<float>(r + 1));
+                    w = v;
+                }
+                dst[r * W] = w;
+            }
+        } else {
+#pragma unroll 1
+            for (int r = 1; r < r0c; ++r) {
+                float w = 0.0f;
+                if (t >= r) {
+                    const int tt = t - r;
+                    const float xv = ones ? 1.0f : (tt < ncols ? __ldg(xr + tt) : 0.0f);
+                    v = __fdiv_rn(__fadd_rn(__fmul_rn(v, static_cast<float>(r)), xv),
+                                  static_cast<float>(r + 1));
+                    w = v;
+                }
+                dst[r * W] = w;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ float head_merge(const float* __restrict__ src, int4 e, int u, int t, int W) {
+    const float a = src[e.x * W + u];
+    const float b = src[e.y * W + max(u - e.z, 0)];
+    return (t >= e.z && u >= e.z) ? __fadd_rn(a, b) : a;
+}
+
+template <int R0C>
 __global__ void __launch_bounds__(1024)
 k_fdmt_head(const float* __restrict__ x, float* __restrict__ out,
             const HeadGroup* __restrict__ groups, const int4* __restrict__ tab, int ncols,
-            int depth, int group, int rows_per_chan, int tile, int rows_a, int ones) {
+            int out_pitch, int depth, int group, int rows_per_chan, int tile, int rows_a,
+            int rows_b, int ones) {
     extern __shared__ float sm[];
     const int W = blockDim.x;
     const int u = threadIdx.x;
@@ -128,26 +213,14 @@ k_fdmt_head(const float* __restrict__ x, float* __restrict__ out,
     const int t = blockIdx.x * tile - halo + u;
     float* bufa = sm;
     float* bufb = sm + rows_a * W;
+    int4* stab = reinterpret_cast<int4*>(sm + (rows_a + rows_b) * W);
 
-    const int c0 = blockIdx.y * group;
-    for (int c = 0; c < group; ++c) {
-        const float* xr = x + static_cast<size_t>(c0 + c) * ncols;
-        float* dst = bufa + c * rows_per_chan * W + u;
-        float v = 0.0f;
-        if (t >= 0) v = ones ? 1.0f : (t < ncols ? __ldg(xr + t) : 0.0f);
-        dst[0] = v;
-        for (int r = 1; r < rows_per_chan; ++r) {
-            float w = 0.0f;
-            if (t >= r) {
-                const int tt = t - r;
-                const float xv = ones ? 1.0f : (tt < ncols ? __ldg(xr + tt) : 0.0f);
-                v = __fdiv_rn(__fadd_rn(__fmul_rn(v, static_cast<float>(r)), xv),
-                              static_cast<float>(r + 1));
-                w = v;
-            }
-            dst[r * W] = w;
-        }
-    }
+    // stage this group's tables (levels 1..depth are contiguous)
+    const int tab0 = __ldg(&hg->tab_off[1]);
+    const int ntab = __ldg(&hg->tab_off[depth]) + __ldg(&hg->rows[depth]) - tab0;
+    for (int i = u; i < ntab; i += W) stab[i] = __ldg(tab + tab0 + i);
+
+    head_level0<R0C>(x, bufa, blockIdx.y * group, group, rows_per_chan, ncols, t, u, W, ones);
     __syncthreads();
 
     float* src = bufa;
@@ -155,27 +228,92 @@ k_fdmt_head(const float* __restrict__ x, float* __restrict__ out,
     const bool writer = (u >= halo) && (u < halo + tile) && (t < ncols);
     for (int l = 1; l <= depth; ++l) {
         const int rows = __ldg(&hg->rows[l]);
-        const int4* tb = tab + __ldg(&hg->tab_off[l]);
+        const int4* tb = stab + (__ldg(&hg->tab_off[l]) - tab0);
         if (l < depth) {
-            for (int j = 0; j < rows; ++j) {
-                const int4 e = __ldg(tb + j);
-                float v = src[e.x * W + u];
-                if (t >= e.z && u >= e.z) v = __fadd_rn(v, src[e.y * W + u - e.z]);
-                dst[j * W + u] = v;
+            int j = 0;
+            for (; j + 4 <= rows; j += 4) {
+                const float v0 = head_merge(src, tb[j], u, t, W);
+                const float v1 = head_merge(src, tb[j + 1], u, t, W);
+                const float v2 = head_merge(src, tb[j + 2], u, t, W);
+                const float v3 = head_merge(src, tb[j + 3], u, t, W);
+                dst[j * W + u] = v0;
+                dst[(j + 1) * W + u] = v1;
+                dst[(j + 2) * W + u] = v2;
+                dst[(j + 3) * W + u] = v3;
             }
+            for (; j < rows; ++j) dst[j * W + u] = head_merge(src, tb[j], u, t, W);
             __syncthreads();
             float* tmp = src; src = dst; dst = tmp;
         } else {
-            float* o = out + static_cast<size_t>(__ldg(&hg->out_row0)) * ncols + t;
-            for (int j = 0; j < rows; ++j) {
-                const int4 e = __ldg(tb + j);
-                float v = src[e.x * W + u];
-                if (t >= e.z && u >= e.z) v = __fadd_rn(v, src[e.y * W + u - e.z]);
-                if (writer) o[static_cast<size_t>(j) * ncols] = v;
+            float* o = out + static_cast<size_t>(__ldg(&hg->out_row0)) * out_pitch + t;
+            int j = 0;
+            for (; j + 4 <= rows; j += 4) {
+                const float v0 = head_merge(src, tb[j], u, t, W);
+                const float v1 = head_merge(src, tb[j + 1], u, t, W);
+                const float v2 = head_merge(src, tb[j + 2], u, t, W);
+                const float v3 = head_merge(src, tb[j + 3], u, t, W);
+                if (writer) {
+                    o[static_cast<size_t>(j) * out_pitch] = v0;
+                    o[static_cast<size_t>(j + 1) * out_pitch] = v1;
+                    o[static_cast<size_t>(j + 2) * out_pitch] = v2;
+                    o[static_cast<size_t>(j + 3) * out_pitch] = v3;
+                }
+            }
+            for (; j < rows; ++j) {
+                const float v = head_merge(src, tb[j], u, t, W);
+                if (writer) o[static_cast<size_t>(j) * out_pitch] = v;
             }
         }
     }
 }
+
+using HeadKernel = void (*)(const float*, float*, const HeadGroup*, const int4*, int, int, int, int,
+                            int, int, int, int, int);
+
+HeadKernel head_kernel_for(int rows_per_chan) {
+    switch (rows_per_chan) {
+        case 1: return k_fdmt_head<1>;
+        case 2: return k_fdmt_head<2>;
+        case 3: return k_fdmt_head<3>;
+        case 4: return k_fdmt_head<4>;
+        default: return k_fdmt_head<0>;
+    }
+}
+
+// Launches the fused head with its shared-memory opt-in.
+cudaError_t launch_head(const HeadPlan& hp, const FdmtPlanHost& h, const float* d_in, float* dst,
+                        int out_pitch, const HeadGroup* groups, const int* tab, int ones,
+                        cudaStream_t s) {
+    HeadKernel kern = head_kernel_for(h.rows_per_chan0);
+    if (hp.smem_bytes > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(hp.smem_bytes));
+        if (e != cudaSuccess) return e;
+    }
+    dim3 grid((h.ncols + hp.tile - 1) / hp.tile, h.nchan / hp.group);
+    kern<<<grid, hp.width, hp.smem_bytes, s>>>(d_in, dst, groups, reinterpret_cast<const int4*>(tab),
+                                               h.ncols, out_pitch, hp.depth, hp.group,
+                                               h.rows_per_chan0,
+                                               hp.tile, hp.rows_a, hp.rows_b, ones);
+    return cudaGetLastError();
+}
+
+// Launches one merge level (vector stores when the output allows them).
+cudaError_t launch_level(const float* src, float* dst, const int4* tab, int rows, int T,
+                         int in_pitch, int out_pitch, cudaStream_t s) {
+    const int span = kLevelThreads * kLevelVecs;
+    dim3 grid(rows, ((T + 3) / 4 + span - 1) / span);
+    if (grid.y > 65535) return cudaErrorInvalidConfiguration;
+    const bool vout = (out_pitch % 4 == 0) && (reinterpret_cast<uintptr_t>(dst) & 15) == 0;
+    if (vout)
+        k_fdmt_level<true><<<grid, kLevelThreads, 0, s>>>(src, dst, tab, T, in_pitch, out_pitch);
+    else
+        k_fdmt_level<false><<<grid, kLevelThreads, 0, s>>>(src, dst, tab, T, in_pitch, out_pitch);
+    return cudaGetLastError();
+}
+
+// Row pitch (floats) of the workspace planes: ncols rounded up to 128 bytes.
+inline int plane_pitch(int ncols) { return (ncols + 31) / 32 * 32; }
 
 constexpr int kHeadTile = 256;
 constexpr size_t kHeadSmemTwoPerSm = 113 * 1024;  // two CTAs per SM
@@ -242,9 +380,6 @@ extern "C" bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc, bfs_fdmt_p
         BFS_CUDA(cudaMalloc(&p->d_head_tab, hp.tab.size() * sizeof(int)));
         BFS_CUDA(cudaMemcpy(p->d_head_tab, hp.tab.data(), hp.tab.size() * sizeof(int),
                             cudaMemcpyHostToDevice));
-        if (hp.smem_bytes > 48 * 1024)
-            BFS_CUDA(cudaFuncSetAttribute(k_fdmt_head, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          static_cast<int>(hp.smem_bytes)));
     }
 
     // device row tables
@@ -268,7 +403,7 @@ extern "C" bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc, bfs_fdmt_p
     p->external_ws = (desc->flags & BFS_FDMT_EXTERNAL_WS) != 0;
     for (int b = 0; b < 2 && !p->external_ws; ++b) {
         if (p->buf_rows[b] == 0) continue;
-        const size_t bytes = p->buf_rows[b] * static_cast<size_t>(h.ncols) * sizeof(float);
+        const size_t bytes = p->buf_rows[b] * static_cast<size_t>(plane_pitch(h.ncols)) * sizeof(float);
         cudaError_t e = cudaMalloc(&p->d_buf[b], bytes);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -346,7 +481,7 @@ extern "C" bfs_status bfs_fdmt_plan_tables(const bfs_fdmt_plan* plan, int level,
 }
 
 static size_t plane_bytes(const bfs_fdmt_plan* p, int b) {
-    const size_t raw = p->buf_rows[b] * static_cast<size_t>(p->host.ncols) * sizeof(float);
+    const size_t raw = p->buf_rows[b] * static_cast<size_t>(plane_pitch(p->host.ncols)) * sizeof(float);
     return (raw + 255) & ~static_cast<size_t>(255);
 }
 
@@ -360,32 +495,29 @@ static bfs_status fdmt_run(bfs_fdmt_plan* plan, const float* d_in, float* d_out,
                            float* buf0, float* buf1, cudaStream_t s) {
     const FdmtPlanHost& h = plan->host;
     const int T = h.ncols;
+    const int P = plane_pitch(T);
     float* bufs[2] = {buf0, buf1};
     const int k = plan->head.depth;
     if (k > 0) {
         const HeadPlan& hp = plan->head;
-        dim3 grid((T + hp.tile - 1) / hp.tile, h.nchan / hp.group);
-        BFS_ARG(grid.y <= 65535, "nchan too large for this build");
+        BFS_ARG(h.nchan / hp.group <= 65535, "nchan too large for this build");
         float* dst = (k == h.niter) ? d_out : bufs[k & 1];
-        k_fdmt_head<<<grid, hp.width, hp.smem_bytes, s>>>(
-            d_in, dst, plan->d_head_groups, reinterpret_cast<const int4*>(plan->d_head_tab), T, k,
-            hp.group, h.rows_per_chan0, hp.tile, hp.rows_a, b_ones ? 1 : 0);
-        BFS_LAUNCH_CHECK("k_fdmt_head");
+        cudaError_t e = launch_head(hp, h, d_in, dst, (k == h.niter) ? T : P, plan->d_head_groups,
+                                    plan->d_head_tab, b_ones ? 1 : 0, s);
+        if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_head: %s", cudaGetErrorString(e));
     } else {
         dim3 grid((T + kInitThreads * kInitCols - 1) / (kInitThreads * kInitCols), h.nchan);
         BFS_ARG(grid.y <= 65535, "nchan too large for this build");
-        k_fdmt_init<<<grid, kInitThreads, 0, s>>>(d_in, bufs[0], T, h.rows_per_chan0,
+        k_fdmt_init<<<grid, kInitThreads, 0, s>>>(d_in, bufs[0], T, P, h.rows_per_chan0,
                                                   b_ones ? 1 : 0);
         BFS_LAUNCH_CHECK("k_fdmt_init");
     }
-    const int chunk = kLevelThreads * kLevelCols;
     for (int l = k + 1; l <= h.niter; ++l) {
         const float* src = bufs[(l - 1) & 1];
         float* dst = (l == h.niter) ? d_out : bufs[l & 1];
-        dim3 grid(h.lv[l].total_rows(), (T + chunk - 1) / chunk);
-        BFS_ARG(grid.y <= 65535, "ncols too large for this build");
-        k_fdmt_level<<<grid, kLevelThreads, 0, s>>>(src, dst, plan->d_tab + plan->tab_off[l], T);
-        BFS_LAUNCH_CHECK("k_fdmt_level");
+        cudaError_t e = launch_level(src, dst, plan->d_tab + plan->tab_off[l], h.lv[l].total_rows(),
+                                     T, P, (l == h.niter) ? T : P, s);
+        if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_level: %s", cudaGetErrorString(e));
     }
     return BFS_OK;
 }
@@ -493,7 +625,8 @@ extern "C" bfs_status bfs_fdmt_noalloc_scratch_bytes(const bfs_fdmt_plan* plan, 
     if (k > 0)
         total += align256(plan->head.groups.size() * sizeof(HeadGroup)) +
                  align256(plan->head.tab.size() * sizeof(int));
-    total += align256(prow[0] * h.ncols * sizeof(float)) + align256(prow[1] * h.ncols * sizeof(float));
+    const size_t P = static_cast<size_t>(plane_pitch(h.ncols));
+    total += align256(prow[0] * P * sizeof(float)) + align256(prow[1] * P * sizeof(float));
     if (need) *need = total;
     if (capacity) *capacity = kNoAllocScratchBytes;
     return BFS_OK;
@@ -539,7 +672,8 @@ extern "C" bfs_status bfs_fdmt_execute_noalloc(const bfs_fdmt_plan* plan, const 
     }
     float* bufs[2];
     bufs[0] = reinterpret_cast<float*>(p);
-    p += align256(prow[0] * T * sizeof(float));
+    const int P = plane_pitch(T);
+    p += align256(prow[0] * static_cast<size_t>(P) * sizeof(float));
     bufs[1] = reinterpret_cast<float*>(p);
 
     // tables: host vectors -> staged ints -> packed int4 rows
@@ -567,31 +701,24 @@ extern "C" bfs_status bfs_fdmt_execute_noalloc(const bfs_fdmt_plan* plan, const 
                                  cudaMemcpyHostToDevice, s));
         BFS_CUDA(cudaMemcpyAsync(head_tab, hp.tab.data(), hp.tab.size() * sizeof(int),
                                  cudaMemcpyHostToDevice, s));
-        if (hp.smem_bytes > 48 * 1024)
-            BFS_CUDA(cudaFuncSetAttribute(k_fdmt_head, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          static_cast<int>(hp.smem_bytes)));
-        dim3 grid((T + hp.tile - 1) / hp.tile, h.nchan / hp.group);
-        BFS_ARG(grid.y <= 65535, "nchan too large for this build");
+        BFS_ARG(h.nchan / hp.group <= 65535, "nchan too large for this build");
         float* dst = (k == h.niter) ? d_out : bufs[k & 1];
-        k_fdmt_head<<<grid, hp.width, hp.smem_bytes, s>>>(
-            d_in, dst, groups, reinterpret_cast<const int4*>(head_tab), T, k, hp.group,
-            h.rows_per_chan0, hp.tile, hp.rows_a, b_ones ? 1 : 0);
-        BFS_LAUNCH_CHECK("k_fdmt_head");
+        cudaError_t e = launch_head(hp, h, d_in, dst, (k == h.niter) ? T : P, groups, head_tab,
+                                    b_ones ? 1 : 0, s);
+        if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_head: %s", cudaGetErrorString(e));
     } else {
         dim3 grid((T + kInitThreads * kInitCols - 1) / (kInitThreads * kInitCols), h.nchan);
         BFS_ARG(grid.y <= 65535, "nchan too large for this build");
-        k_fdmt_init<<<grid, kInitThreads, 0, s>>>(d_in, bufs[0], T, h.rows_per_chan0,
+        k_fdmt_init<<<grid, kInitThreads, 0, s>>>(d_in, bufs[0], T, P, h.rows_per_chan0,
                                                   b_ones ? 1 : 0);
         BFS_LAUNCH_CHECK("k_fdmt_init");
     }
-    const int chunk = kLevelThreads * kLevelCols;
     for (int l = k + 1; l <= h.niter; ++l) {
         const float* src = bufs[(l - 1) & 1];
         float* dst = (l == h.niter) ? d_out : bufs[l & 1];
-        dim3 grid(h.lv[l].total_rows(), (T + chunk - 1) / chunk);
-        BFS_ARG(grid.y <= 65535, "ncols too large for this build");
-        k_fdmt_level<<<grid, kLevelThreads, 0, s>>>(src, dst, tab + off[l], T);
-        BFS_LAUNCH_CHECK("k_fdmt_level");
+        cudaError_t e = launch_level(src, dst, tab + off[l], h.lv[l].total_rows(), T, P,
+                                     (l == h.niter) ? T : P, s);
+        if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_level: %s", cudaGetErrorString(e));
     }
     return BFS_OK;
 }

@@ -18,6 +18,9 @@ bfs_status fail(bfs_status st, const char* fmt, ...);
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// cudaMallocAsync from the device's default pool, which keeps freed memory.
+bfs_status stream_alloc(void** p, size_t bytes, cudaStream_t s);
+
 #define BFS_CUDA(call)                                                                     \
     do {                                                                                   \
         cudaError_t e_ = (call);                                                           \
@@ -88,6 +91,7 @@ struct HeadPlan {
     int width = 0;          // tile + max halo, rounded to a warp: threads per CTA
     int rows_a = 0;         // shared rows of the even-level buffer (level 0, 2, ...)
     int rows_b = 0;         // shared rows of the odd-level buffer
+    int tab_rows = 0;       // largest per-group table (levels 1..k), staged in shared memory
     size_t smem_bytes = 0;
     std::vector<HeadGroup> groups;
     std::vector<int> tab;   // 4 ints per row: {a_local, b_local, shift, 0}

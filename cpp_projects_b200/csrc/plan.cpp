@@ -201,12 +201,16 @@ bool build_head_plan(const FdmtPlanHost& p, int k, int tile, size_t smem_limit, 
         }
         h.rows_a = std::max(h.rows_a, rows_a);
         h.rows_b = std::max(h.rows_b, rows_b);
+        int trows = 0;
+        for (int l = 1; l <= k; ++l) trows += hg.rows[l];
+        h.tab_rows = std::max(h.tab_rows, trows);
         max_halo = std::max(max_halo, hg.halo);
         h.groups.push_back(hg);
     }
     h.width = ((tile + max_halo) + 31) / 32 * 32;
     if (h.width > 1024) return false;
-    h.smem_bytes = static_cast<size_t>(h.rows_a + h.rows_b) * h.width * sizeof(float);
+    h.smem_bytes = static_cast<size_t>(h.rows_a + h.rows_b) * h.width * sizeof(float) +
+                   static_cast<size_t>(h.tab_rows) * 4 * sizeof(int);
     if (h.smem_bytes > smem_limit) return false;
     *out = std::move(h);
     return true;

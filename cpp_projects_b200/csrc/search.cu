@@ -20,8 +20,12 @@
 // reference's heap order — with a stable device radix sort.
 #include <cub/device/device_radix_sort.cuh>
 
+#include <cmath>
+
 #include "internal.h"
 #include "search_common.cuh"
+
+#define BFS_TRY_ST(x) do { bfs_status st_ = (x); if (st_ != BFS_OK) return st_; } while (0)
 
 namespace bfs {
 namespace {
@@ -30,7 +34,6 @@ constexpr int kBoxThreads = 256;
 constexpr int kBoxTile = 1024;  // start samples per CTA
 constexpr int kMaxPow2Q = 16;
 constexpr int kMaxAllW = 4096;
-constexpr int kWidthBits = 12;
 
 // stats[r] = mean, stats[rows + r] = std (mode 0) or population variance (mode 1)
 __global__ void __cluster_dims__(kStatCluster, 1, 1) __launch_bounds__(kStatThreads)
@@ -130,14 +133,126 @@ k_boxcar(const float* __restrict__ plane, int rows, int cols, const float* __res
     }
 }
 
-__global__ void k_cand_keys(const bfs_cand* __restrict__ c, unsigned n, int cols, int mode,
+// Register-blocked boxcar for a width set fixed at compile time
+// (MODE 0: 1, 2, 4 .. WMAX; MODE 1: 1 .. WMAX).  Each thread owns kRegStarts
+// adjacent start samples; their window x[t .. t + kRegStarts + WMAX - 2] is
+// read once from shared memory with 128-bit loads and the running sums
+// advance from registers.  sqrtf(w) and RN(1/sqrtf(w)) come from the host
+// (IEEE there too).  The exact quotient sum / sqrtf(w) is only evaluated when
+// a one-multiply estimate cannot rule the window out: the estimate
+// qa = RN(sum * RN(1/sqrtf(w))) is within 2^-22 of the true quotient, so for
+// thr > 0 a window with qa <= thr * (1 - 1e-5) (thr_lo) cannot have
+// RN(sum / sqrtf(w)) > thr.  One warp vote per width skips the emission code
+// when no lane has a window above thr_lo.
+constexpr int kRegStarts = 4;
+constexpr int kRegTile = kBoxThreads * kRegStarts;
+
+struct WidthConsts {
+    float sq[33];  // sqrtf(w), w = 1..32 (index w)
+    float rs[33];  // RN(1 / sqrtf(w))
+};
+
+template <int MODE, int WMAX>
+__global__ void __launch_bounds__(kBoxThreads)
+k_boxcar_reg(const float* __restrict__ plane, int rows, int cols, const float* __restrict__ stats,
+             const float* __restrict__ d_thr, float thr_host, float thr_lo_host, int snr_fast,
+             bfs_cand* __restrict__ out, unsigned capacity, unsigned* __restrict__ d_count,
+             const WidthConsts wc) {
+    constexpr int kWin = kRegStarts + WMAX - 1;
+    constexpr int kVec = (kWin + 3) / 4;
+    __shared__ float4 tile4[(kRegTile + 4 * kVec + 3) / 4];
+    float* tile = reinterpret_cast<float*>(tile4);
+    const int row = blockIdx.y;
+    const int t0 = blockIdx.x * kRegTile;
+    const float* x = plane + static_cast<size_t>(row) * cols;
+    constexpr int kSpan = kRegTile + 4 * kVec;
+    // interior tile: every window of every start lies inside the row
+    const bool interior = (t0 + kSpan) <= cols;
+    if (stats) {
+        const float m = stats[row], sd = stats[rows + row];
+        for (int i = threadIdx.x; i < kSpan; i += kBoxThreads) {
+            const int t = t0 + i;
+            tile[i] = (interior || t < cols) ? norm_sample(__ldg(x + t), m, sd) : 0.0f;
+        }
+    } else {
+        for (int i = threadIdx.x; i < kSpan; i += kBoxThreads) {
+            const int t = t0 + i;
+            tile[i] = (interior || t < cols) ? __ldg(x + t) : 0.0f;
+        }
+    }
+    __syncthreads();
+    float thr = thr_host, thr_lo = thr_lo_host;
+    if (d_thr) {
+        thr = __ldg(d_thr);
+        thr_lo = thr > 0.0f ? thr * 0.99999f : -INFINITY;
+    }
+    float win[4 * kVec];
+#pragma unroll
+    for (int v = 0; v < kVec; ++v) {
+        const float4 q = tile4[threadIdx.x + v];
+        win[4 * v] = q.x; win[4 * v + 1] = q.y; win[4 * v + 2] = q.z; win[4 * v + 3] = q.w;
+    }
+    const int tb = t0 + threadIdx.x * kRegStarts;
+    const int lane = threadIdx.x & 31;
+    float sum[kRegStarts];
+#pragma unroll
+    for (int j = 0; j < kRegStarts; ++j) sum[j] = 0.0f;
+#pragma unroll
+    for (int w = 1; w <= WMAX; ++w) {
+#pragma unroll
+        for (int j = 0; j < kRegStarts; ++j) sum[j] = __fadd_rn(sum[j], win[j + w - 1]);
+        if (MODE == 0 && (w & (w - 1)) != 0) continue;
+        const float rs = wc.rs[w];
+        bool maybe[kRegStarts];
+        bool anyp = false;
+#pragma unroll
+        for (int j = 0; j < kRegStarts; ++j) {
+            maybe[j] = __fmul_rn(sum[j], rs) > thr_lo && (interior || (tb + j + w - 1) < cols);
+            anyp |= maybe[j];
+        }
+        if (!__any_sync(0xffffffffu, anyp)) continue;
+        const float sq = wc.sq[w];
+        const int code = (MODE == 1) ? w : (31 - __clz(w));
+#pragma unroll
+        for (int j = 0; j < kRegStarts; ++j) {
+            float snr = 0.0f;
+            bool pass = false;
+            if (maybe[j]) {
+                snr = snr_fast ? __fdividef(sum[j], sq) : __fdiv_rn(sum[j], sq);
+                pass = snr > thr;
+            }
+            const unsigned ballot = __ballot_sync(0xffffffffu, pass);
+            if (ballot) {
+                const int leader = __ffs(ballot) - 1;
+                unsigned base = 0;
+                if (lane == leader) base = atomicAdd(d_count, static_cast<unsigned>(__popc(ballot)));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (pass) {
+                    const unsigned idx = base + __popc(ballot & ((1u << lane) - 1u));
+                    if (idx < capacity) {
+                        bfs_cand c;
+                        c.mt = tb + j; c.mdt = row; c.mwidth = code; c.msnr = snr;
+                        out[idx] = c;
+                    }
+                }
+            }
+        }
+    }
+}
+
+// Canonical key of a candidate: (row * cols + start) << wbits | width code,
+// with the width code 0..Q (pow2 mode) or w-1 (all-widths mode).
+__device__ __forceinline__ unsigned long long cand_key(const bfs_cand& v, int cols, int mode, int wbits) {
+    const unsigned long long cell = static_cast<unsigned long long>(v.mdt) * cols + v.mt;
+    const unsigned long long code = static_cast<unsigned long long>(mode == 0 ? v.mwidth : v.mwidth - 1);
+    return (cell << wbits) | code;
+}
+
+__global__ void k_cand_keys(const bfs_cand* __restrict__ c, unsigned n, int cols, int mode, int wbits,
                             unsigned long long* __restrict__ keys, unsigned* __restrict__ vals) {
     const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const bfs_cand v = c[i];
-    const unsigned long long wcode =
-        static_cast<unsigned long long>(mode == 0 ? v.mwidth : v.mwidth - 1);
-    keys[i] = ((static_cast<unsigned long long>(v.mdt) * cols + v.mt) << kWidthBits) | wcode;
+    keys[i] = cand_key(c[i], cols, mode, wbits);
     vals[i] = i;
 }
 
@@ -145,6 +260,32 @@ __global__ void k_gather_cands(const bfs_cand* __restrict__ src, const unsigned*
                                unsigned n, bfs_cand* __restrict__ dst) {
     const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[i] = src[idx[i]];
+}
+
+// 32-bit variant: the key holds the whole position, the S/N rides along as
+// the sort value, and the records are rebuilt from (key, S/N).
+__global__ void k_cand_keys32(const bfs_cand* __restrict__ c, unsigned n, int cols, int mode, int wbits,
+                              unsigned* __restrict__ keys, unsigned* __restrict__ vals) {
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bfs_cand v = c[i];
+    keys[i] = static_cast<unsigned>(cand_key(v, cols, mode, wbits));
+    vals[i] = __float_as_uint(v.msnr);
+}
+
+__global__ void k_cand_decode32(const unsigned* __restrict__ keys, const unsigned* __restrict__ vals,
+                                unsigned n, int cols, int mode, int wbits, bfs_cand* __restrict__ out) {
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned k = keys[i];
+    const unsigned cell = wbits ? (k >> wbits) : k;
+    const int code = static_cast<int>(k & ((1u << wbits) - 1u));
+    bfs_cand c;
+    c.mt = static_cast<int>(cell % static_cast<unsigned>(cols));
+    c.mdt = static_cast<int>(cell / static_cast<unsigned>(cols));
+    c.mwidth = mode == 0 ? code : code + 1;
+    c.msnr = __uint_as_float(vals[i]);
+    out[i] = c;
 }
 
 int bits_for(unsigned long long v) {
@@ -158,25 +299,43 @@ int bits_for(unsigned long long v) {
 // Sorts n candidates of a rows x cols plane into the canonical order in place.
 // Scratch comes from the stream-ordered pool allocator.
 bfs_status sort_candidates_canonical(bfs_cand* d_c, unsigned n, int rows, int cols, int mode,
-                                     cudaStream_t s) {
+                                     int param, cudaStream_t s) {
     if (n < 2) return BFS_OK;
+    const int wbits = bits_for(static_cast<unsigned long long>(mode == 0 ? param : param - 1));
+    const int cell_bits = bits_for(static_cast<unsigned long long>(rows) * cols - 1);
+    const int end_bit = cell_bits + wbits;
+    const int th = 256, bl = static_cast<int>((n + th - 1) / th);
+    void* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+    if (end_bit <= 32) {
+        unsigned *k = nullptr, *v = nullptr;
+        BFS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, k, k, v, v,
+                                                 static_cast<int>(n), 0, end_bit, s));
+        BFS_TRY_ST(stream_alloc(reinterpret_cast<void**>(&k), n * sizeof(unsigned) * 4, s));
+        v = k + 2 * static_cast<size_t>(n);
+        BFS_TRY_ST(stream_alloc(&cub_tmp, cub_bytes ? cub_bytes : 16, s));
+        k_cand_keys32<<<bl, th, 0, s>>>(d_c, n, cols, mode, wbits, k, v);
+        BFS_LAUNCH_CHECK("k_cand_keys32");
+        BFS_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp, cub_bytes, k, k + n, v, v + n,
+                                                 static_cast<int>(n), 0, end_bit, s));
+        k_cand_decode32<<<bl, th, 0, s>>>(k + n, v + n, n, cols, mode, wbits, d_c);
+        BFS_LAUNCH_CHECK("k_cand_decode32");
+        BFS_CUDA(cudaFreeAsync(k, s));
+        BFS_CUDA(cudaFreeAsync(cub_tmp, s));
+        return BFS_OK;
+    }
     unsigned long long *k_in = nullptr, *k_out = nullptr;
     unsigned *v_in = nullptr, *v_out = nullptr;
     bfs_cand* tmp = nullptr;
-    void* cub_tmp = nullptr;
-    size_t cub_bytes = 0;
-    const int end_bit =
-        bits_for((static_cast<unsigned long long>(rows) * cols) << kWidthBits);
     BFS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, k_in, k_out, v_in, v_out,
                                              static_cast<int>(n), 0, end_bit, s));
-    BFS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&k_in), n * sizeof(unsigned long long) * 2, s));
+    BFS_TRY_ST(stream_alloc(reinterpret_cast<void**>(&k_in), n * sizeof(unsigned long long) * 2, s));
     k_out = k_in + n;
-    BFS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&v_in), n * sizeof(unsigned) * 2, s));
+    BFS_TRY_ST(stream_alloc(reinterpret_cast<void**>(&v_in), n * sizeof(unsigned) * 2, s));
     v_out = v_in + n;
-    BFS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&tmp), n * sizeof(bfs_cand), s));
-    BFS_CUDA(cudaMallocAsync(&cub_tmp, cub_bytes ? cub_bytes : 16, s));
-    const int th = 256, bl = static_cast<int>((n + th - 1) / th);
-    k_cand_keys<<<bl, th, 0, s>>>(d_c, n, cols, mode, k_in, v_in);
+    BFS_TRY_ST(stream_alloc(reinterpret_cast<void**>(&tmp), n * sizeof(bfs_cand), s));
+    BFS_TRY_ST(stream_alloc(&cub_tmp, cub_bytes ? cub_bytes : 16, s));
+    k_cand_keys<<<bl, th, 0, s>>>(d_c, n, cols, mode, wbits, k_in, v_in);
     BFS_LAUNCH_CHECK("k_cand_keys");
     BFS_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp, cub_bytes, k_in, k_out, v_in, v_out,
                                              static_cast<int>(n), 0, end_bit, s));
@@ -217,6 +376,47 @@ bfs_status launch_boxcar(const float* d_plane, int rows, int cols, const float* 
     } else {
         return fail(BFS_ERR_ARG, "unknown widths_mode %d", mode);
     }
+    {
+        // compile-time width sets: pow2 up to 32, every width up to 8
+        const float thr_lo = thr > 0.0f ? thr * 0.99999f : -INFINITY;
+        dim3 grid_r((cols + kRegTile - 1) / kRegTile, rows);
+        WidthConsts wc;
+        for (int w = 0; w <= 32; ++w) {
+            wc.sq[w] = std::sqrt(static_cast<float>(w));  // IEEE-correct on the host
+            wc.rs[w] = w ? 1.0f / wc.sq[w] : 0.0f;
+        }
+        bool launched = true;
+#define BFS_BOX_REG(M, W) k_boxcar_reg<M, W><<<grid_r, kBoxThreads, 0, s>>>(                  \
+            d_plane, rows, cols, d_stats, d_thr, thr, thr_lo, snr_fast, d_out, capacity, d_count, wc)
+        if (mode == BFS_WIDTHS_POW2) {
+            switch (wmax) {
+                case 1: BFS_BOX_REG(0, 1); break;
+                case 2: BFS_BOX_REG(0, 2); break;
+                case 4: BFS_BOX_REG(0, 4); break;
+                case 8: BFS_BOX_REG(0, 8); break;
+                case 16: BFS_BOX_REG(0, 16); break;
+                case 32: BFS_BOX_REG(0, 32); break;
+                default: launched = false;
+            }
+        } else {
+            switch (wmax) {
+                case 1: BFS_BOX_REG(1, 1); break;
+                case 2: BFS_BOX_REG(1, 2); break;
+                case 3: BFS_BOX_REG(1, 3); break;
+                case 4: BFS_BOX_REG(1, 4); break;
+                case 5: BFS_BOX_REG(1, 5); break;
+                case 6: BFS_BOX_REG(1, 6); break;
+                case 7: BFS_BOX_REG(1, 7); break;
+                case 8: BFS_BOX_REG(1, 8); break;
+                default: launched = false;
+            }
+        }
+#undef BFS_BOX_REG
+        if (launched) {
+            BFS_LAUNCH_CHECK("k_boxcar_reg");
+            return BFS_OK;
+        }
+    }
     dim3 grid((cols + kBoxTile - 1) / kBoxTile, rows);
     const size_t smem = sizeof(float) * (kBoxTile + wmax - 1);
     if (mode == BFS_WIDTHS_POW2) {
@@ -250,7 +450,7 @@ extern "C" bfs_status bfs_norm_rows(const float* d_in, float* d_out, int rows, i
     BFS_ARG(d_in && d_out, "null argument");
     cudaStream_t s = as_stream(stream);
     float* stats = d_stats;
-    if (!stats) BFS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&stats), sizeof(float) * 2 * rows, s));
+    if (!stats) BFS_TRY_ST(stream_alloc(reinterpret_cast<void**>(&stats), sizeof(float) * 2 * rows, s));
     bfs_status st = launch_row_stats(d_in, rows, cols, stats, 0, s);
     if (st == BFS_OK) {
         dim3 grid(std::min((cols + 255) / 256, 64), rows);
@@ -269,7 +469,7 @@ extern "C" bfs_status bfs_boxcar_gather(const float* d_plane, int rows, int cols
     BFS_ARG(h_count != nullptr, "h_count is null");
     cudaStream_t s = as_stream(stream);
     unsigned* d_count = nullptr;
-    BFS_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_count), sizeof(unsigned), s));
+    BFS_TRY_ST(stream_alloc(reinterpret_cast<void**>(&d_count), sizeof(unsigned), s));
     BFS_CUDA(cudaMemsetAsync(d_count, 0, sizeof(unsigned), s));
     bfs_status st = launch_boxcar(d_plane, rows, cols, d_stats, thr, d_thr, widths_mode, param,
                                   snr_fast, d_out, capacity, d_count, s);
@@ -284,7 +484,7 @@ extern "C" bfs_status bfs_boxcar_gather(const float* d_plane, int rows, int cols
     if (st != BFS_OK) return st;
     *h_count = count;
     const unsigned n = count < capacity ? count : capacity;
-    st = sort_candidates_canonical(d_out, n, rows, cols, widths_mode, s);
+    st = sort_candidates_canonical(d_out, n, rows, cols, widths_mode, param, s);
     if (st != BFS_OK) return st;
     if (count > capacity)
         return fail(BFS_ERR_OVERFLOW, "%u candidates found, capacity %u", count, capacity);

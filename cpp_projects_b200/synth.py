@@ -68,6 +68,15 @@ def config0(seed: int = 1) -> Beam:
     return Beam(512, 32768, 1200.0, 1600.0, 512, seed, [Pulse(10000, 256.0, 4, 2.0)])
 
 
+def config4(seed: int = 4) -> Beam:
+    """1024 ch x 65536 samples, 1200-1600 MHz, max delay 1024, N(0,1) noise
+    plus 8 injected pulses (the forward shape of the differentiable-FDMT case)."""
+    rng = np.random.default_rng(seed)
+    pulses = [Pulse(int(rng.integers(0, 60000)), float(rng.uniform(0.1, 0.9) * 1023),
+                    int(rng.integers(1, 33)), float(rng.uniform(1.0, 3.0))) for _ in range(8)]
+    return Beam(1024, 65536, 1200.0, 1600.0, 1024, seed, pulses)
+
+
 CONFIG0_SEARCH = dict(widths_mode=0, param=5, thr=7.0, metrics=(16, 8, 1 << 30))
 
 

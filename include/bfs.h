@@ -42,6 +42,10 @@ typedef struct bfs_cand {
 
 const char* bfs_last_error(void);
 const char* bfs_version(void);
+/* Calls that need temporary device memory take it from the current device's
+ * stream-ordered default pool, set to keep freed memory for reuse; this
+ * returns the pool's unused memory to the system. */
+bfs_status bfs_trim_scratch(void);
 
 /* ------------------------------------------------------------------------
  * FDMT
