@@ -39,6 +39,13 @@ class FdmtInfo(ctypes.Structure):
                 ("workspace_bytes", ctypes.c_size_t), ("alg_bytes", ctypes.c_double)]
 
 
+class ChunkDesc(ctypes.Structure):
+    _fields_ = [("fmin", ctypes.c_float), ("fmax", ctypes.c_float), ("npol", ctypes.c_int),
+                ("nchan", ctypes.c_int), ("len_sft", ctypes.c_int), ("nbin", ctypes.c_int),
+                ("nfft", ctypes.c_int), ("noverlap", ctypes.c_int), ("tsamp", ctypes.c_float),
+                ("max_dt", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+
+
 class Cand(ctypes.Structure):
     _fields_ = [("mt", ctypes.c_int), ("mdt", ctypes.c_int), ("mwidth", ctypes.c_int),
                 ("msnr", ctypes.c_float)]
@@ -76,6 +83,15 @@ _SIGNATURES = {
                                ctypes.POINTER(_U32), _P]),
     "bfs_cluster": (_I, [_P, _U32, _P, _P, _P, _P, ctypes.POINTER(_U32), _P]),
     "bfs_select_delegates": (_I, [_P, _P, _U32, _P, _U32, _P, _P]),
+    "bfs_chunk_create": (_I, [ctypes.POINTER(ChunkDesc), ctypes.POINTER(_P)]),
+    "bfs_chunk_destroy": (_I, [_P]),
+    "bfs_chunk_info": (_I, [_P, _P, _I]),
+    "bfs_chunk_coherent_dms": (_I, [ctypes.c_double, ctypes.c_double, _I, _P, _I]),
+    "bfs_chunk_unpack": (_I, [_P, _P, _P, _P]),
+    "bfs_chunk_forward_fft": (_I, [_P, _P, _P]),
+    "bfs_chunk_voltages": (_I, [_P, _P, ctypes.c_double, _P, _P]),
+    "bfs_chunk_detect": (_I, [_P, _P, ctypes.c_double, _P, _P]),
+    "bfs_chunk_process": (_I, [_P, _P, _P, _I, _P, _P]),
 }
 
 _lib = None

@@ -35,7 +35,7 @@ COMMON_INC = [f"-I{INCLUDE}", f"-I{CSRC}", f"-I{CUDA_HOME / 'include'}"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
                      "-Xcompiler", "-fPIC,-ffp-contract=off", "-Xptxas", "-warn-spills"]
 CXX_FLAGS = ["-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-Wall"]
-LINK_LIBS: list[str] = []
+LINK_LIBS = ["-lcufft", "-Xlinker", f"-rpath,{CUDA_HOME / 'lib64'}"]
 
 
 def _sources():

@@ -1,0 +1,334 @@
+// Coherent-dedispersion chunk stage on sm_100a.
+//
+// Reference chain (L/CDMT): CSession_guppi_gpu::unpack_chunk
+// (Session_guppi_gpu.cu:53-60,117-141) -> CChunk_gpu::process (Chunk_gpu.cu:254-460):
+// forward C2C FFT of every nbin-sample segment, then per coherent DM the chirp
+// multiply (CChunk_fly_gpu::elementWiseMult, Chunk_fly_gpu.cu:94-163), inverse
+// C2C FFTs of length mbin = nbin / len_sft, power detection summed over
+// polarisations with a roll by nbin/2 (roll_rows_normalize_sum_kernel,
+// Chunk_gpu.cu:476-494), unpadding + frequency reversal into a fine-channel
+// plane (transpose_unpadd_intensity, :497-516), a per-row circular
+// dedispersion shift (dedisperse, :613-632), statistical preprocessing, the
+// FDMT of the mask and of the data, and fdmt_normalization (:327-359).
+//
+// Layouts (the reference's): raw GUPPI chunk int8 [coarse chan][sample][npol]
+// with npol bytes per sample = (re, im) per polarisation; spectra / voltages
+// complex64 [pol][fft][coarse chan][nbin]; the FDMT input plane float32
+// [fine channel, highest frequency first][msamp].
+//
+// Differences in form: detection, roll, unpadding, reversal and the
+// dedispersion shift are ONE gather kernel here (one read of the voltages,
+// one write of the plane) instead of three passes; the FFTs are cuFFT with
+// the reference's sizes; the chirp phase is FP64 (modf before sincospi) and
+// the complex multiply FP32 without FMA contraction.
+#include <cufft.h>
+
+#include <cmath>
+#include <memory>
+#include <vector>
+
+#include "internal.h"
+
+struct bfs_chunk {
+    bfs_chunk_desc d;
+    int mbin = 0, nov_pc = 0, mbin_adj = 0, msamp = 0, rows = 0;
+    int64_t len_chunk = 0;   // samples per coarse channel in one chunk
+    int64_t cplx_len = 0;    // complex values of one spectrum / voltage buffer
+    cufftHandle fwd = 0, inv = 0;
+    bool have_fwd = false, have_inv = false;
+    bfs_fdmt_plan* fdmt = nullptr;
+    float2* volt = nullptr;  // chirped spectrum, then voltages, per DM
+    float* plane = nullptr;  // rows x msamp FDMT input
+    float* mask = nullptr;   // rows x msamp normalisation input
+    float* norm = nullptr;   // max_dt x msamp FDMT of the mask
+    float* buff = nullptr;   // 4 + 2 rows statistics
+    int* d_shift = nullptr;  // rows dedispersion shifts
+    ~bfs_chunk() {
+        if (have_fwd) cufftDestroy(fwd);
+        if (have_inv) cufftDestroy(inv);
+        if (fdmt) bfs_fdmt_plan_destroy(fdmt);
+        for (void* p : {static_cast<void*>(volt), static_cast<void*>(plane), static_cast<void*>(mask),
+                        static_cast<void*>(norm), static_cast<void*>(buff), static_cast<void*>(d_shift)})
+            if (p) cudaFree(p);
+    }
+};
+
+namespace bfs {
+namespace {
+
+constexpr double kDispersionConstant = 4.148808e9;  // MHz^2 pc^-1 cm^3 us (Chunk_fly_gpu.cu:139)
+
+// int8 GUPPI -> complex64 with overlap-save zero padding.  One thread per
+// (bin, fft, coarse channel); reads all polarisations of a sample at once.
+__global__ void k_unpack_guppi(const signed char* __restrict__ raw, float2* __restrict__ out,
+                               long long nsamp, int noverlap, int nbin, int nfft, int npol,
+                               int nchan) {
+    const int ibin = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ibin >= nbin) return;
+    const int ifft = blockIdx.y, ichan = blockIdx.z;
+    const long long isamp = static_cast<long long>(ibin) + static_cast<long long>(nbin - 2 * noverlap) * ifft - noverlap;
+    const bool valid = isamp >= 0 && isamp < nsamp;
+    const signed char* src = raw + (static_cast<long long>(ichan) * nsamp + (valid ? isamp : 0)) * npol;
+    for (int ipol = 0; ipol < npol / 2; ++ipol) {
+        const size_t o = (static_cast<size_t>(ipol) * nfft * nchan + static_cast<size_t>(ifft) * nchan + ichan) * nbin + ibin;
+        float2 v = make_float2(0.0f, 0.0f);
+        if (valid) v = make_float2(static_cast<float>(src[2 * ipol]), static_cast<float>(src[2 * ipol + 1]));
+        out[o] = v;
+    }
+}
+
+// Chirp: one thread per (bin of the mbin sub-band, sub-band, coarse channel);
+// the factor is evaluated in FP64 and applied to every polarisation and FFT
+// segment at the fft-shifted position of the nbin spectrum.
+__global__ void k_chirp(const float2* __restrict__ in, float2* __restrict__ out, double dm, int nchan,
+                        int len_sft, int mbin, int nbin, int nseg, double fmin, double bw_sub,
+                        double bw_chan) {
+    const int ibin = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ibin >= mbin) return;
+    const int isft = blockIdx.y, ichan = blockIdx.z;
+    // centre of the fine channel, rounded to float as the reference stores it
+    const float f0 = static_cast<float>(fmin + bw_sub * (0.5 + ichan) +
+                                        bw_chan * (isft - len_sft / 2.0 + 0.5));
+    const double fb = -0.5 * bw_chan + (ibin + 0.5) * bw_chan / mbin;
+    const double taper = 1.0 / sqrt(1.0 + pow(fb / (0.47 * bw_chan), 80));
+    const double r = fb / static_cast<double>(f0);
+    const double phase = __dmul_rn(__dmul_rn(dm, r), r) / (static_cast<double>(f0) + fb) * kDispersionConstant;
+    double whole;
+    const double frac = -modf(phase, &whole) * 2.0;
+    double sn, cs;
+    sincospi(frac, &sn, &cs);
+    const float cx = static_cast<float>(cs * taper / static_cast<double>(nbin));
+    const float cy = static_cast<float>(sn * taper / static_cast<double>(nbin));
+    const size_t pos = static_cast<size_t>(ichan) * nbin + (isft * mbin + ibin + nbin / 2) % nbin;
+    const size_t stride = static_cast<size_t>(nbin) * nchan;
+    for (int i = 0; i < nseg; ++i) {
+        const float2 a = in[pos + i * stride];
+        float2 o;
+        o.x = __fsub_rn(__fmul_rn(a.x, cx), __fmul_rn(a.y, cy));
+        o.y = __fadd_rn(__fmul_rn(a.x, cy), __fmul_rn(a.y, cx));
+        out[pos + i * stride] = o;
+    }
+}
+
+// Power detection + roll by nbin/2 + unpadding + frequency reversal +
+// dedispersion shift, as one gather: output row r (fine channel, highest
+// frequency first), column c of the dedispersed plane.
+__global__ void k_detect(const float2* __restrict__ volt, float* __restrict__ plane, int nchan,
+                         int len_sft, int mbin, int nbin, int nfft, int npol2, int nov_pc,
+                         int mbin_adj, int msamp, const int* __restrict__ shift) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= msamp) return;
+    const int r = blockIdx.y;
+    int idx = (c - shift[r]) % msamp;     // dedisperse: out[(idx + s) % msamp] = in[idx]
+    if (idx < 0) idx += msamp;
+    const int isub = r / len_sft;
+    const int ifine = len_sft - 1 - (r % len_sft);
+    const int coarse = nchan - 1 - isub;
+    const int ifft = idx / mbin_adj;
+    const int ibin = idx % mbin_adj;
+    const int p = ifine * mbin + ibin + nov_pc;          // position in the rolled row
+    const int q = (p + nbin / 2) % nbin;                 // position before the roll
+    const size_t pol_stride = static_cast<size_t>(nfft) * nchan * nbin;
+    const size_t base = (static_cast<size_t>(ifft) * nchan + coarse) * nbin + q;
+    float acc = 0.0f;
+    for (int ipol = 0; ipol < npol2; ++ipol) {
+        const float2 v = volt[base + ipol * pol_stride];
+        const double x = v.x, y = v.y;
+        acc = __fadd_rn(acc, static_cast<float>((x * x + y * y) / nbin / nbin));
+    }
+    plane[static_cast<size_t>(r) * msamp + c] = acc;
+}
+
+bfs_status cufft_check(cufftResult r, const char* what) {
+    if (r == CUFFT_SUCCESS) return BFS_OK;
+    return fail(BFS_ERR_CUDA, "%s failed (cufftResult %d)", what, static_cast<int>(r));
+}
+
+}  // namespace
+}  // namespace bfs
+
+using namespace bfs;
+
+extern "C" int bfs_chunk_coherent_dms(double d_min, double d_max, int ncoherent, double* dms, int cap) {
+    // CChunkB::CChunkB (L/CDMT/ChunkB.cpp:171-176): step = d_max / ncoherent,
+    // count = (int)((d_max - d_min) / step), dm_i = d_min + i * step
+    if (ncoherent <= 0 || !(d_max > 0.0)) return 0;
+    const double step = d_max / ncoherent;
+    const int n = static_cast<int>((d_max - d_min) / step);
+    for (int i = 0; i < n && i < cap; ++i) dms[i] = d_min + i * step;
+    return n < 0 ? 0 : n;
+}
+
+extern "C" bfs_status bfs_chunk_create(const bfs_chunk_desc* desc, bfs_chunk** out) {
+    BFS_ARG(desc && out, "null argument");
+    *out = nullptr;
+    const bfs_chunk_desc& d = *desc;
+    BFS_ARG(d.npol == 2 || d.npol == 4, "npol must be 2 or 4 (got %d)", d.npol);
+    BFS_ARG(d.nchan >= 1 && d.len_sft >= 1 && d.nfft >= 1 && d.nbin >= 2, "bad chunk geometry");
+    BFS_ARG(d.nbin % d.len_sft == 0, "nbin must be a multiple of len_sft");
+    BFS_ARG(d.noverlap >= 0 && 2 * d.noverlap < d.nbin, "bad overlap");
+    BFS_ARG(d.tsamp > 0.0f && d.fmax > d.fmin && d.fmin > 0.0f, "bad band or sample time");
+    std::unique_ptr<bfs_chunk> c(new bfs_chunk);
+    c->d = d;
+    // CChunkB geometry (L/CDMT/ChunkB.h:77-98)
+    c->mbin = d.nbin / d.len_sft;
+    c->nov_pc = d.noverlap / d.len_sft;
+    c->mbin_adj = c->mbin - 2 * c->nov_pc;
+    BFS_ARG(c->mbin_adj > 0, "overlap leaves no samples per segment");
+    c->msamp = d.nfft * c->mbin_adj;
+    c->rows = d.nchan * d.len_sft;
+    c->len_chunk = static_cast<int64_t>(d.nbin - 2 * d.noverlap) * d.nfft;
+    c->cplx_len = static_cast<int64_t>(d.npol / 2) * d.nfft * d.nchan * d.nbin;
+    const int max_dt = d.max_dt > 0 ? d.max_dt : d.len_sft;
+    c->d.max_dt = max_dt;
+    // FFT plans with the reference's sizes (Chunk_gpu.cu:197-209)
+    int n = d.nbin;
+    {
+        bfs_status st = cufft_check(cufftPlanMany(&c->fwd, 1, &n, nullptr, 1, d.nbin, nullptr, 1, d.nbin,
+                                                  CUFFT_C2C, d.nfft * d.nchan * d.npol / 2),
+                                    "cufftPlanMany(forward)");
+        if (st != BFS_OK) return st;
+        c->have_fwd = true;
+        int m = c->mbin;
+        st = cufft_check(cufftPlanMany(&c->inv, 1, &m, nullptr, 1, c->mbin, nullptr, 1, c->mbin,
+                                       CUFFT_C2C, d.nfft * d.nchan * d.len_sft * d.npol / 2),
+                         "cufftPlanMany(inverse)");
+        if (st != BFS_OK) return st;
+        c->have_inv = true;
+    }
+    bfs_fdmt_desc fd{};
+    fd.fmin = d.fmin; fd.fmax = d.fmax; fd.nchan = c->rows; fd.ncols = c->msamp; fd.max_dt = max_dt;
+    fd.plan_kind = BFS_PLAN_KEITH; fd.precision = BFS_PREC_F32; fd.fuse_depth = -1;
+    bfs_status st = bfs_fdmt_plan_create(&fd, &c->fdmt);
+    if (st != BFS_OK) return st;
+    BFS_CUDA(cudaMalloc(&c->volt, sizeof(float2) * c->cplx_len));
+    BFS_CUDA(cudaMalloc(&c->plane, sizeof(float) * static_cast<size_t>(c->rows) * c->msamp));
+    BFS_CUDA(cudaMalloc(&c->mask, sizeof(float) * static_cast<size_t>(c->rows) * c->msamp));
+    BFS_CUDA(cudaMalloc(&c->norm, sizeof(float) * static_cast<size_t>(max_dt) * c->msamp));
+    BFS_CUDA(cudaMalloc(&c->buff, sizeof(float) * (4 + 2 * static_cast<size_t>(c->rows))));
+    BFS_CUDA(cudaMalloc(&c->d_shift, sizeof(int) * c->rows));
+    *out = c.release();
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_chunk_destroy(bfs_chunk* c) {
+    delete c;
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_chunk_info(const bfs_chunk* c, int64_t* info, int cap) {
+    BFS_ARG(c && info && cap >= 8, "need 8 entries");
+    info[0] = c->mbin; info[1] = c->nov_pc; info[2] = c->mbin_adj; info[3] = c->msamp;
+    info[4] = c->rows; info[5] = c->len_chunk; info[6] = c->cplx_len; info[7] = c->d.max_dt;
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_chunk_unpack(bfs_chunk* c, const int8_t* d_raw, void* d_cplx, void* stream) {
+    BFS_ARG(c && d_raw && d_cplx, "null argument");
+    const bfs_chunk_desc& d = c->d;
+    dim3 grid((d.nbin + 255) / 256, d.nfft, d.nchan);
+    BFS_ARG(grid.y <= 65535 && grid.z <= 65535, "too many segments or channels");
+    k_unpack_guppi<<<grid, 256, 0, as_stream(stream)>>>(reinterpret_cast<const signed char*>(d_raw),
+                                                         static_cast<float2*>(d_cplx), c->len_chunk,
+                                                         d.noverlap, d.nbin, d.nfft, d.npol, d.nchan);
+    BFS_LAUNCH_CHECK("k_unpack_guppi");
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_chunk_forward_fft(bfs_chunk* c, void* d_cplx, void* stream) {
+    BFS_ARG(c && d_cplx, "null argument");
+    bfs_status st = cufft_check(cufftSetStream(c->fwd, as_stream(stream)), "cufftSetStream");
+    if (st != BFS_OK) return st;
+    return cufft_check(cufftExecC2C(c->fwd, static_cast<cufftComplex*>(d_cplx),
+                                    static_cast<cufftComplex*>(d_cplx), CUFFT_FORWARD),
+                       "cufftExecC2C(forward)");
+}
+
+static bfs_status chunk_voltages(bfs_chunk* c, const void* d_spec, double dm, float2* d_volt,
+                                 cudaStream_t s) {
+    const bfs_chunk_desc& d = c->d;
+    // band arithmetic as in CChunk_fly_gpu::elementWiseMult (Chunk_fly_gpu.cu:96-99)
+    const double bw = static_cast<double>(d.fmax - d.fmin);
+    const double bw_sub = bw / d.nchan;
+    const double bw_chan = bw_sub / d.len_sft;
+    dim3 grid((c->mbin + 255) / 256, d.len_sft, d.nchan);
+    BFS_ARG(grid.y <= 65535 && grid.z <= 65535, "too many sub-bands or channels");
+    k_chirp<<<grid, 256, 0, s>>>(static_cast<const float2*>(d_spec), d_volt, dm, d.nchan, d.len_sft,
+                                 c->mbin, d.nbin, d.nfft * d.npol / 2, static_cast<double>(d.fmin),
+                                 bw_sub, bw_chan);
+    BFS_LAUNCH_CHECK("k_chirp");
+    bfs_status st = cufft_check(cufftSetStream(c->inv, s), "cufftSetStream");
+    if (st != BFS_OK) return st;
+    return cufft_check(cufftExecC2C(c->inv, reinterpret_cast<cufftComplex*>(d_volt),
+                                    reinterpret_cast<cufftComplex*>(d_volt), CUFFT_INVERSE),
+                       "cufftExecC2C(inverse)");
+}
+
+extern "C" bfs_status bfs_chunk_voltages(bfs_chunk* c, const void* d_spec, double dm, void* d_volt,
+                                         void* stream) {
+    BFS_ARG(c && d_spec && d_volt, "null argument");
+    return chunk_voltages(c, d_spec, dm, static_cast<float2*>(d_volt), as_stream(stream));
+}
+
+// Dedispersion shifts of the fine-channel rows (dedisperse, Chunk_gpu.cu:613-632):
+// row i has frequency fmin + (rows-1-i) * foff and moves by
+// round(4148.808 * dm * (fmin^-2 - f^-2) / (len_sft * tsamp)).
+static void chunk_shifts(const bfs_chunk* c, double dm, std::vector<int>& sh) {
+    const bfs_chunk_desc& d = c->d;
+    const double fmin = d.fmin;
+    const double foff = (static_cast<double>(d.fmax) - static_cast<double>(d.fmin)) / (d.nchan * d.len_sft);
+    const double tw = static_cast<double>(static_cast<float>(d.len_sft) * d.tsamp);
+    sh.resize(c->rows);
+    for (int i = 0; i < c->rows; ++i) {
+        const double f = static_cast<double>(c->rows - 1 - i) * foff + fmin;
+        const double delay = 4.148808e3 * dm * (1.0 / (fmin * fmin) - 1.0 / (f * f));
+        sh[i] = static_cast<int>(std::round(delay / tw));
+    }
+}
+
+static bfs_status chunk_detect(bfs_chunk* c, const float2* d_volt, double dm, float* d_plane,
+                               cudaStream_t s) {
+    std::vector<int> sh;
+    chunk_shifts(c, dm, sh);
+    BFS_CUDA(cudaMemcpyAsync(c->d_shift, sh.data(), sizeof(int) * sh.size(), cudaMemcpyHostToDevice, s));
+    const bfs_chunk_desc& d = c->d;
+    dim3 grid((c->msamp + 255) / 256, c->rows);
+    BFS_ARG(grid.y <= 65535, "too many fine channels");
+    k_detect<<<grid, 256, 0, s>>>(d_volt, d_plane, d.nchan, d.len_sft, c->mbin, d.nbin, d.nfft,
+                                  d.npol / 2, c->nov_pc, c->mbin_adj, c->msamp, c->d_shift);
+    BFS_LAUNCH_CHECK("k_detect");
+    // the host vector must outlive the (pageable, staged) copy: wait for it
+    BFS_CUDA(cudaStreamSynchronize(s));
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_chunk_detect(bfs_chunk* c, const void* d_volt, double dm, float* d_plane,
+                                       void* stream) {
+    BFS_ARG(c && d_volt && d_plane, "null argument");
+    return chunk_detect(c, static_cast<const float2*>(d_volt), dm, d_plane, as_stream(stream));
+}
+
+extern "C" bfs_status bfs_chunk_process(bfs_chunk* c, void* d_cplx, const double* dms, int ndm,
+                                        float* d_out, void* stream) {
+    BFS_ARG(c && d_cplx && d_out && (ndm == 0 || dms), "null argument");
+    cudaStream_t s = as_stream(stream);
+    bfs_status st = bfs_chunk_forward_fft(c, d_cplx, stream);
+    if (st != BFS_OK) return st;
+    const size_t plane_out = static_cast<size_t>(c->d.max_dt) * c->msamp;
+    for (int i = 0; i < ndm; ++i) {
+        st = chunk_voltages(c, d_cplx, dms[i], c->volt, s);
+        if (st != BFS_OK) return st;
+        st = chunk_detect(c, c->volt, dms[i], c->plane, s);
+        if (st != BFS_OK) return st;
+        st = bfs_preproc_calc_fdmt_inputs(c->plane, c->rows, c->msamp, c->buff, c->mask, stream);
+        if (st != BFS_OK) return st;
+        st = bfs_fdmt_execute(c->fdmt, c->mask, c->norm, 0, stream);
+        if (st != BFS_OK) return st;
+        float* out = d_out + i * plane_out;
+        st = bfs_fdmt_execute(c->fdmt, c->plane, out, 0, stream);
+        if (st != BFS_OK) return st;
+        st = bfs_fdmt_normalize(out, c->norm, static_cast<int64_t>(plane_out), out, stream);
+        if (st != BFS_OK) return st;
+    }
+    return BFS_OK;
+}

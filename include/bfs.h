@@ -204,6 +204,62 @@ bfs_status bfs_select_delegates(const bfs_cand* d_cands, const int* d_perm, uint
                                 const int* d_offsets, uint32_t ngroups, int* d_delegates,
                                 void* stream);
 
+/* ------------------------------------------------------------------------
+ * Coherent-dedispersion chunk stage.
+ * Replaces CSession_guppi_gpu::unpack_chunk (L/CDMT/Session_guppi_gpu.cu:53-60,
+ * 117-141) and CChunk_gpu / CChunk_fly_gpu::process (L/CDMT/Chunk_gpu.cu:134-460,
+ * L/CDMT/Chunk_fly_gpu.cu:94-163) with the CChunkB geometry
+ * (L/CDMT/ChunkB.h:77-98): mbin = nbin/len_sft, noverlap_per_channel =
+ * noverlap/len_sft, mbin_adjusted = mbin - 2*noverlap_per_channel,
+ * msamp = nfft*mbin_adjusted, rows = nchan*len_sft.
+ * Buffers: raw chunk int8 [nchan][len_chunk][npol] with len_chunk =
+ * (nbin - 2*noverlap)*nfft; spectra/voltages complex64 (float2)
+ * [npol/2][nfft][nchan][nbin]; planes float32 [rows][msamp], row 0 = highest
+ * frequency (the reference's reversed order).
+ * ---------------------------------------------------------------------- */
+typedef struct bfs_chunk_desc {
+    float fmin;        /* MHz, band edges (CChunkB m_Fmin / m_Fmax)            */
+    float fmax;
+    int npol;          /* 2 = one complex polarisation, 4 = two                */
+    int nchan;         /* coarse channels                                      */
+    int len_sft;       /* fine channels per coarse channel                     */
+    int nbin;          /* forward FFT length                                   */
+    int nfft;          /* FFT segments per chunk                               */
+    int noverlap;      /* overlap-save samples on each side of a segment       */
+    float tsamp;       /* coarse-channel sample time, seconds                  */
+    int max_dt;        /* FDMT output rows (0 = len_sft, the reference's value) */
+    int reserved[6];
+} bfs_chunk_desc;
+
+typedef struct bfs_chunk bfs_chunk;
+
+bfs_status bfs_chunk_create(const bfs_chunk_desc* desc, bfs_chunk** chunk);
+bfs_status bfs_chunk_destroy(bfs_chunk* chunk);
+/* info[0..7] = mbin, noverlap_per_channel, mbin_adjusted, msamp, rows,
+ * len_chunk, complex values per buffer, max_dt */
+bfs_status bfs_chunk_info(const bfs_chunk* chunk, int64_t* info, int cap);
+/* Coherent-DM grid of CChunkB::CChunkB (L/CDMT/ChunkB.cpp:171-176); returns the count. */
+int bfs_chunk_coherent_dms(double d_min, double d_max, int ncoherent, double* dms, int cap);
+/* GUPPI unpack with overlap-save zero padding (unpack_chunk_guppi_gpu). */
+bfs_status bfs_chunk_unpack(bfs_chunk* chunk, const int8_t* d_raw, void* d_cplx, void* stream);
+/* In-place forward FFT of every segment (Chunk_gpu.cu:267). */
+bfs_status bfs_chunk_forward_fft(bfs_chunk* chunk, void* d_cplx, void* stream);
+/* Coherently dedispersed voltages for one DM: chirp (FP64 phase) + inverse
+ * FFTs of length mbin (Chunk_fly_gpu.cu:94-163, Chunk_gpu.cu:284-288).
+ * d_spec is not modified. */
+bfs_status bfs_chunk_voltages(bfs_chunk* chunk, const void* d_spec, double dm, void* d_volt,
+                              void* stream);
+/* Power detection + roll + unpadding + frequency reversal + dedispersion shift
+ * (Chunk_gpu.cu:296-321) into a rows x msamp plane.  Synchronises `stream`. */
+bfs_status bfs_chunk_detect(bfs_chunk* chunk, const void* d_volt, double dm, float* d_plane,
+                            void* stream);
+/* CChunkB::process (L/CDMT/ChunkB.h:73-74): forward FFT of d_cplx (in place,
+ * overwritten like the reference's), then per DM voltages, detection,
+ * statistical preprocessing, FDMT of mask and data and fdmt_normalization into
+ * d_out[i] (max_dt x msamp each). */
+bfs_status bfs_chunk_process(bfs_chunk* chunk, void* d_cplx, const double* dms, int ndm,
+                             float* d_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

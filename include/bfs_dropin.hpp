@@ -1,0 +1,195 @@
+// bfs_dropin.hpp — header-only C++ shims with the reference's own names and
+// signatures, implemented on the C ABI in bfs.h.  A reference call site keeps
+// compiling unchanged: include this header instead of FdmtGpu.cuh,
+// Statistical_preprocessing.cuh and Clusterization.cuh, and link libbfs_b200.
+//
+//   CFdmtGpu                      L/FDMT/FdmtGpu.cuh:5-53
+//   statistical_preprocessing::   L/CDMT/Statistical_preprocessing.cuh:9-10
+//   clusterization::              L/Clusterization/Clusterization.cuh:10-67
+//   select_delegates::write_log   L/Clusterization/select_delegates.cu:127-177
+// (L = MyVSLib_C++).  As in the reference, pointers are device pointers,
+// work runs on the default stream and errors are printed to stderr; the
+// extra last_status() reports the bfs_status of the last call.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <fstream>
+#include <iomanip>
+#include <string>
+#include <vector>
+
+#include "bfs.h"
+
+#ifndef fdmt_type_
+#define fdmt_type_ float
+#endif
+
+using Cand = bfs_cand;  // same 16-byte layout as the reference's SCand
+
+namespace bfs_dropin_detail {
+inline bfs_status report(bfs_status st, const char* where) {
+    if (st != BFS_OK) std::fprintf(stderr, "%s failed: %s\n", where, bfs_last_error());
+    return st;
+}
+}  // namespace bfs_dropin_detail
+
+class CFdmtGpu {
+public:
+    CFdmtGpu() = default;
+    CFdmtGpu(const float Fmin, const float Fmax, int nchan, const int cols, int imaxDt)
+        : m_nchan(nchan), m_cols(cols), m_Fmin(Fmin), m_Fmax(Fmax), m_imaxDt(imaxDt) {
+        bfs_fdmt_desc d{};
+        d.fmin = Fmin; d.fmax = Fmax; d.nchan = nchan; d.ncols = cols; d.max_dt = imaxDt;
+        d.plan_kind = BFS_PLAN_KEITH; d.precision = BFS_PREC_F32; d.fuse_depth = -1;
+        m_status = bfs_dropin_detail::report(bfs_fdmt_plan_create(&d, &m_plan), "CFdmtGpu");
+        if (m_plan) {
+            bfs_fdmt_info info{};
+            bfs_fdmt_plan_info(m_plan, &info);
+            m_iNumIter = info.niter;
+        }
+    }
+    CFdmtGpu(const CFdmtGpu& R) : CFdmtGpu(R.m_Fmin, R.m_Fmax, R.m_nchan, R.m_cols, R.m_imaxDt) {}
+    CFdmtGpu& operator=(const CFdmtGpu& R) {
+        if (this != &R) {
+            CFdmtGpu tmp(R);
+            std::swap(m_plan, tmp.m_plan);
+            m_nchan = R.m_nchan; m_cols = R.m_cols; m_Fmin = R.m_Fmin; m_Fmax = R.m_Fmax;
+            m_imaxDt = R.m_imaxDt; m_iNumIter = R.m_iNumIter; m_status = tmp.m_status;
+        }
+        return *this;
+    }
+    ~CFdmtGpu() { if (m_plan) bfs_fdmt_plan_destroy(m_plan); }
+
+    // d_parrImage: nchan x cols on the device; u_parrImOut: imaxDt x cols.
+    void process_image(fdmt_type_* d_parrImage, fdmt_type_* u_parrImOut, const bool b_ones) {
+        if (!m_plan) { m_status = BFS_ERR_ARG; std::fprintf(stderr, "CFdmtGpu: no plan\n"); return; }
+        m_status = bfs_dropin_detail::report(
+            bfs_fdmt_execute(m_plan, d_parrImage, u_parrImOut, b_ones ? 1 : 0, nullptr),
+            "CFdmtGpu::process_image");
+    }
+    bfs_status last_status() const { return m_status; }
+
+    int m_nchan = 0, m_cols = 0;
+    float m_Fmin = 0, m_Fmax = 0;
+    int m_imaxDt = 0, m_iNumIter = 0;
+
+private:
+    bfs_fdmt_plan* m_plan = nullptr;
+    bfs_status m_status = BFS_OK;
+};
+
+namespace statistical_preprocessing {
+inline void calc_fdmt_inputs(float* d_parr_inp, const int NRows, const int NCols, float* d_buff,
+                             float* d_parrNormInput) {
+    bfs_dropin_detail::report(
+        bfs_preproc_calc_fdmt_inputs(d_parr_inp, NRows, NCols, d_buff, d_parrNormInput, nullptr),
+        "calc_fdmt_inputs");
+}
+}  // namespace statistical_preprocessing
+
+namespace select_delegates {
+// Delegate log, the reference's columns and widths.  h_delegates are
+// candidate indices sorted by mt; h_offsets the group starts (ngroups + 1).
+inline void write_log(const std::vector<Cand>& h_cands, const std::vector<int>& h_offsets,
+                      const std::vector<int>& h_delegates, const std::string& filename,
+                      const float delt_bin, const float t_chunkBegin) {
+    std::ofstream log(filename);
+    log << std::setw(10) << "N" << std::setw(10) << "t, bin" << std::setw(10) << "t, sec"
+        << std::setw(10) << "dedisp" << std::setw(10) << "width" << std::setw(10) << "SNR"
+        << std::setw(10) << "num" << std::endl;
+    for (size_t i = 0; i < h_delegates.size(); ++i) {
+        const Cand c = h_cands[h_delegates[i]];
+        // the reference pairs the i-th delegate with the i-th group's size
+        const int num = h_offsets[i + 1] - h_offsets[i];
+        log << std::setw(10) << i + 1 << std::setw(10) << c.mt << std::setw(10)
+            << t_chunkBegin + c.mt * delt_bin << std::setw(10) << c.mdt << std::setw(10)
+            << c.mwidth << std::setw(10) << c.msnr << std::setw(10) << num << std::endl;
+    }
+}
+}  // namespace select_delegates
+
+namespace clusterization {
+
+// Boxcar gather into a freshly cudaMalloc'd array the caller frees (the
+// reference's ownership rule).  val_thresh is a reference to device memory.
+inline bool gather_(const float* d_plane, int Rows, int Cols, const float& val_thresh, int mode,
+                    int param, Cand** d_out, unsigned int* h_count) {
+    *d_out = nullptr;
+    *h_count = 0;
+    uint32_t cap = 1u << 16, n = 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        Cand* buf = nullptr;
+        if (cudaMalloc(reinterpret_cast<void**>(&buf), sizeof(Cand) * (cap ? cap : 1)) != cudaSuccess) {
+            std::fprintf(stderr, "gather: cudaMalloc failed\n");
+            return false;
+        }
+        const bfs_status st = bfs_boxcar_gather(d_plane, Rows, Cols, nullptr, 0.0f, &val_thresh, mode,
+                                                param, 0, buf, cap, &n, nullptr);
+        if (st == BFS_OK) { *d_out = buf; *h_count = n; return true; }
+        cudaFree(buf);
+        if (st != BFS_ERR_OVERFLOW) { bfs_dropin_detail::report(st, "gather"); return false; }
+        cap = n;  // retry with the exact count
+    }
+    return false;
+}
+
+inline void gather_candidates_in_dynamicalArray(const float* d_arr_fdmt, const int Rows, const int Cols,
+                                                const float& val_thresh, const int QUantPower2_Wnd,
+                                                Cand** d_arrCand, unsigned int* h_pquantCand) {
+    gather_(d_arr_fdmt, Rows, Cols, val_thresh, BFS_WIDTHS_POW2, QUantPower2_Wnd, d_arrCand,
+            h_pquantCand);
+}
+
+inline bool gather_candidates_in_heap_with_plan(const float* d_fdmt, const int Rows, const int Cols,
+                                                const float& d_VAlTresh, const int WndWidth,
+                                                Cand** d_pparrCand, unsigned int* h_piQuantCand) {
+    return gather_(d_fdmt, Rows, Cols, d_VAlTresh, BFS_WIDTHS_ALL, WndWidth, d_pparrCand,
+                   h_piQuantCand) && *h_piQuantCand > 0;
+}
+
+// d_pbin_metrics: 3 ints in device memory (as in the reference).
+inline void complete_clusterization(const Cand* d_parrCand, unsigned int quant_candidates,
+                                    const int* d_pbin_metrics, const std::string& filename,
+                                    const float delt_bin, const float t_chunkBegin, bool bwrite) {
+    if (quant_candidates == 0) return;
+    int metrics[3];
+    cudaMemcpy(metrics, d_pbin_metrics, sizeof(metrics), cudaMemcpyDeviceToHost);
+    int *perm = nullptr, *offsets = nullptr, *dl = nullptr;
+    cudaMalloc(reinterpret_cast<void**>(&perm), sizeof(int) * quant_candidates);
+    cudaMalloc(reinterpret_cast<void**>(&offsets), sizeof(int) * (quant_candidates + 1));
+    cudaMalloc(reinterpret_cast<void**>(&dl), sizeof(int) * quant_candidates);
+    uint32_t ng = 0;
+    const bfs_status st = bfs_cluster(d_parrCand, quant_candidates, metrics, perm, offsets, dl, &ng,
+                                      nullptr);
+    if (bfs_dropin_detail::report(st, "complete_clusterization") == BFS_OK && bwrite) {
+        std::vector<Cand> c(quant_candidates);
+        std::vector<int> o(ng + 1), d(ng);
+        cudaMemcpy(c.data(), d_parrCand, sizeof(Cand) * quant_candidates, cudaMemcpyDeviceToHost);
+        cudaMemcpy(o.data(), offsets, sizeof(int) * (ng + 1), cudaMemcpyDeviceToHost);
+        cudaMemcpy(d.data(), dl, sizeof(int) * ng, cudaMemcpyDeviceToHost);
+        select_delegates::write_log(c, o, d, filename, delt_bin, t_chunkBegin);
+    }
+    cudaFree(perm);
+    cudaFree(offsets);
+    cudaFree(dl);
+}
+
+inline bool clusterization_main(const float* d_digitized_fdmt, const int Rows, const int Cols,
+                                const float& d_VAlTresh, const int WndWidth,
+                                const int* d_pbin_metrics, const std::string& filename,
+                                const float delt_bin, const float t_chunkBegin, bool bwrite = true) {
+    Cand* d_cands = nullptr;
+    unsigned int n = 0;
+    if (!gather_candidates_in_heap_with_plan(d_digitized_fdmt, Rows, Cols, d_VAlTresh, WndWidth,
+                                             &d_cands, &n)) {
+        if (d_cands) cudaFree(d_cands);
+        return false;
+    }
+    complete_clusterization(d_cands, n, d_pbin_metrics, filename, delt_bin, t_chunkBegin, bwrite);
+    cudaFree(d_cands);
+    return true;
+}
+
+}  // namespace clusterization

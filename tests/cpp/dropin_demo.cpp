@@ -1,0 +1,48 @@
+// A reference-style driver written against the reference's own names
+// (CFdmtGpu, clusterization::clusterization_main), compiled with
+// include/bfs_dropin.hpp instead of the reference headers.
+//   dropin_demo <fdmt_in.bin> <fdmt_out.bin> <log file>
+// Reads a 64 x 1024 float32 filterbank, writes its FDMT (1200-1600 MHz,
+// max delay 64), then runs clusterization_main on the reference's 3 x 16 test
+// plane (clusterization_forpravir/clusterization_test.cu:63-112) with W = 2,
+// threshold 4 and metrics {2, 1, 2}.
+#include <cstdio>
+#include <vector>
+
+#include "bfs_dropin.hpp"
+
+int main(int argc, char** argv) {
+    if (argc != 4) { std::fprintf(stderr, "usage: %s in.bin out.bin log\n", argv[0]); return 2; }
+    const int nchan = 64, cols = 1024, maxdt = 64;
+    std::vector<float> in(nchan * cols), out(maxdt * cols);
+    FILE* f = std::fopen(argv[1], "rb");
+    if (!f || std::fread(in.data(), sizeof(float), in.size(), f) != in.size()) return 3;
+    std::fclose(f);
+    float *d_in = nullptr, *d_out = nullptr;
+    cudaMalloc(reinterpret_cast<void**>(&d_in), in.size() * sizeof(float));
+    cudaMalloc(reinterpret_cast<void**>(&d_out), out.size() * sizeof(float));
+    cudaMemcpy(d_in, in.data(), in.size() * sizeof(float), cudaMemcpyHostToDevice);
+    CFdmtGpu fdmt(1200.0f, 1600.0f, nchan, cols, maxdt);
+    fdmt.process_image(d_in, d_out, false);
+    cudaMemcpy(out.data(), d_out, out.size() * sizeof(float), cudaMemcpyDeviceToHost);
+    if (fdmt.last_status() != BFS_OK) return 4;
+    f = std::fopen(argv[2], "wb");
+    std::fwrite(out.data(), sizeof(float), out.size(), f);
+    std::fclose(f);
+
+    const int rows = 3, pc = 16;
+    std::vector<float> plane(rows * pc, 2.0f);
+    plane[4] = 140.0f; plane[11] = 120.0f; plane[2 * pc + 4] = 100.0f;
+    float* d_plane = nullptr; float* d_thr = nullptr; int* d_metrics = nullptr;
+    cudaMalloc(reinterpret_cast<void**>(&d_plane), plane.size() * sizeof(float));
+    cudaMalloc(reinterpret_cast<void**>(&d_thr), sizeof(float));
+    cudaMalloc(reinterpret_cast<void**>(&d_metrics), 3 * sizeof(int));
+    const float thr = 4.0f; const int metrics[3] = {2, 1, 2};
+    cudaMemcpy(d_plane, plane.data(), plane.size() * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_thr, &thr, sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_metrics, metrics, sizeof(metrics), cudaMemcpyHostToDevice);
+    const bool found = clusterization::clusterization_main(d_plane, rows, pc, *d_thr, 2, d_metrics,
+                                                           argv[3], 0.00001f, 0.0f);
+    cudaFree(d_in); cudaFree(d_out); cudaFree(d_plane); cudaFree(d_thr); cudaFree(d_metrics);
+    return found ? 0 : 5;
+}

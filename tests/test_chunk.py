@@ -1,0 +1,142 @@
+"""Coherent-dedispersion chunk stage: the GUPPI unpack, FFTs + FP64 chirp,
+the fused detect/roll/unpad/reverse/dedisperse gather and the full
+CChunkB::process chain, against the FP64 oracle (oracle/chunk_oracle.py).
+
+Tolerances: unpack and the detect gather are exact (the gather is checked on
+the GPU's own voltages with the reference's float rounding of each
+polarisation's power); cuFFT + chirp against FP64 numpy within 1e-5 of the
+largest magnitude (north star: voltages within 1e-5 relative)."""
+import numpy as np
+import pytest
+import torch
+
+from cpp_projects_b200.chunk import CChunk_gpu, coherent_dms
+from oracle import chunk_oracle as co
+from oracle import pyoracle
+
+GEO = dict(fmin=1200.0, fmax=1232.0, npol=4, nchan=8, len_sft=8, nbin=4096, nfft=2,
+           noverlap=64, tsamp=0.25e-6, max_dt=16)
+DM = 56.8
+
+
+def _chunk():
+    g = GEO
+    return CChunk_gpu(g["fmin"], g["fmax"], g["npol"], g["nchan"], g["len_sft"], 0, 0, 0.0, 0.0, 1,
+                      6.0, 1, g["nbin"], g["nfft"], g["noverlap"], g["tsamp"], max_dt=g["max_dt"],
+                      dms=[0.0, DM])
+
+
+def _geo():
+    return co.Geometry(**GEO)
+
+
+def _raw(seed=3):
+    g = _geo()
+    return np.random.default_rng(seed).integers(-8, 8, size=(g.nchan, g.len_chunk, g.npol),
+                                                dtype=np.int8)
+
+
+def test_coherent_dm_grid_matches_reference_rule():
+    # CChunkB: step = d_max / ncoherent, count = (int)((d_max - d_min) / step)
+    assert list(coherent_dms(0.0, 100.0, 4)) == [0.0, 25.0, 50.0, 75.0]
+    assert list(coherent_dms(30.0, 50.0, 5)) == [30.0, 40.0]
+    assert len(coherent_dms(0.0, 0.0, 3)) == 0
+
+
+def test_oracle_coherent_dedispersion_compacts_a_dispersed_pulse():
+    g = co.Geometry(1200.0, 1216.0, 2, 4, 4, 8192, 1, 512, 0.25e-6, 8)
+    raw = co.dispersed_pulse_raw(g, 300.0, 3000, 6.0, noise=0.5)
+    spec = co.forward_fft(co.unpack(g, raw))
+    p_right = co.detect(g, co.voltages(g, spec, 300.0), 0.0).max()
+    p_zero = co.detect(g, co.voltages(g, spec, 0.0), 0.0).max()
+    assert p_right > 3 * p_zero
+
+
+@pytest.mark.gpu
+def test_unpack_exact(cuda):
+    ch, g = _chunk(), _geo()
+    raw = _raw()
+    d = ch.complex_buffer(cuda)
+    ch.unpack(torch.from_numpy(raw).to(cuda), d)
+    got = d.cpu().numpy().view(np.complex64).reshape(g.npol // 2, g.nfft, g.nchan, g.nbin)
+    np.testing.assert_array_equal(got, co.unpack(g, raw).astype(np.complex64))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dm", [0.0, DM])
+def test_voltages_within_1e5_of_fp64(cuda, dm):
+    ch, g = _chunk(), _geo()
+    raw = _raw()
+    d = ch.complex_buffer(cuda)
+    ch.unpack(torch.from_numpy(raw).to(cuda), d)
+    ch.forward_fft(d)
+    v = ch.complex_buffer(cuda)
+    ch.voltages(d, dm, v)
+    got = v.cpu().numpy().view(np.complex64).reshape(g.npol // 2, g.nfft, g.nchan, g.nbin)
+    want = co.voltages(g, co.forward_fft(co.unpack(g, raw)), dm)
+    err = np.abs(got - want).max() / np.abs(want).max()
+    print(f"voltages dm={dm}: max |err| / max |v| = {err:.2e}")
+    assert err < 1e-5
+
+
+@pytest.mark.gpu
+def test_detect_gather_exact_and_plane_within_1e5(cuda):
+    ch, g = _chunk(), _geo()
+    raw = _raw()
+    d = ch.complex_buffer(cuda)
+    ch.unpack(torch.from_numpy(raw).to(cuda), d)
+    ch.forward_fft(d)
+    v = ch.complex_buffer(cuda)
+    ch.voltages(d, DM, v)
+    plane = torch.empty((g.rows, g.msamp), device=cuda)
+    ch.detect(v, DM, plane)
+    got = plane.cpu().numpy()
+    volt = v.cpu().numpy().view(np.complex64).reshape(g.npol // 2, g.nfft, g.nchan, g.nbin)
+    exact = co.detect(g, volt, DM, float32_power=True)
+    assert np.array_equal(got, exact)
+    fp64 = co.detect(g, co.voltages(g, co.forward_fft(co.unpack(g, raw)), DM), DM)
+    assert np.abs(got - fp64).max() / np.abs(fp64).max() < 1e-5
+
+
+@pytest.mark.gpu
+def test_process_chain_matches_oracle(cuda):
+    ch, g = _chunk(), _geo()
+    raw = _raw(7)
+    d = ch.complex_buffer(cuda)
+    ch.unpack(torch.from_numpy(raw).to(cuda), d)
+    spec_copy = ch.complex_buffer(cuda)
+    planes = ch.process(d)                      # overwrites d with its FFT, like the reference
+    assert planes.shape == (2, g.max_dt, g.msamp)
+    # oracle chain on the GPU's own detection planes
+    d2 = ch.complex_buffer(cuda)
+    ch.unpack(torch.from_numpy(raw).to(cuda), d2)
+    ch.forward_fft(d2)
+    for i, dm in enumerate([0.0, DM]):
+        ch.voltages(d2, dm, spec_copy)
+        plane = torch.empty((g.rows, g.msamp), device=cuda)
+        ch.detect(spec_copy, dm, plane)
+        x, mask, _ = pyoracle.calc_fdmt_inputs(plane.cpu().numpy())
+        fd = pyoracle.fdmt_f32(g.fmin, g.fmax, x, g.rows, g.msamp, g.max_dt)
+        nm = pyoracle.fdmt_f32(g.fmin, g.fmax, mask, g.rows, g.msamp, g.max_dt)
+        want = pyoracle.fdmt_normalize(fd, nm)
+        got = planes[i].cpu().numpy()
+        assert np.abs(got - want).max() <= 1e-5 * max(1.0, np.abs(want).max())
+
+
+@pytest.mark.gpu
+def test_dispersed_pulse_recovered_at_its_dm(cuda):
+    g = co.Geometry(1200.0, 1216.0, 2, 4, 4, 8192, 1, 512, 0.25e-6, 8)
+    ch = CChunk_gpu(1200.0, 1216.0, 2, 4, 4, 0, 0, 0.0, 0.0, 1, 6.0, 1, 8192, 1, 512, 0.25e-6,
+                    max_dt=8, dms=[0.0, 300.0])
+    raw = co.dispersed_pulse_raw(g, 300.0, 3000, 6.0, noise=0.5)
+    d = ch.complex_buffer(cuda)
+    ch.unpack(torch.from_numpy(raw).to(cuda), d)
+    ch.forward_fft(d)
+    peaks = []
+    for dm in (0.0, 300.0):
+        v = ch.complex_buffer(cuda)
+        ch.voltages(d, dm, v)
+        plane = torch.empty((g.rows, g.msamp), device=cuda)
+        ch.detect(v, 0.0, plane)
+        peaks.append(float(plane.max()))
+    assert peaks[1] > 3 * peaks[0]
