@@ -54,6 +54,7 @@ def parse_args(argv=None):
     ap.add_argument("--workload", choices=["config2", "config0", "config4fwd"], default="config2")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true")
     return ap.parse_args(argv)
 
 
@@ -154,6 +155,55 @@ def cpu_reference_leg(beams, max_seconds: float = 15.0, min_steps: int = 1):
               f"{'reference CFdmtCpu' if ref else 'oracle FDMT port'} ({threads} threads) + "
               f"oracle row-normalise/boxcar ({threads} threads)/cluster (1 thread)")
     return done / secs, secs, sample, kind, threads
+
+
+def reference_gpu_leg(beams, inputs, pipe, dev, stride: int = 4):
+    """The reference's own GPU path — CFdmtGpu::process_image, then (the
+    reference has no per-row normalisation: this build's bfs_norm_rows) the
+    reference's gather_candidates_in_dynamicalArray + complete_clusterization
+    with its log — compiled from the reference's sources (oracle/_ref), on every
+    `stride`-th beam, timed beside this build's pipeline on the same beams."""
+    import tempfile
+
+    import torch
+
+    from cpp_projects_b200 import search
+    from oracle import pyoracle
+    if pyoracle.ref_gpu_lib() is None:
+        return None
+    l = pyoracle.ref_gpu_lib()
+    idx = list(range(0, len(beams), stride))
+    thr = torch.tensor([SEARCH["thr"]], device=dev)
+    metrics = torch.tensor(SEARCH["metrics"], dtype=torch.int32, device=dev)
+    log = tempfile.NamedTemporaryFile(suffix=".log", delete=False).name
+    t_ref = 0.0
+    units = 0
+    for i in idx:
+        b = beams[i]
+        f = pyoracle.RefFdmtGpu(b.fmin, b.fmax, b.nchan, b.nsamp, b.max_dt)
+        out = torch.empty((b.max_dt, b.nsamp), device=dev)
+        z = torch.empty_like(out)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        f.process_image(inputs[i].data_ptr(), out.data_ptr())
+        search.norm_rows(out, out=z)
+        l.ref_search_dynamic(z.data_ptr(), b.max_dt, b.nsamp, thr.data_ptr(), SEARCH["param"],
+                             metrics.data_ptr(), log.encode(), 1e-3, 0.0)
+        torch.cuda.synchronize()
+        t_ref += time.perf_counter() - t0
+        units += b.nchan * b.nsamp
+        del f, out, z
+    os.unlink(log)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in idx:
+        pipe.run_beam(i, inputs[i])
+    torch.cuda.synchronize()
+    t_ours = time.perf_counter() - t0
+    return {"value": units / t_ref, "unit": UNIT, "beams": f"{len(idx)} of {len(beams)} (every {stride}th)",
+            "ours_same_beams": units / t_ours, "speedup": t_ref / t_ours,
+            "path": "reference CFdmtGpu + gather_candidates_in_dynamicalArray + complete_clusterization, "
+                    "sm_100a build of its own sources; wall clock, synchronised"}
 
 
 def run_reference(args):
@@ -298,6 +348,11 @@ def run_ours(args):
                "wall_ms_per_step": 1e3 * wall / args.steps}
         del host
 
+    # ---- the reference's own GPU path on a subset (rank 0, N=1) ---------------
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_ref_gpu:
+        ref_gpu = reference_gpu_leg(beams, inputs, pipe, dev)
+
     # ---- CPU baseline (rank 0, N=1 only) -------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -329,7 +384,8 @@ def run_ours(args):
             "pipeline_balg": {"bytes_per_step": pipe_bytes,
                               "gbs": pipe_bytes / (step_ms / 1e3) / 1e9,
                               "frac_of_peak": pipe_bytes / (step_ms / 1e3) / 1e9 / peak},
-            "e2e": e2e, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": launches,
+            "e2e": e2e, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "clocks": clk,
+            "gpu_launches": launches,
             "candidates": ncand, "delegates": ndel,
         }
         print(json.dumps(line), flush=True)

@@ -13,9 +13,10 @@
 // float quotients of float delays and the row offsets are float products
 // truncated to int.  This file must be compiled with -ffp-contract=off so no
 // multiply-add is fused.  The reference GPU class computes the same offsets on
-// the device with the approximate __fdividef (L/FDMT/FdmtGpu.cu:372-373); the
-// CPU class (the parity oracle) uses exact division, which is what is
-// reproduced here, once, on the host.
+// the device from float reciprocals (fdividef(1.0f, f*f), L/FDMT/FdmtGpu.cu:
+// 372-373,466-469) where the CPU class (the parity oracle) takes double
+// reciprocals; the CPU class's values are what is reproduced here, once, on
+// the host.
 #include <algorithm>
 #include <cmath>
 #include <cstring>

@@ -167,7 +167,8 @@ bfs_status bfs_row_stats(const float* d_in, int rows, int cols, float* d_stats, 
  *   :592-671).
  * The window sum is accumulated sequentially from the start sample (the
  * reference's order); only complete windows are tested; S/N = sum/sqrtf(w)
- * with an IEEE divide (snr_fast != 0 uses the reference GPU's __fdividef).
+ * with an IEEE divide, as the reference's fdividef without --use_fast_math
+ * (snr_fast != 0: the approximate __fdividef, <= 2 ulp, not bit-compatible).
  * A candidate is emitted when S/N > thr; thr is read from d_thr (device) when
  * non-NULL, else from `thr`.  d_stats (optional, from bfs_row_stats) makes the
  * kernel normalise each sample as (x - mean_r)/std_r before summing.

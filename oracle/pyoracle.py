@@ -22,6 +22,7 @@ CAND_DTYPE = np.dtype([("mt", "<i4"), ("mdt", "<i4"), ("mwidth", "<i4"), ("msnr"
 
 _lib = None
 _ref = None
+_ref_gpu = None
 
 
 def build() -> None:
@@ -55,6 +56,57 @@ def ref_lib() -> ctypes.CDLL | None:
             return None
         _ref = ctypes.CDLL(str(path))
     return _ref
+
+
+def ref_gpu_lib() -> ctypes.CDLL | None:
+    """The reference's own GPU classes (oracle/_ref/libref_gpu.so), or None."""
+    global _ref_gpu
+    if _ref_gpu is None:
+        path = HERE / "_ref" / "libref_gpu.so"
+        if not path.exists():
+            return None
+        l = ctypes.CDLL(str(path))
+        l.ref_fdmt_gpu_create.restype = ctypes.c_void_p
+        l.ref_fdmt_gpu_create.argtypes = [_F, _F, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        l.ref_fdmt_gpu_destroy.argtypes = [_P]
+        l.ref_fdmt_gpu_process.argtypes = [_P, _P, _P, ctypes.c_int]
+        for n in ("ref_gather_heap", "ref_gather_dynamic"):
+            getattr(l, n).restype = ctypes.c_uint
+            getattr(l, n).argtypes = [_P, ctypes.c_int, ctypes.c_int, _P, ctypes.c_int, _P, ctypes.c_uint]
+        l.ref_cluster_heap.restype = ctypes.c_uint
+        l.ref_cluster_heap.argtypes = [_P, ctypes.c_int, ctypes.c_int, _P, ctypes.c_int, _P,
+                                       ctypes.c_char_p, _F, _F]
+        l.ref_search_dynamic.restype = ctypes.c_uint
+        l.ref_search_dynamic.argtypes = [_P, ctypes.c_int, ctypes.c_int, _P, ctypes.c_int, _P,
+                                         ctypes.c_char_p, _F, _F]
+        _ref_gpu = l
+    return _ref_gpu
+
+
+class RefFdmtGpu:
+    """The reference's CFdmtGpu (device pointers as ints; default stream)."""
+
+    def __init__(self, fmin, fmax, nchan, cols, max_dt):
+        self.l = ref_gpu_lib()
+        self.h = self.l.ref_fdmt_gpu_create(_F(fmin), _F(fmax), nchan, cols, max_dt)
+
+    def process_image(self, d_in: int, d_out: int, b_ones=False) -> int:
+        return self.l.ref_fdmt_gpu_process(self.h, _P(d_in), _P(d_out), 1 if b_ones else 0)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.l.ref_fdmt_gpu_destroy(self.h)
+            self.h = None
+
+
+def ref_gpu_gather(d_plane: int, rows: int, cols: int, d_thr: int, mode: int, param: int,
+                   cap: int = 1 << 22) -> np.ndarray:
+    """The reference's gather (mode 0: dynamic, widths 2^q; 1: heap, widths 1..W)."""
+    l = ref_gpu_lib()
+    out = np.zeros(cap, CAND_DTYPE)
+    fn = l.ref_gather_dynamic if mode == 0 else l.ref_gather_heap
+    n = fn(_P(d_plane), rows, cols, _P(d_thr), param, _ptr(out), cap)
+    return out[: min(n, cap)].copy()
 
 
 def _ptr(a: np.ndarray):

@@ -103,7 +103,7 @@ def test_boxcar_fast_snr_mode_is_within_two_ulp(cuda):
     got = search.cands_to_numpy(got)
     key = lambda c: set(zip(c["mt"].tolist(), c["mdt"].tolist(), c["mwidth"].tolist()))
     diff = key(got) ^ key(want)
-    # __fdividef differs from the IEEE quotient by <= 2 ulp: only candidates
+    # the fast quotient differs from the IEEE one by <= 2 ulp: only candidates
     # within 2 ulp of the threshold can change side
     assert len(diff) <= 2
     common = np.intersect1d(got[["mt", "mdt", "mwidth"]], want[["mt", "mdt", "mwidth"]])
