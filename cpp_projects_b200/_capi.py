@@ -18,6 +18,7 @@ STATUS_NAMES = {0: "BFS_OK", 1: "BFS_ERR_ARG", 2: "BFS_ERR_CUDA", 3: "BFS_ERR_OV
                 4: "BFS_ERR_TIMEOUT", 5: "BFS_ERR_ALLOC", 6: "BFS_ERR_UNSUPPORTED"}
 BFS_WIDTHS_POW2, BFS_WIDTHS_ALL = 0, 1
 BFS_FDMT_EXTERNAL_WS = 1
+BFS_FUSE_AUTOTUNE = -2
 
 
 class BfsError(RuntimeError):
@@ -30,7 +31,7 @@ class FdmtDesc(ctypes.Structure):
     _fields_ = [("fmin", ctypes.c_float), ("fmax", ctypes.c_float), ("nchan", ctypes.c_int),
                 ("ncols", ctypes.c_int), ("max_dt", ctypes.c_int), ("plan_kind", ctypes.c_int),
                 ("precision", ctypes.c_int), ("fuse_depth", ctypes.c_int),
-                ("flags", ctypes.c_int), ("reserved", ctypes.c_int * 7)]
+                ("flags", ctypes.c_int), ("head_tile", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
 
 
 class FdmtInfo(ctypes.Structure):
@@ -44,6 +45,13 @@ class ChunkDesc(ctypes.Structure):
                 ("nchan", ctypes.c_int), ("len_sft", ctypes.c_int), ("nbin", ctypes.c_int),
                 ("nfft", ctypes.c_int), ("noverlap", ctypes.c_int), ("tsamp", ctypes.c_float),
                 ("max_dt", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+
+
+class BatchDesc(ctypes.Structure):
+    _fields_ = [("nbeams", ctypes.c_int), ("beams", ctypes.POINTER(FdmtDesc)),
+                ("widths_mode", ctypes.c_int), ("param", ctypes.c_int), ("thr", ctypes.c_float),
+                ("metrics", ctypes.c_int * 3), ("capacity", ctypes.c_uint32),
+                ("use_graph", ctypes.c_int), ("reserved", ctypes.c_int * 8)]
 
 
 class Cand(ctypes.Structure):
@@ -64,6 +72,8 @@ _SIGNATURES = {
     "bfs_trim_scratch": (_I, []),
     "bfs_fdmt_plan_create": (_I, [ctypes.POINTER(FdmtDesc), ctypes.POINTER(_P)]),
     "bfs_fdmt_plan_create_host": (_I, [ctypes.POINTER(FdmtDesc), ctypes.POINTER(_P)]),
+    "bfs_fdmt_autotune": (_I, [ctypes.POINTER(FdmtDesc), ctypes.POINTER(_I), ctypes.POINTER(_I),
+                               ctypes.POINTER(_F)]),
     "bfs_fdmt_plan_destroy": (_I, [_P]),
     "bfs_fdmt_plan_info": (_I, [_P, ctypes.POINTER(FdmtInfo)]),
     "bfs_fdmt_plan_rows": (_I, [_P, _P, _I]),
@@ -83,6 +93,12 @@ _SIGNATURES = {
                                ctypes.POINTER(_U32), _P]),
     "bfs_cluster": (_I, [_P, _U32, _P, _P, _P, _P, ctypes.POINTER(_U32), _P]),
     "bfs_select_delegates": (_I, [_P, _P, _U32, _P, _U32, _P, _P]),
+    "bfs_cluster_grouped": (_I, [_P, _U32, _P, _U32, _P, _P, _P, _P, ctypes.POINTER(_U32), _P]),
+    "bfs_batch_create": (_I, [ctypes.POINTER(BatchDesc), ctypes.POINTER(_P)]),
+    "bfs_batch_destroy": (_I, [_P]),
+    "bfs_batch_run": (_I, [_P, _P, _P]),
+    "bfs_batch_counts": (_I, [_P, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
+    "bfs_batch_beam_results": (_I, [_P, _I, _P, _P, _I, ctypes.POINTER(_I), ctypes.POINTER(_U32)]),
     "bfs_chunk_create": (_I, [ctypes.POINTER(ChunkDesc), ctypes.POINTER(_P)]),
     "bfs_chunk_destroy": (_I, [_P]),
     "bfs_chunk_info": (_I, [_P, _P, _I]),

@@ -31,8 +31,22 @@ class Clusters:
         return cands_to_numpy(self.cands.index_select(0, self.delegates.long()))
 
     def group_sizes(self) -> np.ndarray:
+        """Sizes in group order (the order of ``offsets``)."""
         o = self.offsets.cpu().numpy()
         return np.diff(o)
+
+    def delegate_group_sizes(self) -> np.ndarray:
+        """Size of each delegate's own group, in delegate order (computed on
+        the device: position of the delegate in ``perm`` -> its group)."""
+        if self.ngroups == 0:
+            return np.zeros(0, np.int64)
+        n = int(self.perm.shape[0])
+        inv = torch.empty(n, dtype=torch.int64, device=self.perm.device)
+        inv[self.perm.long()] = torch.arange(n, device=self.perm.device)
+        pos = inv[self.delegates.long()]
+        offs = self.offsets.long()
+        g = torch.searchsorted(offs, pos, right=True) - 1
+        return (offs[g + 1] - offs[g]).cpu().numpy()
 
 
 def complete_clusterization(cands: torch.Tensor, metrics, stream=None) -> Clusters:
@@ -74,20 +88,13 @@ def write_log(cl: Clusters, filename: str, delt_bin: float, t_chunkBegin: float,
     The reference pairs the i-th delegate (sorted by mt) with the i-th group's
     size in group order; that quirk is kept unless num_from_delegate_group."""
     drec = cl.delegate_records()
-    dl = cl.delegates.cpu().numpy()
-    sizes = cl.group_sizes()
-    if num_from_delegate_group:
-        gid = np.empty(int(cl.cands.shape[0]), np.int64)
-        perm = cl.perm.cpu().numpy()
-        offs = cl.offsets.cpu().numpy()
-        for g in range(cl.ngroups):
-            gid[perm[offs[g]:offs[g + 1]]] = g
+    sizes = cl.delegate_group_sizes() if num_from_delegate_group else cl.group_sizes()
     with open(filename, "w") as f:
         f.write("".join(s.rjust(10) for s in ("N", "t, bin", "t, sec", "dedisp", "width", "SNR",
                                                 "num")) + "\n")
-        for i, j in enumerate(dl):
+        for i in range(cl.ngroups):
             r = drec[i]
-            num = sizes[gid[j]] if num_from_delegate_group else sizes[i]
+            num = sizes[i]
             t_sec = np.float32(t_chunkBegin) + np.float32(r["mt"]) * np.float32(delt_bin)
             cols = [str(i + 1), str(int(r["mt"])), _fmt_g(float(t_sec)), str(int(r["mdt"])),
                     str(int(r["mwidth"])), _fmt_g(float(r["msnr"])), str(int(num))]

@@ -1,0 +1,336 @@
+// Batched multi-beam search: many beams of uneven channel counts and lengths
+// through FDMT -> per-row statistics -> normalise + boxcar + compaction ->
+// clustering, with the per-beam kernel sequence of every beam captured in ONE
+// CUDA graph and the candidate handling done once for the whole batch.
+//
+// The reference runs one chunk at a time with host round trips between
+// stages (CChunk_gpu::process, L/CDMT/Chunk_gpu.cu:254-460; clusterization_main,
+// L/Clusterization/Clusterization.cu:17-54).  Here:
+//   stage 1 (graph)  for each beam: fused/plain FDMT into a shared DM-time
+//                    plane, row statistics, and the boxcar appending to one
+//                    device-wide candidate array with a shared atomic counter,
+//                    each candidate tagged with its beam — no host sync;
+//   stage 2          one read of the counter, one canonical sort over all
+//                    beams (beam, row, sample, width), one 3-pass clustering
+//                    whose initial groups are the beams, one delegate sort by
+//                    (beam, mt, group), one copy of the delegates to the host.
+// Plans are autotuned per shape and share one workspace; the DM-time plane
+// and statistics buffers are shared (the graph serialises the beams on one
+// stream), so device memory is set by the largest beam plus the candidates.
+#include <cub/device/device_radix_sort.cuh>
+
+#include <memory>
+#include <vector>
+
+#include "internal.h"
+
+namespace bfs {
+bfs_status launch_row_stats(const float* d_in, int rows, int cols, float* d_stats, int mode,
+                            cudaStream_t s);
+bfs_status launch_boxcar(const float* d_plane, int rows, int cols, const float* d_stats,
+                         float thr, const float* d_thr, int mode, int param, int snr_fast,
+                         bfs_cand* d_out, unsigned capacity, unsigned* d_count, cudaStream_t s,
+                         int tag, int* d_tags);
+bfs_status sort_tagged_candidates(const bfs_cand* d_c, const int* d_tags, unsigned n, int max_rows,
+                                  int max_cols, int max_tag, int mode, int param, bfs_cand* d_dst,
+                                  int* d_tdst, cudaStream_t s);
+}  // namespace bfs
+
+struct bfs_batch {
+    std::vector<bfs_fdmt_desc> beams;
+    std::vector<bfs_fdmt_plan*> plans;
+    int widths_mode = 0, param = 5;
+    float thr = 7.0f;
+    int metrics[3] = {16, 8, 1 << 30};
+    unsigned capacity = 0;
+    bool use_graph = true;
+    int max_rows = 0, max_cols = 0;
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    float* plane = nullptr;
+    float* stats = nullptr;
+    bfs_cand* cands = nullptr;     // boxcar output (arrival order)
+    int* tags = nullptr;
+    bfs_cand* sorted = nullptr;    // canonical order
+    int* sorted_tags = nullptr;
+    unsigned* d_count = nullptr;
+    int *perm = nullptr, *offsets = nullptr, *delegates = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<const float*> graph_inputs;
+    int runs = 0;
+    // results of the last run
+    unsigned n_cands = 0, n_groups = 0;
+    std::vector<bfs_cand> h_delegates;
+    std::vector<int> h_delegate_beam, h_delegate_size, h_beam_first, h_beam_count, h_beam_cands;
+    ~bfs_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (auto* p : plans) bfs_fdmt_plan_destroy(p);
+        for (void* p : {ws, static_cast<void*>(plane), static_cast<void*>(stats), static_cast<void*>(cands),
+                        static_cast<void*>(tags), static_cast<void*>(sorted), static_cast<void*>(sorted_tags),
+                        static_cast<void*>(d_count), static_cast<void*>(perm), static_cast<void*>(offsets),
+                        static_cast<void*>(delegates)})
+            if (p) cudaFree(p);
+    }
+};
+
+namespace bfs {
+namespace {
+
+// Inverse of the group-order permutation: position of every candidate.
+__global__ void k_inverse_perm(const int* __restrict__ perm, unsigned n, int* __restrict__ inv) {
+    const unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) inv[perm[p]] = static_cast<int>(p);
+}
+
+// For delegate i (in the (mt, group) order bfs_cluster returns): its record,
+// beam, group size, and the beam as the key of the final stable sort.
+__global__ void k_delegate_info(const bfs_cand* __restrict__ c, const int* __restrict__ tags,
+                                const int* __restrict__ dl, const int* __restrict__ inv,
+                                const int* __restrict__ offsets, unsigned ng,
+                                bfs_cand* __restrict__ rec, int* __restrict__ size,
+                                unsigned* __restrict__ key, unsigned* __restrict__ val) {
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ng) return;
+    const int di = dl[i];
+    const int p = inv[di];
+    int lo = 0, hi = static_cast<int>(ng) - 1;  // group = last offset <= p
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (offsets[mid] <= p) lo = mid; else hi = mid - 1;
+    }
+    rec[i] = c[di];
+    size[i] = offsets[lo + 1] - offsets[lo];
+    key[i] = static_cast<unsigned>(tags[di]);
+    val[i] = i;
+}
+
+__global__ void k_permute_delegates(const bfs_cand* __restrict__ rec, const int* __restrict__ size,
+                                    const unsigned* __restrict__ beam, const unsigned* __restrict__ order,
+                                    unsigned ng, bfs_cand* __restrict__ rec_out, int* __restrict__ size_out,
+                                    int* __restrict__ beam_out) {
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ng) return;
+    rec_out[i] = rec[order[i]];
+    size_out[i] = size[order[i]];
+    beam_out[i] = static_cast<int>(beam[i]);
+}
+
+// Candidates per beam from the tag-sorted list (lower bounds).
+__global__ void k_beam_bounds(const int* __restrict__ sorted_tags, unsigned n, int nb,
+                              unsigned* __restrict__ first) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b > nb) return;
+    unsigned lo = 0, hi = n;
+    while (lo < hi) {
+        const unsigned mid = (lo + hi) >> 1;
+        if (sorted_tags[mid] < b) lo = mid + 1; else hi = mid;
+    }
+    first[b] = lo;
+}
+
+int bits_of(unsigned long long v) {
+    int b = 0;
+    while (b < 64 && (v >> b) != 0ull) ++b;
+    return b;
+}
+
+}  // namespace
+}  // namespace bfs
+
+using namespace bfs;
+
+extern "C" bfs_status bfs_batch_create(const bfs_batch_desc* desc, bfs_batch** out) {
+    BFS_ARG(desc && out && desc->beams && desc->nbeams >= 1, "bad batch description");
+    *out = nullptr;
+    std::unique_ptr<bfs_batch> b(new bfs_batch);
+    b->beams.assign(desc->beams, desc->beams + desc->nbeams);
+    b->widths_mode = desc->widths_mode;
+    b->param = desc->param;
+    b->thr = desc->thr;
+    for (int i = 0; i < 3; ++i) b->metrics[i] = desc->metrics[i];
+    b->capacity = desc->capacity ? desc->capacity : (1u << 26);
+    b->use_graph = desc->use_graph != 0;
+    size_t plane = 0;
+    for (const bfs_fdmt_desc& d0 : b->beams) {
+        bfs_fdmt_desc d = d0;
+        d.flags |= BFS_FDMT_EXTERNAL_WS;
+        bfs_fdmt_plan* p = nullptr;
+        bfs_status st = bfs_fdmt_plan_create(&d, &p);
+        if (st != BFS_OK) return st;
+        b->plans.push_back(p);
+        size_t need = 0;
+        bfs_fdmt_workspace_size(p, &need);
+        b->ws_bytes = std::max(b->ws_bytes, need);
+        plane = std::max(plane, static_cast<size_t>(d.max_dt) * d.ncols);
+        b->max_rows = std::max(b->max_rows, d.max_dt);
+        b->max_cols = std::max(b->max_cols, d.ncols);
+    }
+    BFS_ARG(b->max_rows <= 65535, "max_dt above 65535");
+    BFS_CUDA(cudaMalloc(&b->ws, b->ws_bytes ? b->ws_bytes : 256));
+    BFS_CUDA(cudaMalloc(&b->plane, plane * sizeof(float)));
+    BFS_CUDA(cudaMalloc(&b->stats, 2 * static_cast<size_t>(b->max_rows) * sizeof(float)));
+    const size_t cap = b->capacity;
+    BFS_CUDA(cudaMalloc(&b->cands, cap * sizeof(bfs_cand)));
+    BFS_CUDA(cudaMalloc(&b->tags, cap * sizeof(int)));
+    BFS_CUDA(cudaMalloc(&b->sorted, cap * sizeof(bfs_cand)));
+    BFS_CUDA(cudaMalloc(&b->sorted_tags, cap * sizeof(int)));
+    BFS_CUDA(cudaMalloc(&b->d_count, sizeof(unsigned)));
+    BFS_CUDA(cudaMalloc(&b->perm, cap * sizeof(int)));
+    BFS_CUDA(cudaMalloc(&b->offsets, (cap + 1) * sizeof(int)));
+    BFS_CUDA(cudaMalloc(&b->delegates, cap * sizeof(int)));
+    *out = b.release();
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_batch_destroy(bfs_batch* b) {
+    delete b;
+    return BFS_OK;
+}
+
+// Stage 1 for every beam, enqueued on s (captured or eager).
+static bfs_status enqueue_stage1(bfs_batch* b, const float* const* d_inputs, cudaStream_t s) {
+    BFS_CUDA(cudaMemsetAsync(b->d_count, 0, sizeof(unsigned), s));
+    for (size_t i = 0; i < b->beams.size(); ++i) {
+        const bfs_fdmt_desc& d = b->beams[i];
+        bfs_status st = bfs_fdmt_execute_ws(b->plans[i], d_inputs[i], b->plane, 0, b->ws, b->ws_bytes, s);
+        if (st != BFS_OK) return st;
+        st = launch_row_stats(b->plane, d.max_dt, d.ncols, b->stats, 0, s);
+        if (st != BFS_OK) return st;
+        st = launch_boxcar(b->plane, d.max_dt, d.ncols, b->stats, b->thr, nullptr, b->widths_mode,
+                           b->param, 0, b->cands, b->capacity, b->d_count, s, static_cast<int>(i),
+                           b->tags);
+        if (st != BFS_OK) return st;
+    }
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_batch_run(bfs_batch* b, const float* const* d_inputs, void* stream) {
+    BFS_ARG(b && d_inputs, "null argument");
+    cudaStream_t s = as_stream(stream);
+    const int nb = static_cast<int>(b->beams.size());
+    bool same_inputs = b->exec && b->graph_inputs.size() == static_cast<size_t>(nb);
+    for (int i = 0; same_inputs && i < nb; ++i) same_inputs = b->graph_inputs[i] == d_inputs[i];
+    if (b->use_graph && b->runs >= 1 && !same_inputs) {
+        // (re)capture: the first run was eager (kernel attributes are set then)
+        if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+        if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+        cudaStream_t cs;
+        BFS_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        bfs_status st = e == cudaSuccess ? enqueue_stage1(b, d_inputs, cs)
+                                         : fail(BFS_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
+        cudaGraph_t g = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+        cudaStreamDestroy(cs);
+        if (st != BFS_OK) { if (g) cudaGraphDestroy(g); return st; }
+        if (e2 != cudaSuccess) return fail(BFS_ERR_CUDA, "end capture: %s", cudaGetErrorString(e2));
+        b->graph = g;
+        BFS_CUDA(cudaGraphInstantiate(&b->exec, g, 0));
+        b->graph_inputs.assign(d_inputs, d_inputs + nb);
+        same_inputs = true;
+    }
+    if (b->use_graph && b->exec && same_inputs) {
+        BFS_CUDA(cudaGraphLaunch(b->exec, s));
+    } else {
+        bfs_status st = enqueue_stage1(b, d_inputs, s);
+        if (st != BFS_OK) return st;
+    }
+    ++b->runs;
+
+    // ---- stage 2: all candidates at once ----------------------------------
+    unsigned count = 0;
+    BFS_CUDA(cudaMemcpyAsync(&count, b->d_count, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    BFS_CUDA(cudaStreamSynchronize(s));
+    if (count > b->capacity)
+        return fail(BFS_ERR_OVERFLOW, "%u candidates, batch capacity %u", count, b->capacity);
+    b->n_cands = count;
+    b->h_delegates.clear(); b->h_delegate_beam.clear(); b->h_delegate_size.clear();
+    b->h_beam_first.assign(nb, 0); b->h_beam_count.assign(nb, 0); b->h_beam_cands.assign(nb, 0);
+    b->n_groups = 0;
+    if (count == 0) return BFS_OK;
+    bfs_status st = sort_tagged_candidates(b->cands, b->tags, count, b->max_rows, b->max_cols, nb - 1,
+                                           b->widths_mode, b->param, b->sorted, b->sorted_tags, s);
+    if (st != BFS_OK) return st;
+    uint32_t ng = 0;
+    st = bfs_cluster_grouped(b->sorted, count, b->sorted_tags, static_cast<uint32_t>(nb), b->metrics,
+                             b->perm, b->offsets, b->delegates, &ng, stream);
+    if (st != BFS_OK) return st;
+    b->n_groups = ng;
+    // delegates come back ordered by (mt, group); a stable sort by beam gives (beam, mt, group)
+    const int bbits = std::max(1, bits_of(static_cast<unsigned long long>(nb)));
+    size_t tb = 0;
+    unsigned* nullu = nullptr;
+    BFS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, nullu, nullu, nullu, nullu,
+                                             static_cast<int>(ng), 0, bbits, s));
+    int* inv = nullptr;
+    unsigned* u = nullptr;   // key, key_sorted, val, order, beam_first (nb+1)
+    bfs_cand* rec = nullptr; // rec, rec_out
+    int* ints = nullptr;     // size, size_out, beam_out
+    void* tmp = nullptr;
+    st = stream_alloc(reinterpret_cast<void**>(&inv), sizeof(int) * count, s);
+    if (st == BFS_OK) st = stream_alloc(reinterpret_cast<void**>(&u), sizeof(unsigned) * (4 * ng + nb + 1), s);
+    if (st == BFS_OK) st = stream_alloc(reinterpret_cast<void**>(&rec), sizeof(bfs_cand) * 2 * ng, s);
+    if (st == BFS_OK) st = stream_alloc(reinterpret_cast<void**>(&ints), sizeof(int) * 3 * ng, s);
+    if (st == BFS_OK) st = stream_alloc(&tmp, tb ? tb : 16, s);
+    if (st != BFS_OK) return st;
+    unsigned *key = u, *key_sorted = u + ng, *val = u + 2 * ng, *order = u + 3 * ng, *bfirst = u + 4 * ng;
+    const int th = 256;
+    k_inverse_perm<<<static_cast<int>((count + th - 1) / th), th, 0, s>>>(b->perm, count, inv);
+    BFS_LAUNCH_CHECK("k_inverse_perm");
+    const int blg = static_cast<int>((ng + th - 1) / th);
+    k_delegate_info<<<blg, th, 0, s>>>(b->sorted, b->sorted_tags, b->delegates, inv, b->offsets, ng, rec,
+                                       ints, key, val);
+    BFS_LAUNCH_CHECK("k_delegate_info");
+    BFS_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, key, key_sorted, val, order, static_cast<int>(ng), 0,
+                                             bbits, s));
+    k_permute_delegates<<<blg, th, 0, s>>>(rec, ints, key_sorted, order, ng, rec + ng, ints + ng,
+                                           ints + 2 * ng);
+    BFS_LAUNCH_CHECK("k_permute_delegates");
+    k_beam_bounds<<<(nb + 1 + th - 1) / th, th, 0, s>>>(b->sorted_tags, count, nb, bfirst);
+    BFS_LAUNCH_CHECK("k_beam_bounds");
+    b->h_delegates.resize(ng);
+    b->h_delegate_size.resize(ng);
+    b->h_delegate_beam.resize(ng);
+    std::vector<unsigned> first(nb + 1);
+    BFS_CUDA(cudaMemcpyAsync(b->h_delegates.data(), rec + ng, sizeof(bfs_cand) * ng, cudaMemcpyDeviceToHost, s));
+    BFS_CUDA(cudaMemcpyAsync(b->h_delegate_size.data(), ints + ng, sizeof(int) * ng, cudaMemcpyDeviceToHost, s));
+    BFS_CUDA(cudaMemcpyAsync(b->h_delegate_beam.data(), ints + 2 * ng, sizeof(int) * ng, cudaMemcpyDeviceToHost, s));
+    BFS_CUDA(cudaMemcpyAsync(first.data(), bfirst, sizeof(unsigned) * (nb + 1), cudaMemcpyDeviceToHost, s));
+    cudaFreeAsync(inv, s);
+    cudaFreeAsync(u, s);
+    cudaFreeAsync(rec, s);
+    cudaFreeAsync(ints, s);
+    cudaFreeAsync(tmp, s);
+    BFS_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < nb; ++i) b->h_beam_cands[i] = static_cast<int>(first[i + 1] - first[i]);
+    for (uint32_t i = 0; i < ng; ++i) {
+        const int beam = b->h_delegate_beam[i];
+        if (b->h_beam_count[beam] == 0) b->h_beam_first[beam] = static_cast<int>(i);
+        ++b->h_beam_count[beam];
+    }
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_batch_counts(const bfs_batch* b, uint32_t* n_cands, uint32_t* n_groups) {
+    BFS_ARG(b != nullptr, "null argument");
+    if (n_cands) *n_cands = b->n_cands;
+    if (n_groups) *n_groups = b->n_groups;
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_batch_beam_results(const bfs_batch* b, int beam, bfs_cand* delegates,
+                                             int* group_sizes, int cap, int* n_delegates,
+                                             uint32_t* n_candidates) {
+    BFS_ARG(b != nullptr && beam >= 0 && beam < static_cast<int>(b->beams.size()), "bad beam");
+    const int n = b->h_beam_count.empty() ? 0 : b->h_beam_count[beam];
+    if (n_delegates) *n_delegates = n;
+    if (n_candidates) *n_candidates = b->h_beam_cands.empty() ? 0u : static_cast<uint32_t>(b->h_beam_cands[beam]);
+    const int first = n ? b->h_beam_first[beam] : 0;
+    for (int i = 0; i < n && i < cap; ++i) {
+        if (delegates) delegates[i] = b->h_delegates[first + i];
+        if (group_sizes) group_sizes[i] = b->h_delegate_size[first + i];
+    }
+    return BFS_OK;
+}

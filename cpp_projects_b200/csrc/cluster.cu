@@ -272,7 +272,16 @@ static bfs_status cluster_pass(const bfs_cand* d_cands, unsigned n, int field, i
 extern "C" bfs_status bfs_cluster(const bfs_cand* d_cands, uint32_t n, const int* metrics,
                                   int* d_perm, int* d_offsets, int* d_delegates,
                                   uint32_t* h_ngroups, void* stream) {
+    return bfs_cluster_grouped(d_cands, n, nullptr, 0, metrics, d_perm, d_offsets, d_delegates,
+                               h_ngroups, stream);
+}
+
+extern "C" bfs_status bfs_cluster_grouped(const bfs_cand* d_cands, uint32_t n, const int* d_group0,
+                                          uint32_t ngroups0, const int* metrics, int* d_perm,
+                                          int* d_offsets, int* d_delegates, uint32_t* h_ngroups,
+                                          void* stream) {
     BFS_ARG(metrics && h_ngroups, "null argument");
+    BFS_ARG(d_group0 == nullptr || ngroups0 >= 1, "ngroups0 must be >= 1 with d_group0");
     *h_ngroups = 0;
     if (n == 0) return BFS_OK;
     BFS_ARG(d_cands && d_perm && d_offsets && d_delegates, "null argument");
@@ -312,7 +321,9 @@ extern "C" bfs_status bfs_cluster(const bfs_cand* d_cands, uint32_t n, const int
         BFS_CUDA(cudaMemcpyAsync(h_range, range, sizeof(h_range), cudaMemcpyDeviceToHost, s));
         BFS_CUDA(cudaStreamSynchronize(s));
     }
-    unsigned groups = 1;
+    unsigned groups = d_group0 ? ngroups0 : 1u;
+    if (d_group0)
+        BFS_CUDA(cudaMemcpyAsync(gid, d_group0, sizeof(unsigned) * n, cudaMemcpyDeviceToDevice, s));
     for (int field = 0; field < 3; ++field) {
         const int fmin = static_cast<int>(h_range[2 * field] ^ 0x80000000u);
         const int fmax = static_cast<int>(h_range[2 * field + 1] ^ 0x80000000u);
@@ -323,12 +334,14 @@ extern "C" bfs_status bfs_cluster(const bfs_cand* d_cands, uint32_t n, const int
         bfs_status st;
         if (end_bit <= 32)
             st = cluster_pass<unsigned>(d_cands, n, field, fmin, fbits, end_bit,
-                                        static_cast<long long>(metrics[field]), gid, field == 0,
+                                        static_cast<long long>(metrics[field]), gid,
+                                        field == 0 && d_group0 == nullptr,
                                         k_in, k_out, v_in, v_out, flags, scan, tmp, tmp_bytes, s);
         else
             st = cluster_pass<unsigned long long>(d_cands, n, field, fmin, fbits, end_bit,
                                                   static_cast<long long>(metrics[field]), gid,
-                                                  field == 0, k_in, k_out, v_in, v_out, flags, scan,
+                                                  field == 0 && d_group0 == nullptr, k_in, k_out,
+                                                  v_in, v_out, flags, scan,
                                                   tmp, tmp_bytes, s);
         if (st != BFS_OK) return st;
         BFS_CUDA(cudaMemcpyAsync(&groups, scan + (n - 1), sizeof(unsigned), cudaMemcpyDeviceToHost, s));

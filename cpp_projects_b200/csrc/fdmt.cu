@@ -20,7 +20,10 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 
 #include "internal.h"
 
@@ -286,9 +289,20 @@ cudaError_t launch_head(const HeadPlan& hp, const FdmtPlanHost& h, const float* 
                         cudaStream_t s) {
     HeadKernel kern = head_kernel_for(h.rows_per_chan0);
     if (hp.smem_bytes > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(hp.smem_bytes));
-        if (e != cudaSuccess) return e;
+        // opt in once per (kernel, size) so later launches (also inside a
+        // stream capture) make no attribute call
+        static std::mutex mu;
+        static std::map<std::pair<const void*, int>, size_t> done;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        std::lock_guard<std::mutex> lock(mu);
+        size_t& have = done[{reinterpret_cast<const void*>(kern), dev}];
+        if (have < hp.smem_bytes) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 static_cast<int>(hp.smem_bytes));
+            if (e != cudaSuccess) return e;
+            have = hp.smem_bytes;
+        }
     }
     dim3 grid((h.ncols + hp.tile - 1) / hp.tile, h.nchan / hp.group);
     kern<<<grid, hp.width, hp.smem_bytes, s>>>(d_in, dst, groups, reinterpret_cast<const int4*>(tab),
@@ -335,12 +349,13 @@ static bfs_status plan_host_part(const bfs_fdmt_desc* desc, std::unique_ptr<bfs_
     if (st != BFS_OK) return st;
     const FdmtPlanHost& h = p->host;
     // fused head: explicit depth, or the deepest one that keeps two CTAs per SM
+    const int tile = desc->head_tile > 0 ? desc->head_tile : kHeadTile;
     if (desc->fuse_depth != 0) {
         const int want = desc->fuse_depth < 0 ? kHeadMaxDepth : desc->fuse_depth;
         const size_t limit = desc->fuse_depth < 0 ? kHeadSmemTwoPerSm : kHeadSmemMax;
         for (int k = std::min(want, h.niter); k >= 1; --k) {
             HeadPlan hp;
-            if (build_head_plan(h, k, kHeadTile, limit, &hp)) {
+            if (build_head_plan(h, k, tile, limit, &hp)) {
                 p->head = std::move(hp);
                 break;
             }
@@ -350,6 +365,115 @@ static bfs_status plan_host_part(const bfs_fdmt_desc* desc, std::unique_ptr<bfs_
                 "fuse_depth %d is not usable for this plan", desc->fuse_depth);
     }
     p->fuse_depth = p->head.depth;
+    return BFS_OK;
+}
+
+static inline int bfs_fdmt_plan_depth_of(int d) { return d; }
+
+// ---------------------------------------------------------------------------
+// Autotuner: fusion depth and head tile measured on the plan's own shape.
+// ---------------------------------------------------------------------------
+namespace {
+struct TuneKey {
+    int nchan, max_dt, cols_bucket;
+    uint32_t fmin_bits, fmax_bits;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(nchan, max_dt, cols_bucket, fmin_bits, fmax_bits) <
+               std::tie(o.nchan, o.max_dt, o.cols_bucket, o.fmin_bits, o.fmax_bits);
+    }
+};
+struct TuneVal { int depth, tile; float ms; };
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneVal> g_tune;
+
+TuneKey tune_key(const bfs_fdmt_desc& d) {
+    TuneKey k{};
+    k.nchan = d.nchan; k.max_dt = d.max_dt;
+    int b = 0;
+    while ((1 << b) < d.ncols && b < 30) ++b;
+    k.cols_bucket = b;
+    std::memcpy(&k.fmin_bits, &d.fmin, 4);
+    std::memcpy(&k.fmax_bits, &d.fmax, 4);
+    return k;
+}
+}  // namespace
+
+static bfs_status tune_fdmt(const bfs_fdmt_desc& base, TuneVal* best) {
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune.find(tune_key(base));
+        if (it != g_tune.end()) { *best = it->second; return BFS_OK; }
+    }
+    struct Cand { int depth, tile; };
+    std::vector<Cand> cands = {{0, 0}};
+    for (int k : {2, 3, 4, 5})
+        for (int tile : {256, 512}) cands.push_back({k, tile});
+    const size_t in_n = static_cast<size_t>(base.nchan) * base.ncols;
+    const size_t out_n = static_cast<size_t>(base.max_dt) * base.ncols;
+    float *d_in = nullptr, *d_out = nullptr;
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    TuneVal win{0, 0, 1e30f};
+    bfs_status st = BFS_OK;
+    cudaStream_t s = nullptr;
+    if (cudaMalloc(&d_in, in_n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&d_out, out_n * sizeof(float)) != cudaSuccess ||
+        cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        st = fail(BFS_ERR_ALLOC, "autotune: cannot allocate scratch for a %dx%d FDMT", base.nchan, base.ncols);
+    }
+    if (st == BFS_OK) cudaMemsetAsync(d_in, 0, in_n * sizeof(float), s);
+    for (const Cand& c : cands) {
+        if (st != BFS_OK) break;
+        bfs_fdmt_desc d = base;
+        d.fuse_depth = c.depth;
+        d.head_tile = c.tile;
+        d.flags = BFS_FDMT_EXTERNAL_WS;
+        bfs_fdmt_plan* p = nullptr;
+        if (bfs_fdmt_plan_create(&d, &p) != BFS_OK) continue;  // depth/tile not usable here
+        size_t need = 0;
+        bfs_fdmt_workspace_size(p, &need);
+        if (need > ws_bytes) {
+            if (ws) cudaFree(ws);
+            ws = nullptr;
+            if (cudaMalloc(&ws, need) != cudaSuccess) { bfs_fdmt_plan_destroy(p); ws_bytes = 0; continue; }
+            ws_bytes = need;
+        }
+        float ms = 1e30f;
+        bool ok = bfs_fdmt_execute_ws(p, d_in, d_out, 0, ws, ws_bytes, s) == BFS_OK;
+        for (int rep = 0; rep < 3 && ok; ++rep) {
+            cudaEventRecord(e0, s);
+            ok = bfs_fdmt_execute_ws(p, d_in, d_out, 0, ws, ws_bytes, s) == BFS_OK;
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, e0, e1);
+            ms = std::min(ms, t);
+        }
+        bfs_fdmt_plan_destroy(p);
+        if (ok && ms < win.ms) win = TuneVal{bfs_fdmt_plan_depth_of(c.depth), c.tile, ms};
+    }
+    if (ws) cudaFree(ws);
+    if (d_in) cudaFree(d_in);
+    if (d_out) cudaFree(d_out);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaGetLastError();
+    if (st != BFS_OK) return st;
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune[tune_key(base)] = win;
+    *best = win;
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_fdmt_autotune(const bfs_fdmt_desc* desc, int* depth, int* tile, float* ms) {
+    BFS_ARG(desc != nullptr, "null argument");
+    TuneVal v{};
+    bfs_status st = tune_fdmt(*desc, &v);
+    if (st != BFS_OK) return st;
+    if (depth) *depth = v.depth;
+    if (tile) *tile = v.tile;
+    if (ms) *ms = v.ms;
     return BFS_OK;
 }
 
@@ -363,9 +487,18 @@ extern "C" bfs_status bfs_fdmt_plan_create_host(const bfs_fdmt_desc* desc, bfs_f
     return BFS_OK;
 }
 
-extern "C" bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc, bfs_fdmt_plan** plan) {
-    BFS_ARG(plan != nullptr, "null argument");
+extern "C" bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc_in, bfs_fdmt_plan** plan) {
+    BFS_ARG(plan != nullptr && desc_in != nullptr, "null argument");
     *plan = nullptr;
+    bfs_fdmt_desc tuned = *desc_in;
+    if (tuned.fuse_depth == BFS_FUSE_AUTOTUNE) {
+        TuneVal v{};
+        bfs_status ts = tune_fdmt(*desc_in, &v);
+        if (ts != BFS_OK) return ts;
+        tuned.fuse_depth = v.depth;
+        tuned.head_tile = v.tile;
+    }
+    const bfs_fdmt_desc* desc = &tuned;
     std::unique_ptr<bfs_fdmt_plan> p;
     bfs_status st = plan_host_part(desc, p);
     if (st != BFS_OK) return st;

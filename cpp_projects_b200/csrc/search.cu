@@ -73,7 +73,8 @@ template <int MODE>
 __global__ void __launch_bounds__(kBoxThreads)
 k_boxcar(const float* __restrict__ plane, int rows, int cols, const float* __restrict__ stats,
          const float* __restrict__ d_thr, float thr_host, int wmax, int snr_fast,
-         bfs_cand* __restrict__ out, unsigned capacity, unsigned* __restrict__ d_count) {
+         bfs_cand* __restrict__ out, unsigned capacity, unsigned* __restrict__ d_count,
+         int tag, int* __restrict__ tags) {
     extern __shared__ float tile[];
     const int row = blockIdx.y;
     const int t0 = blockIdx.x * kBoxTile;
@@ -126,6 +127,7 @@ k_boxcar(const float* __restrict__ plane, int rows, int cols, const float* __res
                         bfs_cand c;
                         c.mt = t; c.mdt = row; c.mwidth = code; c.msnr = snr;
                         out[idx] = c;
+                        if (tags) tags[idx] = tag;
                     }
                 }
             }
@@ -157,7 +159,7 @@ __global__ void __launch_bounds__(kBoxThreads)
 k_boxcar_reg(const float* __restrict__ plane, int rows, int cols, const float* __restrict__ stats,
              const float* __restrict__ d_thr, float thr_host, float thr_lo_host, int snr_fast,
              bfs_cand* __restrict__ out, unsigned capacity, unsigned* __restrict__ d_count,
-             const WidthConsts wc) {
+             const WidthConsts wc, int tag, int* __restrict__ tags) {
     constexpr int kWin = kRegStarts + WMAX - 1;
     constexpr int kVec = (kWin + 3) / 4;
     __shared__ float4 tile4[(kRegTile + 4 * kVec + 3) / 4];
@@ -233,6 +235,7 @@ k_boxcar_reg(const float* __restrict__ plane, int rows, int cols, const float* _
                         bfs_cand c;
                         c.mt = tb + j; c.mdt = row; c.mwidth = code; c.msnr = snr;
                         out[idx] = c;
+                        if (tags) tags[idx] = tag;
                     }
                 }
             }
@@ -349,6 +352,63 @@ bfs_status sort_candidates_canonical(bfs_cand* d_c, unsigned n, int rows, int co
     return BFS_OK;
 }
 
+namespace {
+__global__ void k_tagged_keys(const bfs_cand* __restrict__ c, const int* __restrict__ tags, unsigned n,
+                              int row_bits, int col_bits, int mode, int wbits,
+                              unsigned long long* __restrict__ keys, unsigned* __restrict__ vals) {
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bfs_cand v = c[i];
+    const unsigned long long code = static_cast<unsigned long long>(mode == 0 ? v.mwidth : v.mwidth - 1);
+    unsigned long long k = static_cast<unsigned long long>(tags[i]);
+    k = (k << row_bits) | static_cast<unsigned long long>(v.mdt);
+    k = (k << col_bits) | static_cast<unsigned long long>(v.mt);
+    keys[i] = (k << wbits) | code;
+    vals[i] = i;
+}
+
+__global__ void k_gather_tagged(const bfs_cand* __restrict__ src, const int* __restrict__ tsrc,
+                                const unsigned* __restrict__ idx, unsigned n, bfs_cand* __restrict__ dst,
+                                int* __restrict__ tdst) {
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { dst[i] = src[idx[i]]; tdst[i] = tsrc[idx[i]]; }
+}
+}  // namespace
+
+// Canonical order across beams: (tag, row, sample, width); candidates and
+// their tags are permuted together (into dst / tdst).
+bfs_status sort_tagged_candidates(const bfs_cand* d_c, const int* d_tags, unsigned n, int max_rows,
+                                  int max_cols, int max_tag, int mode, int param, bfs_cand* d_dst,
+                                  int* d_tdst, cudaStream_t s) {
+    if (n == 0) return BFS_OK;
+    const int wbits = bits_for(static_cast<unsigned long long>(mode == 0 ? param : param - 1));
+    const int row_bits = bits_for(static_cast<unsigned long long>(max_rows - 1));
+    const int col_bits = bits_for(static_cast<unsigned long long>(max_cols - 1));
+    const int tag_bits = bits_for(static_cast<unsigned long long>(max_tag));
+    const int end_bit = tag_bits + row_bits + col_bits + wbits;
+    BFS_ARG(end_bit <= 64, "candidate key needs %d bits", end_bit);
+    unsigned long long* k = nullptr;
+    unsigned* v = nullptr;
+    void* tmp = nullptr;
+    size_t tmp_bytes = 0;
+    BFS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, k, k, v, v, static_cast<int>(n), 0,
+                                             end_bit > 0 ? end_bit : 1, s));
+    BFS_TRY_ST(stream_alloc(reinterpret_cast<void**>(&k), sizeof(unsigned long long) * 2 * n, s));
+    BFS_TRY_ST(stream_alloc(reinterpret_cast<void**>(&v), sizeof(unsigned) * 2 * n, s));
+    BFS_TRY_ST(stream_alloc(&tmp, tmp_bytes, s));
+    const int th = 256, bl = static_cast<int>((n + th - 1) / th);
+    k_tagged_keys<<<bl, th, 0, s>>>(d_c, d_tags, n, row_bits, col_bits, mode, wbits, k, v);
+    BFS_LAUNCH_CHECK("k_tagged_keys");
+    BFS_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k, k + n, v, v + n, static_cast<int>(n), 0,
+                                             end_bit > 0 ? end_bit : 1, s));
+    k_gather_tagged<<<bl, th, 0, s>>>(d_c, d_tags, v + n, n, d_dst, d_tdst);
+    BFS_LAUNCH_CHECK("k_gather_tagged");
+    BFS_CUDA(cudaFreeAsync(k, s));
+    BFS_CUDA(cudaFreeAsync(v, s));
+    BFS_CUDA(cudaFreeAsync(tmp, s));
+    return BFS_OK;
+}
+
 bfs_status launch_row_stats(const float* d_in, int rows, int cols, float* d_stats, int mode,
                             cudaStream_t s) {
     BFS_ARG(d_in && d_stats, "null argument");
@@ -362,7 +422,8 @@ bfs_status launch_row_stats(const float* d_in, int rows, int cols, float* d_stat
 
 bfs_status launch_boxcar(const float* d_plane, int rows, int cols, const float* d_stats,
                          float thr, const float* d_thr, int mode, int param, int snr_fast,
-                         bfs_cand* d_out, unsigned capacity, unsigned* d_count, cudaStream_t s) {
+                         bfs_cand* d_out, unsigned capacity, unsigned* d_count, cudaStream_t s,
+                         int tag, int* d_tags) {
     BFS_ARG(d_plane && d_count, "null argument");
     BFS_ARG(rows >= 1 && cols >= 1 && rows <= 65535, "bad shape %dx%d", rows, cols);
     BFS_ARG(capacity == 0 || d_out, "d_out is null");
@@ -387,7 +448,8 @@ bfs_status launch_boxcar(const float* d_plane, int rows, int cols, const float* 
         }
         bool launched = true;
 #define BFS_BOX_REG(M, W) k_boxcar_reg<M, W><<<grid_r, kBoxThreads, 0, s>>>(                  \
-            d_plane, rows, cols, d_stats, d_thr, thr, thr_lo, snr_fast, d_out, capacity, d_count, wc)
+            d_plane, rows, cols, d_stats, d_thr, thr, thr_lo, snr_fast, d_out, capacity, d_count, wc, \
+            tag, d_tags)
         if (mode == BFS_WIDTHS_POW2) {
             switch (wmax) {
                 case 1: BFS_BOX_REG(0, 1); break;
@@ -424,13 +486,13 @@ bfs_status launch_boxcar(const float* d_plane, int rows, int cols, const float* 
             BFS_CUDA(cudaFuncSetAttribute(k_boxcar<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           static_cast<int>(smem)));
         k_boxcar<0><<<grid, kBoxThreads, smem, s>>>(d_plane, rows, cols, d_stats, d_thr, thr, wmax,
-                                                    snr_fast, d_out, capacity, d_count);
+                                                    snr_fast, d_out, capacity, d_count, tag, d_tags);
     } else {
         if (smem > 48 * 1024)
             BFS_CUDA(cudaFuncSetAttribute(k_boxcar<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           static_cast<int>(smem)));
         k_boxcar<1><<<grid, kBoxThreads, smem, s>>>(d_plane, rows, cols, d_stats, d_thr, thr, wmax,
-                                                    snr_fast, d_out, capacity, d_count);
+                                                    snr_fast, d_out, capacity, d_count, tag, d_tags);
     }
     BFS_LAUNCH_CHECK("k_boxcar");
     return BFS_OK;
@@ -472,7 +534,7 @@ extern "C" bfs_status bfs_boxcar_gather(const float* d_plane, int rows, int cols
     BFS_TRY_ST(stream_alloc(reinterpret_cast<void**>(&d_count), sizeof(unsigned), s));
     BFS_CUDA(cudaMemsetAsync(d_count, 0, sizeof(unsigned), s));
     bfs_status st = launch_boxcar(d_plane, rows, cols, d_stats, thr, d_thr, widths_mode, param,
-                                  snr_fast, d_out, capacity, d_count, s);
+                                  snr_fast, d_out, capacity, d_count, s, 0, nullptr);
     unsigned count = 0;
     if (st == BFS_OK) {
         cudaError_t e = cudaMemcpyAsync(&count, d_count, sizeof(unsigned), cudaMemcpyDeviceToHost, s);

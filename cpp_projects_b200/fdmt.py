@@ -19,9 +19,20 @@ from . import _capi
 from ._tensors import dev_ptr, stream_handle
 
 
+def autotune(Fmin: float, Fmax: float, nchan: int, cols: int, imaxDt: int) -> tuple[int, int, float]:
+    """Time the fused-head depths and tile widths for this shape on the
+    current device (cached per shape): returns (fuse_depth, head_tile, ms)."""
+    desc = _capi.FdmtDesc(fmin=float(Fmin), fmax=float(Fmax), nchan=int(nchan), ncols=int(cols),
+                          max_dt=int(imaxDt))
+    depth, tile, ms = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_float(0)
+    _capi.call("bfs_fdmt_autotune", ctypes.byref(desc), ctypes.byref(depth), ctypes.byref(tile),
+               ctypes.byref(ms))
+    return depth.value, tile.value, ms.value
+
+
 class CFdmtGpu:
     def __init__(self, Fmin: float, Fmax: float, nchan: int, cols: int, imaxDt: int,
-                 fuse_depth: int = -1, external_ws: bool = False):
+                 fuse_depth: int = -1, external_ws: bool = False, head_tile: int = 0):
         self.m_Fmin = float(Fmin)
         self.m_Fmax = float(Fmax)
         self.m_nchan = int(nchan)
@@ -30,7 +41,8 @@ class CFdmtGpu:
         desc = _capi.FdmtDesc(fmin=self.m_Fmin, fmax=self.m_Fmax, nchan=self.m_nchan,
                               ncols=self.m_cols, max_dt=self.m_imaxDt, plan_kind=0,
                               precision=0, fuse_depth=int(fuse_depth),
-                              flags=_capi.BFS_FDMT_EXTERNAL_WS if external_ws else 0)
+                              flags=_capi.BFS_FDMT_EXTERNAL_WS if external_ws else 0,
+                              head_tile=int(head_tile))
         self._plan = ctypes.c_void_p()
         _capi.call("bfs_fdmt_plan_create", ctypes.byref(desc), ctypes.byref(self._plan))
         info = _capi.FdmtInfo()

@@ -21,6 +21,13 @@ from .cluster import complete_clusterization
 from .fdmt import CFdmtGpu
 
 
+def fdmt_launches(plan: CFdmtGpu) -> int:
+    """Kernels one FDMT launches: init + one per level, or the fused head
+    (init + the first ``depth`` levels) + one per remaining level."""
+    depth = plan.info.fuse_depth
+    return 1 + plan.m_iNumIter - depth
+
+
 @dataclass
 class BeamShape:
     nchan: int
@@ -33,8 +40,8 @@ class BeamShape:
 @dataclass
 class BeamResult:
     n_candidates: int
-    delegates: np.ndarray      # Cand records of the delegates, sorted by mt
-    group_sizes: np.ndarray
+    delegates: np.ndarray      # Cand records of the delegates, sorted by (mt, group)
+    group_sizes: np.ndarray    # size of each delegate's own group
 
 
 class SearchPipeline:
@@ -79,13 +86,13 @@ class SearchPipeline:
         search.launch_row_stats(plane, stats)
         cands, n = search.boxcar_gather(plane, self.thr, self.widths_mode, self.param,
                                         stats=stats, out=self.cands)
-        # init + one per level, row statistics, boxcar, canonical sort (keys + gather),
+        # FDMT, row statistics, boxcar, canonical sort (keys + gather),
         # clustering (3 passes x keys/flags/scatter, offsets, delegates, delegate keys)
-        self.launches += 1 + self.plans[i].m_iNumIter + 2 + (2 if n >= 2 else 0) + (12 if n else 0)
+        self.launches += fdmt_launches(self.plans[i]) + 2 + (2 if n >= 2 else 0) + (12 if n else 0)
         if n == 0:
             return BeamResult(0, np.zeros(0, search.CAND_DTYPE), np.zeros(0, np.int64))
         cl = complete_clusterization(cands, self.metrics)
-        return BeamResult(n, cl.delegate_records(), cl.group_sizes())
+        return BeamResult(n, cl.delegate_records(), cl.delegate_group_sizes())
 
     def run(self, inputs: list[torch.Tensor], fdmt_timing: list | None = None) -> list[BeamResult]:
         out = []
@@ -95,6 +102,86 @@ class SearchPipeline:
                 ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                 fdmt_timing.append(ev)
             out.append(self.run_beam(i, x, ev))
+        return out
+
+
+class BatchedSearch:
+    """All beams in one native batch (include/bfs.h bfs_batch_*): autotuned
+    FDMT plans, every beam's FDMT + row statistics + boxcar captured in one
+    CUDA graph, then one sort and one clustering for all beams."""
+
+    def __init__(self, shapes: list[BeamShape], widths_mode: int = 0, param: int = 5,
+                 thr: float = 7.0, metrics=(16, 8, 1 << 30), capacity: int = 1 << 26,
+                 fuse_depth: int = -2, use_graph: bool = True):
+        import ctypes
+        from . import _capi
+        self._capi = _capi
+        self.shapes = list(shapes)
+        descs = (_capi.FdmtDesc * len(shapes))()
+        for d, sh in zip(descs, shapes):
+            d.fmin, d.fmax, d.nchan, d.ncols, d.max_dt = sh.fmin, sh.fmax, sh.nchan, sh.nsamp, sh.max_dt
+            d.fuse_depth = fuse_depth
+        bd = _capi.BatchDesc(nbeams=len(shapes), beams=descs, widths_mode=widths_mode, param=param,
+                             thr=thr, capacity=capacity, use_graph=1 if use_graph else 0)
+        for i, m in enumerate(metrics):
+            bd.metrics[i] = int(m)
+        self._descs = descs
+        self._h = ctypes.c_void_p()
+        _capi.call("bfs_batch_create", ctypes.byref(bd), ctypes.byref(self._h))
+        self._ptrs = (ctypes.c_void_p * len(shapes))()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                self._capi.lib().bfs_batch_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @property
+    def chan_samples(self) -> int:
+        return sum(s.nchan * s.nsamp for s in self.shapes)
+
+    def launches_per_run(self, n_candidates: int) -> int:
+        """Kernels of this library one run launches (CUB's not counted): per
+        beam the FDMT, row statistics and boxcar; then the tagged sort (keys
+        + gather), clustering (3 passes x keys/flags/scatter, offsets,
+        delegate lanes/tree, delegate keys) and the per-beam split (inverse
+        permutation, delegate info, permutation, beam bounds)."""
+        import ctypes
+        k = 0
+        for d in self._descs:
+            info = self._capi.FdmtInfo()
+            p = ctypes.c_void_p()
+            dd = self._capi.FdmtDesc.from_buffer_copy(d)
+            if dd.fuse_depth == self._capi.BFS_FUSE_AUTOTUNE:  # the batch's plans: cached choice
+                from .fdmt import autotune
+                dd.fuse_depth, dd.head_tile, _ = autotune(dd.fmin, dd.fmax, dd.nchan, dd.ncols, dd.max_dt)
+            self._capi.call("bfs_fdmt_plan_create_host", ctypes.byref(dd), ctypes.byref(p))
+            self._capi.call("bfs_fdmt_plan_info", p, ctypes.byref(info))
+            self._capi.lib().bfs_fdmt_plan_destroy(p)
+            k += 1 + info.niter - info.fuse_depth + 2
+        return k + ((2 + 12 + 4) if n_candidates else 0)
+
+    def run(self, inputs: list[torch.Tensor], stream=None) -> list[BeamResult]:
+        import ctypes
+        from ._tensors import dev_ptr, stream_handle
+        for i, x in enumerate(inputs):
+            self._ptrs[i] = dev_ptr(x, torch.float32, "input")
+        self._capi.call("bfs_batch_run", self._h, self._ptrs, stream_handle(stream))
+        out = []
+        for b in range(len(self.shapes)):
+            nd, nc = ctypes.c_int(0), ctypes.c_uint32(0)
+            self._capi.call("bfs_batch_beam_results", self._h, b, None, None, 0, ctypes.byref(nd),
+                            ctypes.byref(nc))
+            rec = np.zeros(nd.value, search.CAND_DTYPE)
+            sizes = np.zeros(nd.value, np.int32)
+            if nd.value:
+                self._capi.call("bfs_batch_beam_results", self._h, b,
+                                rec.ctypes.data_as(ctypes.c_void_p), sizes.ctypes.data_as(ctypes.c_void_p),
+                                nd.value, ctypes.byref(nd), ctypes.byref(nc))
+            out.append(BeamResult(int(nc.value), rec, sizes.astype(np.int64)))
         return out
 
 

@@ -59,6 +59,7 @@ bfs_status bfs_trim_scratch(void);
 enum { BFS_PLAN_KEITH = 0 };
 enum { BFS_PREC_F32 = 0 };
 enum { BFS_FDMT_EXTERNAL_WS = 1 };
+enum { BFS_FUSE_AUTOTUNE = -2 };
 
 typedef struct bfs_fdmt_desc {
     float fmin;        /* MHz, lower band edge                          */
@@ -68,9 +69,11 @@ typedef struct bfs_fdmt_desc {
     int max_dt;        /* output rows (>= 1)                            */
     int plan_kind;     /* BFS_PLAN_KEITH                                */
     int precision;     /* BFS_PREC_F32                                  */
-    int fuse_depth;    /* -1 = autotuned; 0 = level-by-level; k = fuse levels 0..k in one kernel */
+    int fuse_depth;    /* BFS_FUSE_AUTOTUNE (-2): measured per shape (cached); -1: deepest
+                          head keeping 2 CTAs/SM; 0: level-by-level; k: fuse levels 0..k */
     int flags;         /* BFS_FDMT_EXTERNAL_WS: the plan allocates no planes; use _execute_ws */
-    int reserved[7];
+    int head_tile;     /* samples per CTA of the fused head (0 = 256)                  */
+    int reserved[6];
 } bfs_fdmt_desc;
 
 typedef struct bfs_fdmt_plan bfs_fdmt_plan;
@@ -85,6 +88,11 @@ typedef struct bfs_fdmt_info {
 } bfs_fdmt_info;
 
 bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc, bfs_fdmt_plan** plan);
+/* The autotuner alone (no reference counterpart): times fusion depths
+ * {0,2,3,4,5} x head tiles {256,512} on this shape with zero input (the
+ * kernels' cost does not depend on the values) and returns the fastest;
+ * results are cached per (nchan, max_dt, band, ncols rounded up to 2^k). */
+bfs_status bfs_fdmt_autotune(const bfs_fdmt_desc* desc, int* depth, int* head_tile, float* ms);
 /* Same plan without device resources (introspection only; execute fails). */
 bfs_status bfs_fdmt_plan_create_host(const bfs_fdmt_desc* desc, bfs_fdmt_plan** plan);
 bfs_status bfs_fdmt_plan_destroy(bfs_fdmt_plan* plan);
@@ -200,10 +208,52 @@ bfs_status bfs_boxcar_gather(const float* d_plane, int rows, int cols, const flo
 bfs_status bfs_cluster(const bfs_cand* d_cands, uint32_t n, const int* metrics /* host, 3 */,
                        int* d_perm, int* d_offsets, int* d_delegates, uint32_t* h_ngroups,
                        void* stream);
+/* bfs_cluster with initial groups (no reference counterpart; used by the
+ * batched runner to cluster many beams at once): candidate i starts in group
+ * d_group0[i] (0..ngroups0-1, non-decreasing in the candidate order), so no
+ * group ever spans two initial groups.  d_group0 = NULL is bfs_cluster. */
+bfs_status bfs_cluster_grouped(const bfs_cand* d_cands, uint32_t n, const int* d_group0,
+                               uint32_t ngroups0, const int* metrics, int* d_perm, int* d_offsets,
+                               int* d_delegates, uint32_t* h_ngroups, void* stream);
 /* The reference's per-group argmax on its own (select_delegates_kernel). */
 bfs_status bfs_select_delegates(const bfs_cand* d_cands, const int* d_perm, uint32_t n,
                                 const int* d_offsets, uint32_t ngroups, int* d_delegates,
                                 void* stream);
+
+/* ------------------------------------------------------------------------
+ * Batched multi-beam search (no single reference counterpart: it batches the
+ * reference's per-chunk FDMT + clusterization_main sequence over many beams).
+ * Every beam's FDMT (autotuned plans sharing one workspace), row statistics
+ * and boxcar are captured once into a CUDA graph and replayed; the candidates
+ * of all beams are sorted and clustered in one pass (beams are the initial
+ * groups, so no cluster spans two beams).  Results per beam: delegates in
+ * (mt, group) order with their group sizes.
+ * ---------------------------------------------------------------------- */
+typedef struct bfs_batch_desc {
+    int nbeams;
+    const bfs_fdmt_desc* beams;  /* per-beam FDMT descriptions (fuse_depth as usual) */
+    int widths_mode;             /* BFS_WIDTHS_POW2 / BFS_WIDTHS_ALL                  */
+    int param;                   /* Q or W                                           */
+    float thr;                   /* S/N threshold on the row-normalised planes       */
+    int metrics[3];              /* clustering metrics (mt, mdt, mwidth)             */
+    uint32_t capacity;           /* candidates over all beams (0 = 2^26)             */
+    int use_graph;               /* capture stage 1 in a CUDA graph                  */
+    int reserved[8];
+} bfs_batch_desc;
+
+typedef struct bfs_batch bfs_batch;
+
+bfs_status bfs_batch_create(const bfs_batch_desc* desc, bfs_batch** batch);
+bfs_status bfs_batch_destroy(bfs_batch* batch);
+/* d_inputs: host array of nbeams device pointers (nchan x ncols each).  The
+ * first run is eager; later runs replay the captured graph while the input
+ * pointers are unchanged (a new set is captured again).  Synchronises. */
+bfs_status bfs_batch_run(bfs_batch* batch, const float* const* d_inputs, void* stream);
+bfs_status bfs_batch_counts(const bfs_batch* batch, uint32_t* n_cands, uint32_t* n_groups);
+/* Host copies of one beam's delegates (cap entries) and group sizes. */
+bfs_status bfs_batch_beam_results(const bfs_batch* batch, int beam, bfs_cand* delegates,
+                                  int* group_sizes, int cap, int* n_delegates,
+                                  uint32_t* n_candidates);
 
 /* ------------------------------------------------------------------------
  * Coherent-dedispersion chunk stage.

@@ -5,7 +5,8 @@ import numpy as np
 import pytest
 import torch
 
-from cpp_projects_b200 import CFdmtGpu, synth
+from cpp_projects_b200 import BfsError, CFdmtGpu, synth
+from cpp_projects_b200._capi import BFS_ERR_ARG
 from oracle import pyoracle
 
 pytestmark = pytest.mark.gpu
@@ -39,6 +40,29 @@ def test_fdmt_bit_exact_vs_oracle(cuda, case, fuse):
     got = d_out.cpu().numpy()
     want = pyoracle.fdmt_f32(fmin, fmax, x, nchan, ncols, max_dt)
     assert np.array_equal(_bits(got), _bits(want))
+
+
+@pytest.mark.parametrize("case", CASES[:5] + CASES[8:])
+@pytest.mark.parametrize("fuse,tile", [(-2, 0), (3, 512), (5, 256), (2, 512)])
+def test_fdmt_autotuned_and_wide_tiles_bit_exact(cuda, case, fuse, tile):
+    fmin, fmax, nchan, ncols, max_dt = case
+    x = np.random.default_rng(12).standard_normal((nchan, ncols)).astype(np.float32)
+    try:
+        f = CFdmtGpu(fmin, fmax, nchan, ncols, max_dt, fuse_depth=fuse, head_tile=tile)
+    except BfsError as e:  # an explicit depth deeper than this plan's head allows
+        assert fuse > 0 and e.status == BFS_ERR_ARG
+        pytest.skip(f"fuse_depth {fuse} not usable for {nchan} channels")
+    d_out = torch.full((max_dt, ncols), float("nan"), device=cuda)
+    f.process_image(torch.from_numpy(x).to(cuda), d_out, False)
+    want = pyoracle.fdmt_f32(fmin, fmax, x, nchan, ncols, max_dt)
+    assert np.array_equal(_bits(d_out.cpu().numpy()), _bits(want))
+
+
+def test_autotune_returns_a_valid_choice(cuda):
+    from cpp_projects_b200.fdmt import autotune
+    depth, tile, ms = autotune(1200.0, 1600.0, 1024, 65536, 1024)
+    assert depth in (0, 2, 3, 4, 5) and tile in (256, 512) and ms > 0
+    assert autotune(1200.0, 1600.0, 1024, 65536, 1024)[:2] == (depth, tile)  # cached
 
 
 @pytest.mark.parametrize("fuse", [0, -1])
