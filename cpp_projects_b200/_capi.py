@@ -19,6 +19,7 @@ STATUS_NAMES = {0: "BFS_OK", 1: "BFS_ERR_ARG", 2: "BFS_ERR_CUDA", 3: "BFS_ERR_OV
 BFS_WIDTHS_POW2, BFS_WIDTHS_ALL = 0, 1
 BFS_FDMT_EXTERNAL_WS = 1
 BFS_FUSE_AUTOTUNE = -2
+BFS_PREC_F32, BFS_PREC_F16, BFS_PREC_BF16 = 0, 1, 2
 
 
 class BfsError(RuntimeError):

@@ -15,6 +15,17 @@
 // odd level that reaches HBM, with rows padded to a 128-byte pitch so every
 // merge level moves float4s whatever ncols is; the last level is written
 // straight into the caller's output (pitch ncols).
+//
+// Reduced precision (opt-in, BFS_PREC_F16 / BFS_PREC_BF16): the planes that
+// reach HBM between levels are stored as 16-bit values with a 128-byte row
+// pitch; every sum is still formed in FP32 and the last level writes FP32.
+// Row g of a stored plane holds v_g * 2^-e_g, e_g = ceil(log2(channels summed
+// into row g)): a power-of-two per-row scale (exact, so it adds no rounding)
+// that keeps the stored value within the input's own range (the row's channel
+// mean), so FP16 cannot overflow where FP32 input fits FP16.  Levels inside
+// the fused head stay FP32 in shared memory; only its output plane is stored.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -33,9 +44,10 @@ struct bfs_fdmt_plan {
     bool host_only = false;
     bool external_ws = false;
     int fuse_depth = 0;
-    int4* d_tab = nullptr;             // per level, per output row: {a, b, shift, 0}
+    int precision = BFS_PREC_F32;      // storage of the planes between levels
+    int4* d_tab = nullptr;             // per level, per output row: {a, b, shift, exps}
     std::vector<size_t> tab_off;       // offset of each level's table in d_tab
-    float* d_buf[2] = {nullptr, nullptr};
+    void* d_buf[2] = {nullptr, nullptr};
     size_t buf_rows[2] = {0, 0};
     size_t ws_bytes = 0;
     bfs::HeadPlan head;                     // fused levels 0..k (depth 0 = not used)
@@ -45,7 +57,7 @@ struct bfs_fdmt_plan {
         if (d_tab) cudaFree(d_tab);
         if (d_head_groups) cudaFree(d_head_groups);
         if (d_head_tab) cudaFree(d_head_tab);
-        for (float* b : d_buf)
+        for (void* b : d_buf)
             if (b) cudaFree(b);
     }
 };
@@ -57,20 +69,38 @@ constexpr int kInitThreads = 256;
 constexpr int kInitCols = 4;        // columns per thread (strided by the block)
 constexpr int kLevelThreads = 256;
 
-// Level 0.  grid: (ceil(ncols / (256*4)), nchan).
+// 16-bit storage helpers.  The scale 2^e is built from its exponent bits
+// (|e| < 127), so multiplying by it is exact.
+__device__ __forceinline__ float to_f32(__half v) { return __half2float(v); }
+__device__ __forceinline__ float to_f32(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <typename D> __device__ __forceinline__ D from_f32(float v);
+template <> __device__ __forceinline__ float from_f32<float>(float v) { return v; }
+template <> __device__ __forceinline__ __half from_f32<__half>(float v) { return __float2half_rn(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 from_f32<__nv_bfloat16>(float v) {
+    return __float2bfloat16_rn(v);
+}
+__device__ __forceinline__ float exp2_int(int e) { return __int_as_float((127 + e) << 23); }
+// exponents packed in a table row's w: input a | input b << 8 | output << 16 (signed bytes)
+__device__ __forceinline__ int exp_field(int w, int k) {
+    return static_cast<int>(static_cast<signed char>((w >> (8 * k)) & 0xff));
+}
+
+// Level 0.  grid: (ceil(ncols / (256*4)), nchan).  D = float, or the 16-bit
+// storage type (level-0 rows sum one channel: scale 2^0).
+template <typename D>
 __global__ void __launch_bounds__(kInitThreads)
-k_fdmt_init(const float* __restrict__ x, float* __restrict__ out, int ncols, int out_pitch,
+k_fdmt_init(const float* __restrict__ x, D* __restrict__ out, int ncols, int out_pitch,
             int rows_per_chan, int ones) {
     const int c = blockIdx.y;
     const float* xr = x + static_cast<size_t>(c) * ncols;
-    float* o = out + static_cast<size_t>(c) * rows_per_chan * out_pitch;
+    D* o = out + static_cast<size_t>(c) * rows_per_chan * out_pitch;
     const int base = blockIdx.x * (kInitThreads * kInitCols) + threadIdx.x;
 #pragma unroll
     for (int k = 0; k < kInitCols; ++k) {
         const int t = base + k * kInitThreads;
         if (t >= ncols) break;
         float v = ones ? 1.0f : __ldg(xr + t);
-        o[t] = v;
+        o[t] = from_f32<D>(v);
         for (int r = 1; r < rows_per_chan; ++r) {
             float w = 0.0f;
             if (t >= r) {
@@ -79,7 +109,7 @@ k_fdmt_init(const float* __restrict__ x, float* __restrict__ out, int ncols, int
                               static_cast<float>(r + 1));
                 w = v;
             }
-            o[static_cast<size_t>(r) * out_pitch + t] = w;
+            o[static_cast<size_t>(r) * out_pitch + t] = from_f32<D>(w);
         }
     }
 }
@@ -137,6 +167,122 @@ k_fdmt_level(const float* __restrict__ in, float* __restrict__ out, const int4* 
             if (t + 1 < ncols) ro[t + 1] = o.y;
             if (t + 2 < ncols) ro[t + 2] = o.z;
             if (t + 3 < ncols) ro[t + 3] = o.w;
+        }
+    }
+}
+
+// One merge level over 16-bit planes (S = __half or __nv_bfloat16).  The
+// input plane has a 128-byte pitch, so both rows move as aligned 8-element
+// (16-byte) vectors: the tail row directly; the head row, shifted by s = 8*sv
+// + r samples, as the aligned vector q - sv of each thread plus the one
+// before it, taken from the neighbouring lane by a warp shuffle (lane 0
+// loads its own), and the 8 wanted elements cut out of the pair with funnel
+// shifts.  Both rows are widened to FP32 and rescaled by their rows' 2^e
+// (exact); the sum is rounded once in FP32; the output is a 16-bit plane
+// (D = S, 8-element vectors after scaling by 2^-e_out) or the caller's FP32
+// plane (D = float, the last level).
+// grid: (rows, ceil(ceil(ncols / 8) / (256 * kLevel16Vecs)))
+constexpr int kLevel16Vecs = 2;
+
+// words[0..7] = the 16 elements of vectors (q-sv-1, q-sv); out = elements
+// P0..P0+7 (P0 = 8 - r, 1..7).
+template <int P0>
+__device__ __forceinline__ uint4 cut8(const uint32_t (&w)[8]) {
+    uint32_t o[4];
+    if constexpr ((P0 & 1) == 0) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) o[i] = w[P0 / 2 + i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) o[i] = __funnelshift_r(w[P0 / 2 + i], w[P0 / 2 + i + 1], 16);
+    }
+    return make_uint4(o[0], o[1], o[2], o[3]);
+}
+
+__device__ __forceinline__ uint4 cut8(const uint32_t (&w)[8], int p0) {
+    switch (p0) {
+        case 1: return cut8<1>(w);
+        case 2: return cut8<2>(w);
+        case 3: return cut8<3>(w);
+        case 4: return cut8<4>(w);
+        case 5: return cut8<5>(w);
+        case 6: return cut8<6>(w);
+        default: return cut8<7>(w);
+    }
+}
+
+template <typename S, typename D, bool VOUT>
+__global__ void __launch_bounds__(kLevelThreads)
+k_fdmt_level16(const S* __restrict__ in, D* __restrict__ out, const int4* __restrict__ tab,
+               int ncols, int in_pitch, int out_pitch) {
+    const int g = blockIdx.x;
+    const int4 e = __ldg(tab + g);
+    const float sa = exp2_int(exp_field(e.w, 0));
+    const float sb = exp2_int(exp_field(e.w, 1));
+    const float so = exp2_int(-exp_field(e.w, 2));
+    const uint4* ra = reinterpret_cast<const uint4*>(in + static_cast<size_t>(e.x) * in_pitch);
+    const uint4* rb = reinterpret_cast<const uint4*>(in + static_cast<size_t>(e.y < 0 ? e.x : e.y) * in_pitch);
+    D* ro = out + static_cast<size_t>(g) * out_pitch;
+    const int s = e.z;
+    const int sv = s >> 3, r = s & 7;
+    const bool has_b = e.y >= 0;
+    const int nv = (ncols + 7) >> 3;
+    const int lane = threadIdx.x & 31;
+    const int base = blockIdx.y * (kLevelThreads * kLevel16Vecs) + threadIdx.x;
+    const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+    uint4 va[kLevel16Vecs], vb[kLevel16Vecs];
+#pragma unroll
+    for (int k = 0; k < kLevel16Vecs; ++k) {
+        const int q = base + k * kLevelThreads;
+        va[k] = (q < nv) ? __ldg(ra + q) : zero;
+        // head row: aligned vector q - sv (and q - sv - 1 when r > 0); the
+        // shuffles run on every lane (warp-uniform: has_b and r are per row)
+        const int qh = q - sv;
+        uint4 hi = (has_b && qh >= 0 && qh < nv) ? __ldg(rb + qh) : zero;
+        if (has_b && r != 0) {
+            uint4 lo;
+            lo.x = __shfl_up_sync(0xffffffffu, hi.x, 1);
+            lo.y = __shfl_up_sync(0xffffffffu, hi.y, 1);
+            lo.z = __shfl_up_sync(0xffffffffu, hi.z, 1);
+            lo.w = __shfl_up_sync(0xffffffffu, hi.w, 1);
+            if (lane == 0) lo = (qh - 1 >= 0 && qh - 1 < nv) ? __ldg(rb + qh - 1) : zero;
+            const uint32_t w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+            hi = cut8(w, 8 - r);
+        }
+        vb[k] = hi;
+    }
+#pragma unroll
+    for (int k = 0; k < kLevel16Vecs; ++k) {
+        const int q = base + k * kLevelThreads;
+        if (q >= nv) continue;
+        const int t = 8 * q;
+        const S* ha = reinterpret_cast<const S*>(&va[k]);
+        const S* hb = reinterpret_cast<const S*>(&vb[k]);
+        float o[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            o[i] = __fmul_rn(to_f32(ha[i]), sa);
+            if (has_b && t + i >= s) o[i] = __fadd_rn(o[i], __fmul_rn(to_f32(hb[i]), sb));
+        }
+        if constexpr (sizeof(D) == 2) {
+            uint4 pk;
+            S* hp = reinterpret_cast<S*>(&pk);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) hp[i] = from_f32<S>(__fmul_rn(o[i], so));
+            reinterpret_cast<uint4*>(ro)[q] = pk;
+        } else {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int t0 = t + 4 * h;
+                if (VOUT && t0 + 4 <= ncols) {
+                    reinterpret_cast<float4*>(ro + t0)[0] =
+                        make_float4(o[4 * h], o[4 * h + 1], o[4 * h + 2], o[4 * h + 3]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        if (t0 + i < ncols) ro[t0 + i] = o[4 * h + i];
+                }
+            }
         }
     }
 }
@@ -202,12 +348,14 @@ __device__ __forceinline__ float head_merge(const float* __restrict__ src, int4 
     return (t >= e.z && u >= e.z) ? __fadd_rn(a, b) : a;
 }
 
-template <int R0C>
+template <int R0C, typename D>
 __global__ void __launch_bounds__(1024)
-k_fdmt_head(const float* __restrict__ x, float* __restrict__ out,
+k_fdmt_head(const float* __restrict__ x, D* __restrict__ out,
             const HeadGroup* __restrict__ groups, const int4* __restrict__ tab, int ncols,
             int out_pitch, int depth, int group, int rows_per_chan, int tile, int rows_a,
             int rows_b, int ones) {
+    // a 16-bit output plane holds the level-`depth` rows (2^depth channels each) / 2^depth
+    const float oscale = exp2_int(-depth);
     extern __shared__ float sm[];
     const int W = blockDim.x;
     const int u = threadIdx.x;
@@ -248,7 +396,11 @@ k_fdmt_head(const float* __restrict__ x, float* __restrict__ out,
             __syncthreads();
             float* tmp = src; src = dst; dst = tmp;
         } else {
-            float* o = out + static_cast<size_t>(__ldg(&hg->out_row0)) * out_pitch + t;
+            D* o = out + static_cast<size_t>(__ldg(&hg->out_row0)) * out_pitch + t;
+            auto put = [&](int row, float v) {
+                if constexpr (sizeof(D) == 4) o[static_cast<size_t>(row) * out_pitch] = from_f32<D>(v);
+                else o[static_cast<size_t>(row) * out_pitch] = from_f32<D>(__fmul_rn(v, oscale));
+            };
             int j = 0;
             for (; j + 4 <= rows; j += 4) {
                 const float v0 = head_merge(src, tb[j], u, t, W);
@@ -256,38 +408,41 @@ k_fdmt_head(const float* __restrict__ x, float* __restrict__ out,
                 const float v2 = head_merge(src, tb[j + 2], u, t, W);
                 const float v3 = head_merge(src, tb[j + 3], u, t, W);
                 if (writer) {
-                    o[static_cast<size_t>(j) * out_pitch] = v0;
-                    o[static_cast<size_t>(j + 1) * out_pitch] = v1;
-                    o[static_cast<size_t>(j + 2) * out_pitch] = v2;
-                    o[static_cast<size_t>(j + 3) * out_pitch] = v3;
+                    put(j, v0);
+                    put(j + 1, v1);
+                    put(j + 2, v2);
+                    put(j + 3, v3);
                 }
             }
             for (; j < rows; ++j) {
                 const float v = head_merge(src, tb[j], u, t, W);
-                if (writer) o[static_cast<size_t>(j) * out_pitch] = v;
+                if (writer) put(j, v);
             }
         }
     }
 }
 
-using HeadKernel = void (*)(const float*, float*, const HeadGroup*, const int4*, int, int, int, int,
+template <typename D>
+using HeadKernel = void (*)(const float*, D*, const HeadGroup*, const int4*, int, int, int, int,
                             int, int, int, int, int);
 
-HeadKernel head_kernel_for(int rows_per_chan) {
+template <typename D>
+HeadKernel<D> head_kernel_for(int rows_per_chan) {
     switch (rows_per_chan) {
-        case 1: return k_fdmt_head<1>;
-        case 2: return k_fdmt_head<2>;
-        case 3: return k_fdmt_head<3>;
-        case 4: return k_fdmt_head<4>;
-        default: return k_fdmt_head<0>;
+        case 1: return k_fdmt_head<1, D>;
+        case 2: return k_fdmt_head<2, D>;
+        case 3: return k_fdmt_head<3, D>;
+        case 4: return k_fdmt_head<4, D>;
+        default: return k_fdmt_head<0, D>;
     }
 }
 
 // Launches the fused head with its shared-memory opt-in.
-cudaError_t launch_head(const HeadPlan& hp, const FdmtPlanHost& h, const float* d_in, float* dst,
+template <typename D>
+cudaError_t launch_head(const HeadPlan& hp, const FdmtPlanHost& h, const float* d_in, D* dst,
                         int out_pitch, const HeadGroup* groups, const int* tab, int ones,
                         cudaStream_t s) {
-    HeadKernel kern = head_kernel_for(h.rows_per_chan0);
+    HeadKernel<D> kern = head_kernel_for<D>(h.rows_per_chan0);
     if (hp.smem_bytes > 48 * 1024) {
         // opt in once per (kernel, size) so later launches (also inside a
         // stream capture) make no attribute call
@@ -326,8 +481,27 @@ cudaError_t launch_level(const float* src, float* dst, const int4* tab, int rows
     return cudaGetLastError();
 }
 
-// Row pitch (floats) of the workspace planes: ncols rounded up to 128 bytes.
-inline int plane_pitch(int ncols) { return (ncols + 31) / 32 * 32; }
+// Launches one merge level over 16-bit planes.
+template <typename S, typename D>
+cudaError_t launch_level16(const S* src, D* dst, const int4* tab, int rows, int T, int in_pitch,
+                           int out_pitch, cudaStream_t s) {
+    const int span = kLevelThreads * kLevel16Vecs;
+    dim3 grid(rows, ((T + 7) / 8 + span - 1) / span);
+    if (grid.y > 65535) return cudaErrorInvalidConfiguration;
+    const bool vout = (out_pitch % 4 == 0) && (reinterpret_cast<uintptr_t>(dst) & 15) == 0;
+    if (sizeof(D) == 2 || vout)
+        k_fdmt_level16<S, D, true><<<grid, kLevelThreads, 0, s>>>(src, dst, tab, T, in_pitch, out_pitch);
+    else
+        k_fdmt_level16<S, D, false><<<grid, kLevelThreads, 0, s>>>(src, dst, tab, T, in_pitch, out_pitch);
+    return cudaGetLastError();
+}
+
+// Row pitch (elements) of the workspace planes: ncols rounded up to 128 bytes.
+inline int plane_pitch(int ncols, int elem_bytes = 4) {
+    const int per = 128 / elem_bytes;
+    return (ncols + per - 1) / per * per;
+}
+inline int elem_bytes_of(int precision) { return precision == BFS_PREC_F32 ? 4 : 2; }
 
 constexpr int kHeadTile = 256;
 constexpr size_t kHeadSmemTwoPerSm = 113 * 1024;  // two CTAs per SM
@@ -338,12 +512,38 @@ constexpr size_t kHeadSmemMax = 227 * 1024;
 
 using namespace bfs;
 
+// Scale exponent of every row of every level: ceil(log2(channels summed into
+// the row)); level-0 rows cover one channel, a merged row the channels of
+// its two inputs, a carried-over row those of its one input.
+static std::vector<std::vector<int>> row_exponents(const FdmtPlanHost& h) {
+    std::vector<std::vector<int>> cnt(h.niter + 1), ex(h.niter + 1);
+    cnt[0].assign(h.lv[0].total_rows(), 1);
+    for (int l = 1; l <= h.niter; ++l) {
+        const FdmtLevel& L = h.lv[l];
+        cnt[l].resize(L.total_rows());
+        for (int g = 0; g < L.total_rows(); ++g)
+            cnt[l][g] = cnt[l - 1][L.a_row[g]] + (L.b_row[g] >= 0 ? cnt[l - 1][L.b_row[g]] : 0);
+    }
+    for (int l = 0; l <= h.niter; ++l) {
+        ex[l].resize(cnt[l].size());
+        for (size_t g = 0; g < cnt[l].size(); ++g) {
+            int e = 0;
+            while ((1 << e) < cnt[l][g]) ++e;
+            ex[l][g] = e;
+        }
+    }
+    return ex;
+}
+
 static bfs_status plan_host_part(const bfs_fdmt_desc* desc, std::unique_ptr<bfs_fdmt_plan>& p) {
     BFS_ARG(desc != nullptr, "null argument");
     BFS_ARG(desc->plan_kind == BFS_PLAN_KEITH, "unsupported plan_kind %d", desc->plan_kind);
-    BFS_ARG(desc->precision == BFS_PREC_F32, "unsupported precision %d", desc->precision);
+    BFS_ARG(desc->precision == BFS_PREC_F32 || desc->precision == BFS_PREC_F16 ||
+                desc->precision == BFS_PREC_BF16,
+            "unsupported precision %d", desc->precision);
     p.reset(new bfs_fdmt_plan);
     p->host_only = true;
+    p->precision = desc->precision;
     bfs_status st = build_fdmt_plan(desc->fmin, desc->fmax, desc->nchan, desc->ncols,
                                     desc->max_dt, &p->host);
     if (st != BFS_OK) return st;
@@ -375,11 +575,11 @@ static inline int bfs_fdmt_plan_depth_of(int d) { return d; }
 // ---------------------------------------------------------------------------
 namespace {
 struct TuneKey {
-    int nchan, max_dt, cols_bucket;
+    int nchan, max_dt, cols_bucket, precision;
     uint32_t fmin_bits, fmax_bits;
     bool operator<(const TuneKey& o) const {
-        return std::tie(nchan, max_dt, cols_bucket, fmin_bits, fmax_bits) <
-               std::tie(o.nchan, o.max_dt, o.cols_bucket, o.fmin_bits, o.fmax_bits);
+        return std::tie(nchan, max_dt, cols_bucket, precision, fmin_bits, fmax_bits) <
+               std::tie(o.nchan, o.max_dt, o.cols_bucket, o.precision, o.fmin_bits, o.fmax_bits);
     }
 };
 struct TuneVal { int depth, tile; float ms; };
@@ -388,7 +588,7 @@ std::map<TuneKey, TuneVal> g_tune;
 
 TuneKey tune_key(const bfs_fdmt_desc& d) {
     TuneKey k{};
-    k.nchan = d.nchan; k.max_dt = d.max_dt;
+    k.nchan = d.nchan; k.max_dt = d.max_dt; k.precision = d.precision;
     int b = 0;
     while ((1 << b) < d.ncols && b < 30) ++b;
     k.cols_bucket = b;
@@ -515,14 +715,23 @@ extern "C" bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc_in, bfs_fdm
                             cudaMemcpyHostToDevice));
     }
 
-    // device row tables
+    // device row tables; with 16-bit planes w packs the per-row scale exponents
+    const std::vector<std::vector<int>> ex = row_exponents(h);
     std::vector<int4> tab;
     p->tab_off.assign(h.niter + 1, 0);
     for (int l = 1; l <= h.niter; ++l) {
         p->tab_off[l] = tab.size();
         const FdmtLevel& L = h.lv[l];
-        for (int g = 0; g < L.total_rows(); ++g)
-            tab.push_back(make_int4(L.a_row[g], L.b_row[g], L.shift[g], 0));
+        for (int g = 0; g < L.total_rows(); ++g) {
+            int w = 0;
+            if (p->precision != BFS_PREC_F32) {
+                const int ea = ex[l - 1][L.a_row[g]];
+                const int eb = L.b_row[g] >= 0 ? ex[l - 1][L.b_row[g]] : 0;
+                const int eo = l == h.niter ? 0 : ex[l][g];
+                w = (ea & 0xff) | ((eb & 0xff) << 8) | ((eo & 0xff) << 16);
+            }
+            tab.push_back(make_int4(L.a_row[g], L.b_row[g], L.shift[g], w));
+        }
     }
     if (!tab.empty()) {
         BFS_CUDA(cudaMalloc(&p->d_tab, tab.size() * sizeof(int4)));
@@ -534,9 +743,10 @@ extern "C" bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc_in, bfs_fdm
     for (int l = p->head.depth; l < h.niter; ++l)
         p->buf_rows[l & 1] = std::max(p->buf_rows[l & 1], static_cast<size_t>(h.lv[l].total_rows()));
     p->external_ws = (desc->flags & BFS_FDMT_EXTERNAL_WS) != 0;
+    const int eb = elem_bytes_of(p->precision);
     for (int b = 0; b < 2 && !p->external_ws; ++b) {
         if (p->buf_rows[b] == 0) continue;
-        const size_t bytes = p->buf_rows[b] * static_cast<size_t>(plane_pitch(h.ncols)) * sizeof(float);
+        const size_t bytes = p->buf_rows[b] * static_cast<size_t>(plane_pitch(h.ncols, eb)) * eb;
         cudaError_t e = cudaMalloc(&p->d_buf[b], bytes);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -574,10 +784,15 @@ extern "C" bfs_status bfs_fdmt_plan_head(const bfs_fdmt_plan* plan, int* params,
     return BFS_OK;
 }
 
-static double fdmt_alg_bytes(const FdmtPlanHost& h) {
-    double rows = h.nchan + h.lv[0].total_rows();
-    for (int l = 1; l <= h.niter; ++l) rows += 3.0 * h.lv[l].total_rows();
-    return 4.0 * rows * h.ncols;
+// Bytes of the level-by-level algorithm: the input read, the level-0 plane
+// written, each level's two input rows read and output row written per
+// output row; intermediate planes of eb bytes per value, the output FP32.
+static double fdmt_alg_bytes(const FdmtPlanHost& h, int precision) {
+    const double eb = elem_bytes_of(precision);
+    double bytes = 4.0 * h.nchan + eb * h.lv[0].total_rows();
+    for (int l = 1; l <= h.niter; ++l)
+        bytes += (l < h.niter ? 3.0 * eb : 2.0 * eb + 4.0) * h.lv[l].total_rows();
+    return bytes * h.ncols;
 }
 
 extern "C" bfs_status bfs_fdmt_plan_info(const bfs_fdmt_plan* plan, bfs_fdmt_info* info) {
@@ -590,7 +805,7 @@ extern "C" bfs_status bfs_fdmt_plan_info(const bfs_fdmt_plan* plan, bfs_fdmt_inf
     for (const auto& L : h.lv) tot += L.total_rows();
     info->rows_total = tot;
     info->workspace_bytes = plan->ws_bytes;
-    info->alg_bytes = fdmt_alg_bytes(h);
+    info->alg_bytes = fdmt_alg_bytes(h, plan->precision);
     return BFS_OK;
 }
 
@@ -614,7 +829,8 @@ extern "C" bfs_status bfs_fdmt_plan_tables(const bfs_fdmt_plan* plan, int level,
 }
 
 static size_t plane_bytes(const bfs_fdmt_plan* p, int b) {
-    const size_t raw = p->buf_rows[b] * static_cast<size_t>(plane_pitch(p->host.ncols)) * sizeof(float);
+    const int eb = elem_bytes_of(p->precision);
+    const size_t raw = p->buf_rows[b] * static_cast<size_t>(plane_pitch(p->host.ncols, eb)) * eb;
     return (raw + 255) & ~static_cast<size_t>(255);
 }
 
@@ -624,8 +840,53 @@ extern "C" bfs_status bfs_fdmt_workspace_size(const bfs_fdmt_plan* plan, size_t*
     return BFS_OK;
 }
 
+// The same schedule over 16-bit planes (storage type S).
+template <typename S>
+static bfs_status fdmt_run16(bfs_fdmt_plan* plan, const float* d_in, float* d_out, int b_ones,
+                             S* buf0, S* buf1, cudaStream_t s) {
+    const FdmtPlanHost& h = plan->host;
+    const int T = h.ncols;
+    const int P = plane_pitch(T, 2);
+    S* bufs[2] = {buf0, buf1};
+    const int k = plan->head.depth;
+    if (k > 0) {
+        const HeadPlan& hp = plan->head;
+        BFS_ARG(h.nchan / hp.group <= 65535, "nchan too large for this build");
+        cudaError_t e = (k == h.niter)
+            ? launch_head<float>(hp, h, d_in, d_out, T, plan->d_head_groups, plan->d_head_tab,
+                                 b_ones ? 1 : 0, s)
+            : launch_head<S>(hp, h, d_in, bufs[k & 1], P, plan->d_head_groups, plan->d_head_tab,
+                             b_ones ? 1 : 0, s);
+        if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_head: %s", cudaGetErrorString(e));
+    } else {
+        dim3 grid((T + kInitThreads * kInitCols - 1) / (kInitThreads * kInitCols), h.nchan);
+        BFS_ARG(grid.y <= 65535, "nchan too large for this build");
+        k_fdmt_init<S><<<grid, kInitThreads, 0, s>>>(d_in, bufs[0], T, P, h.rows_per_chan0,
+                                                     b_ones ? 1 : 0);
+        BFS_LAUNCH_CHECK("k_fdmt_init");
+    }
+    for (int l = k + 1; l <= h.niter; ++l) {
+        const S* src = bufs[(l - 1) & 1];
+        const int4* tab = plan->d_tab + plan->tab_off[l];
+        const int rows = h.lv[l].total_rows();
+        cudaError_t e = (l == h.niter)
+            ? launch_level16<S, float>(src, d_out, tab, rows, T, P, T, s)
+            : launch_level16<S, S>(src, bufs[l & 1], tab, rows, T, P, P, s);
+        if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_level16: %s", cudaGetErrorString(e));
+    }
+    return BFS_OK;
+}
+
 static bfs_status fdmt_run(bfs_fdmt_plan* plan, const float* d_in, float* d_out, int b_ones,
-                           float* buf0, float* buf1, cudaStream_t s) {
+                           void* buf0_, void* buf1_, cudaStream_t s) {
+    if (plan->precision == BFS_PREC_F16)
+        return fdmt_run16<__half>(plan, d_in, d_out, b_ones, static_cast<__half*>(buf0_),
+                                  static_cast<__half*>(buf1_), s);
+    if (plan->precision == BFS_PREC_BF16)
+        return fdmt_run16<__nv_bfloat16>(plan, d_in, d_out, b_ones, static_cast<__nv_bfloat16*>(buf0_),
+                                         static_cast<__nv_bfloat16*>(buf1_), s);
+    float* buf0 = static_cast<float*>(buf0_);
+    float* buf1 = static_cast<float*>(buf1_);
     const FdmtPlanHost& h = plan->host;
     const int T = h.ncols;
     const int P = plane_pitch(T);
@@ -635,14 +896,14 @@ static bfs_status fdmt_run(bfs_fdmt_plan* plan, const float* d_in, float* d_out,
         const HeadPlan& hp = plan->head;
         BFS_ARG(h.nchan / hp.group <= 65535, "nchan too large for this build");
         float* dst = (k == h.niter) ? d_out : bufs[k & 1];
-        cudaError_t e = launch_head(hp, h, d_in, dst, (k == h.niter) ? T : P, plan->d_head_groups,
-                                    plan->d_head_tab, b_ones ? 1 : 0, s);
+        cudaError_t e = launch_head<float>(hp, h, d_in, dst, (k == h.niter) ? T : P,
+                                           plan->d_head_groups, plan->d_head_tab, b_ones ? 1 : 0, s);
         if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_head: %s", cudaGetErrorString(e));
     } else {
         dim3 grid((T + kInitThreads * kInitCols - 1) / (kInitThreads * kInitCols), h.nchan);
         BFS_ARG(grid.y <= 65535, "nchan too large for this build");
-        k_fdmt_init<<<grid, kInitThreads, 0, s>>>(d_in, bufs[0], T, P, h.rows_per_chan0,
-                                                  b_ones ? 1 : 0);
+        k_fdmt_init<float><<<grid, kInitThreads, 0, s>>>(d_in, bufs[0], T, P, h.rows_per_chan0,
+                                                         b_ones ? 1 : 0);
         BFS_LAUNCH_CHECK("k_fdmt_init");
     }
     for (int l = k + 1; l <= h.niter; ++l) {
@@ -675,8 +936,7 @@ extern "C" bfs_status bfs_fdmt_execute_ws(bfs_fdmt_plan* plan, const float* d_in
             "workspace of %zu bytes is smaller than the %zu needed", workspace_bytes, need);
     BFS_ARG((reinterpret_cast<uintptr_t>(d_workspace) & 255) == 0, "workspace must be 256-byte aligned");
     char* w = static_cast<char*>(d_workspace);
-    return fdmt_run(plan, d_in, d_out, b_ones, reinterpret_cast<float*>(w),
-                    reinterpret_cast<float*>(w + plane_bytes(plan, 0)), as_stream(stream));
+    return fdmt_run(plan, d_in, d_out, b_ones, w, w + plane_bytes(plan, 0), as_stream(stream));
 }
 
 // ---------------------------------------------------------------------------
@@ -768,6 +1028,7 @@ extern "C" bfs_status bfs_fdmt_noalloc_scratch_bytes(const bfs_fdmt_plan* plan, 
 extern "C" bfs_status bfs_fdmt_execute_noalloc(const bfs_fdmt_plan* plan, const float* d_in,
                                                float* d_out, int b_ones, void* stream) {
     BFS_ARG(plan != nullptr && d_out != nullptr, "null argument");
+    BFS_ARG(plan->precision == BFS_PREC_F32, "the allocation-free entry point runs FP32 plans only");
     BFS_ARG(b_ones || d_in != nullptr, "d_in is null");
     size_t need = 0;
     bfs_status st = bfs_fdmt_noalloc_scratch_bytes(plan, &need, nullptr);
@@ -836,14 +1097,14 @@ extern "C" bfs_status bfs_fdmt_execute_noalloc(const bfs_fdmt_plan* plan, const 
                                  cudaMemcpyHostToDevice, s));
         BFS_ARG(h.nchan / hp.group <= 65535, "nchan too large for this build");
         float* dst = (k == h.niter) ? d_out : bufs[k & 1];
-        cudaError_t e = launch_head(hp, h, d_in, dst, (k == h.niter) ? T : P, groups, head_tab,
-                                    b_ones ? 1 : 0, s);
+        cudaError_t e = launch_head<float>(hp, h, d_in, dst, (k == h.niter) ? T : P, groups,
+                                           head_tab, b_ones ? 1 : 0, s);
         if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_head: %s", cudaGetErrorString(e));
     } else {
         dim3 grid((T + kInitThreads * kInitCols - 1) / (kInitThreads * kInitCols), h.nchan);
         BFS_ARG(grid.y <= 65535, "nchan too large for this build");
-        k_fdmt_init<<<grid, kInitThreads, 0, s>>>(d_in, bufs[0], T, P, h.rows_per_chan0,
-                                                  b_ones ? 1 : 0);
+        k_fdmt_init<float><<<grid, kInitThreads, 0, s>>>(d_in, bufs[0], T, P, h.rows_per_chan0,
+                                                         b_ones ? 1 : 0);
         BFS_LAUNCH_CHECK("k_fdmt_init");
     }
     for (int l = k + 1; l <= h.niter; ++l) {

@@ -32,15 +32,17 @@ def autotune(Fmin: float, Fmax: float, nchan: int, cols: int, imaxDt: int) -> tu
 
 class CFdmtGpu:
     def __init__(self, Fmin: float, Fmax: float, nchan: int, cols: int, imaxDt: int,
-                 fuse_depth: int = -1, external_ws: bool = False, head_tile: int = 0):
+                 fuse_depth: int = -1, external_ws: bool = False, head_tile: int = 0,
+                 precision: int = 0):
         self.m_Fmin = float(Fmin)
         self.m_Fmax = float(Fmax)
         self.m_nchan = int(nchan)
         self.m_cols = int(cols)
         self.m_imaxDt = int(imaxDt)
+        self.precision = int(precision)
         desc = _capi.FdmtDesc(fmin=self.m_Fmin, fmax=self.m_Fmax, nchan=self.m_nchan,
                               ncols=self.m_cols, max_dt=self.m_imaxDt, plan_kind=0,
-                              precision=0, fuse_depth=int(fuse_depth),
+                              precision=int(precision), fuse_depth=int(fuse_depth),
                               flags=_capi.BFS_FDMT_EXTERNAL_WS if external_ws else 0,
                               head_tile=int(head_tile))
         self._plan = ctypes.c_void_p()

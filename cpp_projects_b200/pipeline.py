@@ -47,13 +47,13 @@ class BeamResult:
 class SearchPipeline:
     def __init__(self, shapes: list[BeamShape], widths_mode: int = 0, param: int = 5,
                  thr: float = 7.0, metrics=(16, 8, 1 << 30), capacity: int = 1 << 26,
-                 device: torch.device | str = "cuda:0", fuse_depth: int = -1):
+                 device: torch.device | str = "cuda:0", fuse_depth: int = -1, precision: int = 0):
         self.device = torch.device(device)
         self.shapes = list(shapes)
         self.widths_mode, self.param, self.thr = widths_mode, param, float(thr)
         self.metrics = tuple(int(m) for m in metrics)
         self.plans = [CFdmtGpu(s.fmin, s.fmax, s.nchan, s.nsamp, s.max_dt, fuse_depth=fuse_depth,
-                               external_ws=True) for s in self.shapes]
+                               external_ws=True, precision=precision) for s in self.shapes]
         ws = max(p.workspace_size() for p in self.plans)
         self.workspace = torch.empty(ws, dtype=torch.uint8, device=self.device)
         plane = max(s.max_dt * s.nsamp for s in self.shapes)
@@ -112,7 +112,7 @@ class BatchedSearch:
 
     def __init__(self, shapes: list[BeamShape], widths_mode: int = 0, param: int = 5,
                  thr: float = 7.0, metrics=(16, 8, 1 << 30), capacity: int = 1 << 26,
-                 fuse_depth: int = -2, use_graph: bool = True):
+                 fuse_depth: int = -2, use_graph: bool = True, precision: int = 0):
         import ctypes
         from . import _capi
         self._capi = _capi
@@ -121,6 +121,7 @@ class BatchedSearch:
         for d, sh in zip(descs, shapes):
             d.fmin, d.fmax, d.nchan, d.ncols, d.max_dt = sh.fmin, sh.fmax, sh.nchan, sh.nsamp, sh.max_dt
             d.fuse_depth = fuse_depth
+            d.precision = precision
         bd = _capi.BatchDesc(nbeams=len(shapes), beams=descs, widths_mode=widths_mode, param=param,
                              thr=thr, capacity=capacity, use_graph=1 if use_graph else 0)
         for i, m in enumerate(metrics):
@@ -186,13 +187,15 @@ class BatchedSearch:
 
 
 def device_filterbank(nchan: int, nsamp: int, fmin: float, fmax: float, seed: int, pulses,
-                      device, out: torch.Tensor | None = None) -> torch.Tensor:
-    """Seeded N(0,1) filterbank generated on the device with the same pulse
-    model as synth.filterbank (the noise stream differs from numpy's)."""
+                      device, out: torch.Tensor | None = None, gain=None) -> torch.Tensor:
+    """Seeded N(0,1) filterbank generated on the device with the same gain
+    and pulse model as synth.filterbank (the noise stream differs from numpy's)."""
     from .synth import track
     g = torch.Generator(device=device).manual_seed(int(seed))
     x = out if out is not None else torch.empty((nchan, nsamp), dtype=torch.float32, device=device)
     x.normal_(generator=g)
+    if gain is not None:
+        x *= torch.as_tensor(np.asarray(gain, np.float32), device=device)[:, None]
     for p in pulses:
         tt = torch.from_numpy(track(nchan, fmin, fmax, p.t0, p.span)).to(device)
         cols = tt[:, None] + torch.arange(int(p.width), device=device)[None, :]

@@ -77,6 +77,27 @@ def config4(seed: int = 4) -> Beam:
     return Beam(1024, 65536, 1200.0, 1600.0, 1024, seed, pulses)
 
 
+def config3(seed: int = 3) -> Beam:
+    """4096 ch x 2^17 samples, 1100-1500 MHz, max delay 4096: N(0,1) noise
+    times a slow per-channel bandpass gain in [0.5, 2] (2 to the power of two
+    low-order sinusoids across the band), plus 20 pulses of width 1-64,
+    amplitude 1-3 and delay span 10-90 % of the max delay (the
+    reduced-precision FDMT case)."""
+    rng = np.random.default_rng(seed)
+    nchan, nsamp = 4096, 1 << 17
+    u = np.arange(nchan) / nchan
+    ph = rng.uniform(0.0, 2 * np.pi, 2)
+    gain = 2.0 ** (0.6 * np.sin(2 * np.pi * u + ph[0]) + 0.4 * np.sin(4 * np.pi * u + ph[1]))
+    pulses = []
+    for _ in range(20):
+        span = float(rng.uniform(0.1, 0.9) * (nchan - 1))
+        width = int(rng.integers(1, 65))
+        amp = float(rng.uniform(1.0, 3.0))
+        t0 = int(rng.integers(0, nsamp - int(span) - width))
+        pulses.append(Pulse(t0, span, width, amp))
+    return Beam(nchan, nsamp, 1100.0, 1500.0, nchan, seed, pulses, gain.astype(np.float32))
+
+
 CONFIG0_SEARCH = dict(widths_mode=0, param=5, thr=7.0, metrics=(16, 8, 1 << 30))
 
 
@@ -104,4 +125,5 @@ def config2(seed: int = 2, nbeams: int = 48, max_nchan: int = 4096) -> list[Beam
 
 def manifest(beams: list[Beam]) -> list[dict]:
     return [dict(nchan=b.nchan, nsamp=b.nsamp, max_dt=b.max_dt, seed=b.seed,
-                 pulses=[p.__dict__ for p in b.pulses]) for b in beams]
+                 pulses=[p.__dict__ for p in b.pulses],
+                 gain=None if b.gain is None else "per-channel, [0.5, 2]") for b in beams]

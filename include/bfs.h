@@ -57,7 +57,12 @@ bfs_status bfs_trim_scratch(void);
  * row d = delay d samples across the band.
  * ---------------------------------------------------------------------- */
 enum { BFS_PLAN_KEITH = 0 };
-enum { BFS_PREC_F32 = 0 };
+/* Storage of the FDMT planes between levels (no reference counterpart: the
+ * reference is FP32 throughout).  F16 / BF16 store those planes as 16-bit
+ * values, row g scaled by 2^-ceil(log2(channels summed into g)); sums are
+ * formed in FP32 and the output is FP32.  F32 is the default and the only
+ * precision bit-identical to the reference. */
+enum { BFS_PREC_F32 = 0, BFS_PREC_F16 = 1, BFS_PREC_BF16 = 2 };
 enum { BFS_FDMT_EXTERNAL_WS = 1 };
 enum { BFS_FUSE_AUTOTUNE = -2 };
 
@@ -68,7 +73,7 @@ typedef struct bfs_fdmt_desc {
     int ncols;         /* time samples per row (>= 1)                   */
     int max_dt;        /* output rows (>= 1)                            */
     int plan_kind;     /* BFS_PLAN_KEITH                                */
-    int precision;     /* BFS_PREC_F32                                  */
+    int precision;     /* BFS_PREC_F32 (default), BFS_PREC_F16, BFS_PREC_BF16 */
     int fuse_depth;    /* BFS_FUSE_AUTOTUNE (-2): measured per shape (cached); -1: deepest
                           head keeping 2 CTAs/SM; 0: level-by-level; k: fuse levels 0..k */
     int flags;         /* BFS_FDMT_EXTERNAL_WS: the plan allocates no planes; use _execute_ws */

@@ -15,6 +15,7 @@
 #include "oracle.h"
 
 #include <math.h>
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -150,9 +151,63 @@ int orc_fdmt_tables(float fmin, float fmax, int nchan, int max_dt, int level,
     return n;
 }
 
-#define DEFINE_RUN(NAME, T)                                                              \
-int NAME(float fmin, float fmax, int nchan, int cols, int max_dt,                        \
-         const T* in, T* out, int b_ones) {                                              \
+/* ---- reduced-precision planes -------------------------------------------
+ * The value of the binary16 (IEEE 754 half: 11 significant bits, exponent
+ * -14..15, subnormal quantum 2^-24) nearest to v, ties to even, as a float;
+ * beyond the largest finite half (65504) rounding gives infinity.  Scaling a
+ * float by a power of two is exact here, so the nearest multiple of the
+ * quantum is taken with nearbyintf (round-to-nearest-even mode). */
+static float round_f16(float v) {
+    if (isnan(v)) return v;
+    float a = fabsf(v);
+    if (a >= 65520.0f) return copysignf(INFINITY, v);
+    float q;
+    if (a < 6.103515625e-05f) { /* 2^-14: subnormal halves */
+        q = nearbyintf(a * 16777216.0f) / 16777216.0f;
+    } else {
+        int e;
+        frexpf(a, &e); /* a = m 2^e, m in [0.5, 1): quantum 2^(e-11) */
+        float sc = ldexpf(1.0f, 11 - e);
+        q = nearbyintf(a * sc) / sc;
+    }
+    return copysignf(q, v);
+}
+
+/* bfloat16: the upper 16 bits of the float, rounded to nearest even. */
+static float round_bf16(float v) {
+    if (isnan(v)) return v;
+    uint32_t u;
+    memcpy(&u, &v, 4);
+    u = (u + 0x7fffu + ((u >> 16) & 1u)) & 0xffff0000u;
+    memcpy(&v, &u, 4);
+    return v;
+}
+
+/* Plane of level l stored at 16 bits: row g keeps round(v * 2^-e_g) * 2^e_g,
+ * e_g = ceil(log2(channels summed into row g)). */
+static void round_plane(float* pl, int rows, int cols, const int* cnt, int prec) {
+    for (int g = 0; g < rows; ++g) {
+        int e = 0;
+        while ((1 << e) < cnt[g]) ++e;
+        float dn = ldexpf(1.0f, -e), up = ldexpf(1.0f, e);
+        float* r = pl + (size_t)g * cols;
+        for (int t = 0; t < cols; ++t) {
+            float x = r[t] * dn;
+            r[t] = (prec == ORC_PREC_BF16 ? round_bf16(x) : round_f16(x)) * up;
+        }
+    }
+}
+
+void orc_round16(const float* in, float* out, int64_t n, int prec) {
+    for (int64_t i = 0; i < n; ++i) out[i] = prec == ORC_PREC_BF16 ? round_bf16(in[i]) : round_f16(in[i]);
+}
+
+#define NO_ROUND(pl, rows, cols, cnt, prec) ((void)0)
+#define DO_ROUND(pl, rows, cols, cnt, prec) round_plane(pl, rows, cols, cnt, prec)
+
+#define DEFINE_RUN(NAME, T, ROUND)                                                       \
+static int NAME(float fmin, float fmax, int nchan, int cols, int max_dt,                 \
+                const T* in, T* out, int b_ones, int prec, int kstore) {                 \
     oplan p;                                                                             \
     if (plan_build(&p, fmin, fmax, nchan, max_dt) || cols < 1) { plan_free(&p); return -1; } \
     int maxr[2] = {0, 0};                                                                \
@@ -165,6 +220,10 @@ int NAME(float fmin, float fmax, int nchan, int cols, int max_dt,               
     pl[0] = (T*)calloc((size_t)maxr[0] * cols, sizeof(T));                               \
     pl[1] = (T*)calloc((size_t)(maxr[1] > 0 ? maxr[1] : 1) * cols, sizeof(T));          \
     int nr0 = p.rows[0][0];                                                              \
+    int* cnt[2];                                 /* channels summed per row */           \
+    cnt[0] = (int*)malloc(sizeof(int) * (size_t)(maxr[0] > maxr[1] ? maxr[0] : maxr[1]) + 4); \
+    cnt[1] = (int*)malloc(sizeof(int) * (size_t)(maxr[0] > maxr[1] ? maxr[0] : maxr[1]) + 4); \
+    for (int g = 0; g < nchan * nr0; ++g) cnt[0][g] = 1;                                 \
     /* level 0: row r of channel c is the running mean of x[t-r..t]; 0 for t < r */      \
     for (int c = 0; c < nchan; ++c) {                                                    \
         T* base = pl[0] + (size_t)c * nr0 * cols;                                        \
@@ -181,6 +240,7 @@ int NAME(float fmin, float fmax, int nchan, int cols, int max_dt,               
             }                                                                            \
         }                                                                                \
     }                                                                                    \
+    if (prec && kstore == 0 && p.niter > 0) ROUND(pl[0], nchan * nr0, cols, cnt[0], prec); \
     int rmax = 0;                                                                        \
     for (int l = 1; l <= p.niter; ++l) { int r = p.cum[l][p.nsub[l]]; if (r > rmax) rmax = r; } \
     int* a = (int*)malloc(sizeof(int) * (rmax + 1));                                     \
@@ -193,17 +253,35 @@ int NAME(float fmin, float fmax, int nchan, int cols, int max_dt,               
         for (int g = 0; g < nr; ++g) {                                                   \
             const T* ra = src + (size_t)a[g] * cols;                                     \
             T* ro = dst + (size_t)g * cols;                                              \
+            cnt[l & 1][g] = cnt[(l - 1) & 1][a[g]] + (b[g] >= 0 ? cnt[(l - 1) & 1][b[g]] : 0); \
             if (b[g] < 0) { memcpy(ro, ra, sizeof(T) * cols); continue; }                \
             const T* rb = src + (size_t)b[g] * cols;                                     \
             int sh = s[g];                                                               \
             for (int t = 0; t < cols; ++t) ro[t] = (t >= sh) ? ra[t] + rb[t - sh] : ra[t]; \
         }                                                                                \
+        if (prec && l >= kstore && l < p.niter) ROUND(dst, nr, cols, cnt[l & 1], prec);  \
     }                                                                                    \
     memcpy(out, pl[p.niter & 1], sizeof(T) * (size_t)max_dt * cols);                    \
-    free(a); free(b); free(s); free(pl[0]); free(pl[1]);                                 \
+    free(a); free(b); free(s); free(pl[0]); free(pl[1]); free(cnt[0]); free(cnt[1]);     \
     plan_free(&p);                                                                       \
     return 0;                                                                            \
 }
 
-DEFINE_RUN(orc_fdmt_run_f32, float)
-DEFINE_RUN(orc_fdmt_run_f64, double)
+DEFINE_RUN(run_f32, float, DO_ROUND)
+DEFINE_RUN(run_f64, double, NO_ROUND)
+
+int orc_fdmt_run_f32(float fmin, float fmax, int nchan, int cols, int max_dt,
+                     const float* in, float* out, int b_ones) {
+    return run_f32(fmin, fmax, nchan, cols, max_dt, in, out, b_ones, 0, 0);
+}
+
+int orc_fdmt_run_f64(float fmin, float fmax, int nchan, int cols, int max_dt,
+                     const double* in, double* out, int b_ones) {
+    return run_f64(fmin, fmax, nchan, cols, max_dt, in, out, b_ones, 0, 0);
+}
+
+int orc_fdmt_run_lowp(float fmin, float fmax, int nchan, int cols, int max_dt,
+                      const float* in, float* out, int b_ones, int prec, int kstore) {
+    if (prec != ORC_PREC_F16 && prec != ORC_PREC_BF16) return -3;
+    return run_f32(fmin, fmax, nchan, cols, max_dt, in, out, b_ones, prec, kstore);
+}

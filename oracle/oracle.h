@@ -35,6 +35,15 @@ int orc_fdmt_run_f32(float fmin, float fmax, int nchan, int cols, int max_dt,
                      const float* in, float* out, int b_ones);
 int orc_fdmt_run_f64(float fmin, float fmax, int nchan, int cols, int max_dt,
                      const double* in, double* out, int b_ones);
+/* The FP32 FDMT with the planes of levels kstore..niter-1 rounded as a
+ * 16-bit store would round them (prec ORC_PREC_F16 / ORC_PREC_BF16), row g
+ * scaled by 2^-ceil(log2(channels summed into g)) first; levels below kstore
+ * (a fused head's shared-memory levels) stay FP32. */
+enum { ORC_PREC_F16 = 1, ORC_PREC_BF16 = 2 };
+int orc_fdmt_run_lowp(float fmin, float fmax, int nchan, int cols, int max_dt,
+                      const float* in, float* out, int b_ones, int prec, int kstore);
+/* out[i] = in[i] rounded to the nearest binary16 / bfloat16 (ties to even). */
+void orc_round16(const float* in, float* out, int64_t n, int prec);
 
 /* --- search (reference: MyVSLib_C++/Clusterization/ sources) --------------- */
 int64_t orc_boxcar(const float* plane, int rows, int cols, float thr, int mode,

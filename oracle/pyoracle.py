@@ -149,6 +149,29 @@ def fdmt_f64(fmin, fmax, x: np.ndarray | None, nchan, ncols, max_dt, b_ones=Fals
     return out
 
 
+PREC_F16, PREC_BF16 = 1, 2
+
+
+def fdmt_lowp(fmin, fmax, x: np.ndarray | None, nchan, ncols, max_dt, prec: int, kstore: int,
+              b_ones=False) -> np.ndarray:
+    """The FP32 FDMT whose planes of levels kstore..niter-1 are rounded to
+    FP16 (prec 1) or BF16 (prec 2) with the per-row power-of-two scale."""
+    out = np.zeros((max_dt, ncols), np.float32)
+    xin = np.zeros(1, np.float32) if b_ones else np.ascontiguousarray(x, np.float32)
+    rc = lib().orc_fdmt_run_lowp(_F(fmin), _F(fmax), nchan, ncols, max_dt, _ptr(xin), _ptr(out),
+                                 1 if b_ones else 0, int(prec), int(kstore))
+    if rc != 0:
+        raise ValueError(f"oracle FDMT failed ({rc})")
+    return out
+
+
+def round16(x: np.ndarray, prec: int) -> np.ndarray:
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty_like(x)
+    lib().orc_round16(_ptr(x), _ptr(out), ctypes.c_int64(x.size), int(prec))
+    return out
+
+
 def ref_fdmt_cpu(fmin, fmax, x: np.ndarray | None, nchan, ncols, max_dt, b_ones=False,
                  threads=1) -> np.ndarray | None:
     """Runs the reference's CFdmtCpu::process_image (None if not built)."""
