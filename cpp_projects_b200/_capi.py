@@ -95,6 +95,11 @@ _SIGNATURES = {
     "bfs_cluster": (_I, [_P, _U32, _P, _P, _P, _P, ctypes.POINTER(_U32), _P]),
     "bfs_select_delegates": (_I, [_P, _P, _U32, _P, _U32, _P, _P]),
     "bfs_cluster_grouped": (_I, [_P, _U32, _P, _U32, _P, _P, _P, _P, ctypes.POINTER(_U32), _P]),
+    "bfs_fdmt_adjoint": (_I, [_P, _P, _P, _P]),
+    "bfs_fdmt_adjoint_workspace_size": (_I, [_P, ctypes.POINTER(ctypes.c_size_t)]),
+    "bfs_fdmt_adjoint_ws": (_I, [_P, _P, _P, _P, ctypes.c_size_t, _P]),
+    "bfs_boxcar_snr_cells": (_I, [_P, _I, _I, _P, _P, _I, _P, _P]),
+    "bfs_boxcar_snr_cells_adjoint": (_I, [_P, _I, _I, _P, _P, _I, _P, _P, _P, _P]),
     "bfs_batch_create": (_I, [ctypes.POINTER(BatchDesc), ctypes.POINTER(_P)]),
     "bfs_batch_destroy": (_I, [_P]),
     "bfs_batch_run": (_I, [_P, _P, _P]),

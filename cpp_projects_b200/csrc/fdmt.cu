@@ -38,29 +38,7 @@
 
 #include "internal.h"
 
-struct bfs_fdmt_plan {
-    bfs::FdmtPlanHost host;
-    int device = -1;
-    bool host_only = false;
-    bool external_ws = false;
-    int fuse_depth = 0;
-    int precision = BFS_PREC_F32;      // storage of the planes between levels
-    int4* d_tab = nullptr;             // per level, per output row: {a, b, shift, exps}
-    std::vector<size_t> tab_off;       // offset of each level's table in d_tab
-    void* d_buf[2] = {nullptr, nullptr};
-    size_t buf_rows[2] = {0, 0};
-    size_t ws_bytes = 0;
-    bfs::HeadPlan head;                     // fused levels 0..k (depth 0 = not used)
-    bfs::HeadGroup* d_head_groups = nullptr;
-    int* d_head_tab = nullptr;
-    ~bfs_fdmt_plan() {
-        if (d_tab) cudaFree(d_tab);
-        if (d_head_groups) cudaFree(d_head_groups);
-        if (d_head_tab) cudaFree(d_head_tab);
-        for (void* b : d_buf)
-            if (b) cudaFree(b);
-    }
-};
+#include "fdmt_plan.h"
 
 namespace bfs {
 namespace {

@@ -70,6 +70,18 @@ struct FdmtPlanHost {
 bfs_status build_fdmt_plan(float fmin, float fmax, int nchan, int ncols, int max_dt,
                            FdmtPlanHost* out);
 
+// Inverse row tables of the adjoint: for level l >= 1 and every row i of the
+// level-(l-1) plane, the level-l rows g that read row i, with the shift of
+// the read (0 as the tail row a_g, s_g as the head row b_g), in ascending g.
+struct AdjointTables {
+    std::vector<size_t> off_pos;  // per level: start of its nrows+1 offsets in `off`
+    std::vector<size_t> ent_pos;  // per level: start of its entries in `ent`
+    std::vector<int> off;         // CSR offsets (relative to the level's entries)
+    std::vector<int> ent;         // pairs {g, shift}
+    bool built = false;
+};
+void build_adjoint_tables(const FdmtPlanHost& p, AdjointTables* out);
+
 // ---------------------------------------------------------------------------
 // Fused "head" of the FDMT: levels 0..k of one group of 2^k adjacent channels
 // computed by one CTA over a time tile, all intermediate levels in shared

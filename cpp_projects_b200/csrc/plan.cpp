@@ -217,4 +217,40 @@ bool build_head_plan(const FdmtPlanHost& p, int k, int tile, size_t smem_limit, 
     return true;
 }
 
+
+void build_adjoint_tables(const FdmtPlanHost& p, AdjointTables* out) {
+    out->off_pos.assign(p.niter + 1, 0);
+    out->ent_pos.assign(p.niter + 1, 0);
+    out->off.clear();
+    out->ent.clear();
+    for (int l = 1; l <= p.niter; ++l) {
+        const FdmtLevel& L = p.lv[l];
+        const int nin = p.lv[l - 1].total_rows();
+        const int nout = L.total_rows();
+        std::vector<int> cnt(nin + 1, 0);
+        for (int g = 0; g < nout; ++g) {
+            ++cnt[L.a_row[g] + 1];
+            if (L.b_row[g] >= 0) ++cnt[L.b_row[g] + 1];
+        }
+        for (int i = 0; i < nin; ++i) cnt[i + 1] += cnt[i];
+        out->off_pos[l] = out->off.size();
+        out->ent_pos[l] = out->ent.size() / 2;
+        out->off.insert(out->off.end(), cnt.begin(), cnt.end());
+        std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+        std::vector<int> ent(2 * static_cast<size_t>(cnt[nin]));
+        for (int g = 0; g < nout; ++g) {  // ascending g: each row's list is in g order
+            int k = fill[L.a_row[g]]++;
+            ent[2 * k] = g;
+            ent[2 * k + 1] = 0;
+            if (L.b_row[g] >= 0) {
+                k = fill[L.b_row[g]]++;
+                ent[2 * k] = g;
+                ent[2 * k + 1] = L.shift[g];
+            }
+        }
+        out->ent.insert(out->ent.end(), ent.begin(), ent.end());
+    }
+    out->built = true;
+}
+
 }  // namespace bfs

@@ -89,6 +89,32 @@ class CFdmtGpu:
                    ctypes.c_size_t(workspace.numel() * workspace.element_size()),
                    stream_handle(stream))
 
+    # --- adjoint -------------------------------------------------------------
+    def adjoint(self, d_grad_out: torch.Tensor, d_grad_in: torch.Tensor | None = None,
+                stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+        """d_grad_in (nchan x cols) = F^T d_grad_out (imaxDt x cols)."""
+        if d_grad_out.numel() != self.m_imaxDt * self.m_cols:
+            raise ValueError(f"d_grad_out must hold {self.m_imaxDt}x{self.m_cols} floats")
+        if d_grad_in is None:
+            d_grad_in = torch.empty((self.m_nchan, self.m_cols), dtype=torch.float32,
+                                    device=d_grad_out.device)
+        if d_grad_in.numel() != self.m_nchan * self.m_cols:
+            raise ValueError(f"d_grad_in must hold {self.m_nchan}x{self.m_cols} floats")
+        _capi.call("bfs_fdmt_adjoint", self._plan, dev_ptr(d_grad_out, torch.float32, "d_grad_out"),
+                   dev_ptr(d_grad_in, torch.float32, "d_grad_in"), stream_handle(stream))
+        return d_grad_in
+
+    def adjoint_workspace_size(self) -> int:
+        n = ctypes.c_size_t(0)
+        _capi.call("bfs_fdmt_adjoint_workspace_size", self._plan, ctypes.byref(n))
+        return int(n.value)
+
+    def adjoint_ws(self, d_grad_out: torch.Tensor, d_grad_in: torch.Tensor, workspace: torch.Tensor,
+                   stream: torch.cuda.Stream | None = None) -> None:
+        _capi.call("bfs_fdmt_adjoint_ws", self._plan, dev_ptr(d_grad_out, torch.float32, "d_grad_out"),
+                   dev_ptr(d_grad_in, torch.float32, "d_grad_in"), dev_ptr(workspace, None, "workspace"),
+                   ctypes.c_size_t(workspace.numel() * workspace.element_size()), stream_handle(stream))
+
     # --- plan introspection ------------------------------------------------
     def rows_per_level(self) -> np.ndarray:
         rows = np.zeros(self.m_iNumIter + 1, np.int32)

@@ -187,7 +187,7 @@ class BatchedSearch:
 
 
 def device_filterbank(nchan: int, nsamp: int, fmin: float, fmax: float, seed: int, pulses,
-                      device, out: torch.Tensor | None = None, gain=None) -> torch.Tensor:
+                      device, out: torch.Tensor | None = None, gain=None, rfi=()) -> torch.Tensor:
     """Seeded N(0,1) filterbank generated on the device with the same gain
     and pulse model as synth.filterbank (the noise stream differs from numpy's)."""
     from .synth import track
@@ -196,6 +196,10 @@ def device_filterbank(nchan: int, nsamp: int, fmin: float, fmax: float, seed: in
     x.normal_(generator=g)
     if gain is not None:
         x *= torch.as_tensor(np.asarray(gain, np.float32), device=device)[:, None]
+    if len(rfi):
+        t = torch.arange(nsamp, dtype=torch.float64, device=device)
+        for c, f, ph, a in rfi:
+            x[c] += (a * torch.sin(2 * np.pi * f * t + ph)).float()
     for p in pulses:
         tt = torch.from_numpy(track(nchan, fmin, fmax, p.t0, p.span)).to(device)
         cols = tt[:, None] + torch.arange(int(p.width), device=device)[None, :]

@@ -101,3 +101,41 @@ def gather_candidates_in_heap_with_plan(d_fdmt: torch.Tensor, Rows: int, Cols: i
                                         d_VAlTresh, WndWidth: int, **kw):
     plane = d_fdmt.view(Rows, Cols)
     return boxcar_gather(plane, d_VAlTresh, _capi.BFS_WIDTHS_ALL, WndWidth, **kw)
+
+
+# ---- S/N at cells and its gradient --------------------------------------------
+def _cells_tensor(cells, rows: int, cols: int, device) -> torch.Tensor:
+    c = torch.as_tensor(cells, dtype=torch.int32).reshape(-1, 3)
+    ch = c.cpu()
+    if len(ch) and not (bool((ch[:, 0] >= 0).all()) and bool((ch[:, 0] < rows).all())
+                        and bool((ch[:, 1] >= 0).all()) and bool((ch[:, 2] >= 1).all())
+                        and bool((ch[:, 1] + ch[:, 2] <= cols).all())):
+        raise ValueError("cells must be {row, start, width} inside the plane")
+    return c.to(device).contiguous()
+
+
+def snr_cells(plane: torch.Tensor, stats: torch.Tensor, cells, stream=None) -> torch.Tensor:
+    """Boxcar S/N at cells (n x {row, start, width}) of the plane normalised
+    by ``stats`` (means, stds); the same value the boxcar search reports."""
+    rows, cols = plane.shape
+    c = _cells_tensor(cells, rows, cols, plane.device)
+    out = torch.empty(c.shape[0], dtype=torch.float32, device=plane.device)
+    _capi.call("bfs_boxcar_snr_cells", dev_ptr(plane, torch.float32, "plane"), rows, cols,
+               dev_ptr(stats, torch.float32, "stats"), dev_ptr(c), int(c.shape[0]), dev_ptr(out),
+               stream_handle(stream))
+    return out
+
+
+def snr_cells_adjoint(plane: torch.Tensor, stats: torch.Tensor, cells, snr: torch.Tensor,
+                      gsnr: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    """Gradient of sum_k gsnr[k] * S_k with respect to the plane (the row
+    statistics' dependence on the plane included)."""
+    rows, cols = plane.shape
+    c = _cells_tensor(cells, rows, cols, plane.device)
+    out = torch.empty_like(plane) if out is None else out
+    _capi.call("bfs_boxcar_snr_cells_adjoint", dev_ptr(plane, torch.float32, "plane"), rows, cols,
+               dev_ptr(stats, torch.float32, "stats"), dev_ptr(c), int(c.shape[0]),
+               dev_ptr(snr, torch.float32, "snr"), dev_ptr(gsnr.contiguous(), torch.float32, "gsnr"),
+               dev_ptr(out, torch.float32, "out"), stream_handle(stream))
+    return out
+

@@ -34,6 +34,7 @@ class Beam:
     seed: int
     pulses: list = field(default_factory=list)
     gain: np.ndarray | None = None   # optional per-channel bandpass gain
+    rfi: list = field(default_factory=list)  # (channel, cycles per sample, phase, amplitude)
 
 
 def channel_centres(nchan: int, fmin: float, fmax: float) -> np.ndarray:
@@ -51,6 +52,9 @@ def filterbank(beam: Beam) -> np.ndarray:
     x = rng.standard_normal((beam.nchan, beam.nsamp), dtype=np.float32)
     if beam.gain is not None:
         x *= beam.gain[:, None].astype(np.float32)
+    t = np.arange(beam.nsamp, dtype=np.float64)
+    for c, f, ph, a in beam.rfi:
+        x[c] += (a * np.sin(2 * np.pi * f * t + ph)).astype(np.float32)
     for p in beam.pulses:
         tt = track(beam.nchan, beam.fmin, beam.fmax, p.t0, p.span)
         for c in range(beam.nchan):
@@ -68,13 +72,19 @@ def config0(seed: int = 1) -> Beam:
     return Beam(512, 32768, 1200.0, 1600.0, 512, seed, [Pulse(10000, 256.0, 4, 2.0)])
 
 
-def config4(seed: int = 4) -> Beam:
+def config4(seed: int = 4, rfi: bool = False) -> Beam:
     """1024 ch x 65536 samples, 1200-1600 MHz, max delay 1024, N(0,1) noise
-    plus 8 injected pulses (the forward shape of the differentiable-FDMT case)."""
+    plus 8 injected pulses (the differentiable-FDMT case); with ``rfi``, 10 %
+    of the channels also carry a narrowband sinusoid of amplitude 5."""
     rng = np.random.default_rng(seed)
     pulses = [Pulse(int(rng.integers(0, 60000)), float(rng.uniform(0.1, 0.9) * 1023),
                     int(rng.integers(1, 33)), float(rng.uniform(1.0, 3.0))) for _ in range(8)]
-    return Beam(1024, 65536, 1200.0, 1600.0, 1024, seed, pulses)
+    lines = []
+    if rfi:
+        chans = rng.choice(1024, 102, replace=False)
+        lines = [(int(c), float(rng.uniform(0.005, 0.25)), float(rng.uniform(0, 2 * np.pi)), 5.0)
+                 for c in sorted(chans)]
+    return Beam(1024, 65536, 1200.0, 1600.0, 1024, seed, pulses, rfi=lines)
 
 
 def config3(seed: int = 3) -> Beam:

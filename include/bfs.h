@@ -143,6 +143,21 @@ bfs_status bfs_fdmt_execute_noalloc(const bfs_fdmt_plan* plan, const float* d_in
 bfs_status bfs_fdmt_noalloc_scratch_bytes(const bfs_fdmt_plan* plan, size_t* need,
                                           size_t* capacity);
 
+/* Adjoint (transpose) of the FDMT: d_grad_in (nchan x ncols) = F^T d_grad_out
+ * (max_dt x ncols), with F the plan's linear transform (b_ones = 0).  No
+ * reference counterpart (the reference has no gradients).  Each level's
+ * adjoint is a gather over inverse row tables in a fixed order, so the FP32
+ * result is deterministic; it needs no forward planes (every level is
+ * linear).  Computed in FP32 whatever the plan's precision.  The first
+ * adjoint call on a plan uploads its inverse tables (allocates, synchronous);
+ * bfs_fdmt_adjoint also allocates the plan's adjoint planes then, so make
+ * that first call outside any stream capture. */
+bfs_status bfs_fdmt_adjoint(bfs_fdmt_plan* plan, const float* d_grad_out, float* d_grad_in,
+                            void* stream);
+bfs_status bfs_fdmt_adjoint_workspace_size(const bfs_fdmt_plan* plan, size_t* bytes);
+bfs_status bfs_fdmt_adjoint_ws(bfs_fdmt_plan* plan, const float* d_grad_out, float* d_grad_in,
+                               void* d_workspace, size_t workspace_bytes, void* stream);
+
 /* ------------------------------------------------------------------------
  * Statistical preprocessing of the FDMT input.
  * Replaces statistical_preprocessing::calc_fdmt_inputs
@@ -196,6 +211,21 @@ bfs_status bfs_boxcar_gather(const float* d_plane, int rows, int cols, const flo
                              float thr, const float* d_thr, int widths_mode, int param,
                              int snr_fast, bfs_cand* d_out, uint32_t capacity,
                              uint32_t* h_count, void* stream);
+
+/* Boxcar S/N at given cells and its gradient (no reference counterpart).
+ * d_cells: n x {row, start, width} (device ints); d_stats: 2*rows floats
+ * {means, stds} as bfs_row_stats writes.  S = sum_{j<width} (y - m)/s over
+ * samples start..start+width-1, / sqrt(width), evaluated as the boxcar
+ * kernels evaluate it (a cell outside the plane gives NaN).  The adjoint
+ * writes the whole d_gplane (rows x cols) with d(sum_k gsnr_k S_k)/dy,
+ * including the dependence of each row's mean and std on the row (at most
+ * 512 cells per row; synchronises `stream`). */
+bfs_status bfs_boxcar_snr_cells(const float* d_plane, int rows, int cols, const float* d_stats,
+                                const int* d_cells, int n, float* d_snr, void* stream);
+bfs_status bfs_boxcar_snr_cells_adjoint(const float* d_plane, int rows, int cols,
+                                        const float* d_stats, const int* d_cells, int n,
+                                        const float* d_snr, const float* d_gsnr, float* d_gplane,
+                                        void* stream);
 
 /* ------------------------------------------------------------------------
  * Clustering + delegates.

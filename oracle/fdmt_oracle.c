@@ -285,3 +285,68 @@ int orc_fdmt_run_lowp(float fmin, float fmax, int nchan, int cols, int max_dt,
     if (prec != ORC_PREC_F16 && prec != ORC_PREC_BF16) return -3;
     return run_f32(fmin, fmax, nchan, cols, max_dt, in, out, b_ones, prec, kstore);
 }
+
+/* ---- adjoint --------------------------------------------------------------
+ * Transpose of the FDMT (the product's adjoint, no reference counterpart):
+ *   merge level l: gin[i][u] = sum, over the level-l rows g that read row i
+ *     (as tail a_g, shift 0, or head b_g, shift s_g) in ascending g, of
+ *     gout[g][u + shift] where u + shift < cols;
+ *   level 0: gx[c][u] = sum_{r} sum_{r' >= r} [u+r >= r'][u+r < cols]
+ *     g0[c,r'][u+r] / (r'+1), r ascending, then r'.
+ * With T = float the sums run in exactly that order. */
+#define DEFINE_ADJ(NAME, T)                                                              \
+int NAME(float fmin, float fmax, int nchan, int cols, int max_dt, const T* gy, T* gx) {  \
+    oplan p;                                                                             \
+    if (plan_build(&p, fmin, fmax, nchan, max_dt) || cols < 1) { plan_free(&p); return -1; } \
+    if (p.cum[p.niter][p.nsub[p.niter]] != max_dt) { plan_free(&p); return -2; }         \
+    int rmax = 0;                                                                        \
+    for (int l = 0; l <= p.niter; ++l) { int r = p.cum[l][p.nsub[l]]; if (r > rmax) rmax = r; } \
+    T* cur = (T*)malloc(sizeof(T) * (size_t)max_dt * cols);                              \
+    memcpy(cur, gy, sizeof(T) * (size_t)max_dt * cols);                                  \
+    int* a = (int*)malloc(sizeof(int) * (rmax + 1));                                     \
+    int* b = (int*)malloc(sizeof(int) * (rmax + 1));                                     \
+    int* s = (int*)malloc(sizeof(int) * (rmax + 1));                                     \
+    int* cnt = (int*)malloc(sizeof(int) * (rmax + 2));                                   \
+    int* eg = (int*)malloc(sizeof(int) * 2 * (rmax + 1));                                \
+    int* es = (int*)malloc(sizeof(int) * 2 * (rmax + 1));                                \
+    for (int l = p.niter; l >= 1; --l) {                                                 \
+        int nout = level_tables(&p, l, a, b, s, rmax + 1);                               \
+        int nin = p.cum[l - 1][p.nsub[l - 1]];                                           \
+        for (int i = 0; i <= nin; ++i) cnt[i] = 0;                                       \
+        for (int g = 0; g < nout; ++g) { ++cnt[a[g] + 1]; if (b[g] >= 0) ++cnt[b[g] + 1]; } \
+        for (int i = 0; i < nin; ++i) cnt[i + 1] += cnt[i];                              \
+        int* fill = (int*)malloc(sizeof(int) * ((size_t)nin + 1));                       \
+        memcpy(fill, cnt, sizeof(int) * (nin + 1));                                      \
+        for (int g = 0; g < nout; ++g) {                                                 \
+            int k = fill[a[g]]++; eg[k] = g; es[k] = 0;                                  \
+            if (b[g] >= 0) { k = fill[b[g]]++; eg[k] = g; es[k] = s[g]; }                \
+        }                                                                                \
+        T* nxt = (T*)calloc((size_t)(unsigned)nin * (size_t)(unsigned)cols, sizeof(T));  \
+        for (int i = 0; i < nin; ++i) {                                                  \
+            T* o = nxt + (size_t)i * cols;                                               \
+            for (int k = cnt[i]; k < cnt[i + 1]; ++k) {                                  \
+                const T* src = cur + (size_t)eg[k] * cols;                               \
+                int sh = es[k];                                                          \
+                for (int u = 0; u + sh < cols; ++u) o[u] = o[u] + src[u + sh];          \
+            }                                                                            \
+        }                                                                                \
+        free(fill); free(cur); cur = nxt;                                                \
+    }                                                                                    \
+    int R = p.rows[0][0];                                                                \
+    for (int c = 0; c < nchan; ++c) {                                                    \
+        const T* g0 = cur + (size_t)c * R * cols;                                        \
+        for (int u = 0; u < cols; ++u) {                                                 \
+            T acc = 0;                                                                   \
+            for (int r = 0; r < R && u + r < cols; ++r)                                  \
+                for (int rr = r; rr < R && u + r >= rr; ++rr)                            \
+                    acc = acc + g0[(size_t)rr * cols + u + r] / (T)(rr + 1);             \
+            gx[(size_t)c * cols + u] = acc;                                              \
+        }                                                                                \
+    }                                                                                    \
+    free(cur); free(a); free(b); free(s); free(cnt); free(eg); free(es);                 \
+    plan_free(&p);                                                                       \
+    return 0;                                                                            \
+}
+
+DEFINE_ADJ(orc_fdmt_adjoint_f32, float)
+DEFINE_ADJ(orc_fdmt_adjoint_f64, double)

@@ -44,6 +44,12 @@ int orc_fdmt_run_lowp(float fmin, float fmax, int nchan, int cols, int max_dt,
                       const float* in, float* out, int b_ones, int prec, int kstore);
 /* out[i] = in[i] rounded to the nearest binary16 / bfloat16 (ties to even). */
 void orc_round16(const float* in, float* out, int64_t n, int prec);
+/* Adjoint (transpose) of the FDMT: gx (nchan x cols) = F^T gy (max_dt x cols);
+ * the FP32 version sums in the product's fixed order. */
+int orc_fdmt_adjoint_f32(float fmin, float fmax, int nchan, int cols, int max_dt,
+                         const float* gy, float* gx);
+int orc_fdmt_adjoint_f64(float fmin, float fmax, int nchan, int cols, int max_dt,
+                         const double* gy, double* gx);
 
 /* --- search (reference: MyVSLib_C++/Clusterization/ sources) --------------- */
 int64_t orc_boxcar(const float* plane, int rows, int cols, float thr, int mode,

@@ -172,6 +172,43 @@ def round16(x: np.ndarray, prec: int) -> np.ndarray:
     return out
 
 
+def fdmt_adjoint_f32(fmin, fmax, gy: np.ndarray, nchan, ncols, max_dt) -> np.ndarray:
+    """F^T gy in FP32, summed in the product's order."""
+    gx = np.zeros((nchan, ncols), np.float32)
+    g = np.ascontiguousarray(gy, np.float32)
+    if lib().orc_fdmt_adjoint_f32(_F(fmin), _F(fmax), nchan, ncols, max_dt, _ptr(g), _ptr(gx)) != 0:
+        raise ValueError("oracle adjoint failed")
+    return gx
+
+
+def fdmt_adjoint_f64(fmin, fmax, gy: np.ndarray, nchan, ncols, max_dt) -> np.ndarray:
+    gx = np.zeros((nchan, ncols), np.float64)
+    g = np.ascontiguousarray(gy, np.float64)
+    if lib().orc_fdmt_adjoint_f64(_F(fmin), _F(fmax), nchan, ncols, max_dt, _ptr(g), _ptr(gx)) != 0:
+        raise ValueError("oracle adjoint failed")
+    return gx
+
+
+def snr_cells_f64(y: np.ndarray, cells: np.ndarray):
+    """S/N at cells {row, start, width} of the plane y with FP64 row mean and
+    population std; returns (snr, dsnr_dy) where dsnr_dy[k] is the gradient
+    of S_k with respect to row cells[k, 0] (a length-ncols vector)."""
+    y = np.asarray(y, np.float64)
+    n = y.shape[1]
+    snr = np.zeros(len(cells))
+    grads = []
+    for k, (d, t, w) in enumerate(np.asarray(cells, np.int64)):
+        row = y[d]
+        m = row.mean()
+        sd = np.sqrt(((row - m) ** 2).mean())
+        z = (row - m) / sd
+        snr[k] = z[t:t + w].sum() / np.sqrt(w)
+        win = np.zeros(n)
+        win[t:t + w] = 1.0
+        grads.append((win - w / n) / (sd * np.sqrt(w)) - snr[k] * (row - m) / (n * sd * sd))
+    return snr, grads
+
+
 def ref_fdmt_cpu(fmin, fmax, x: np.ndarray | None, nchan, ncols, max_dt, b_ones=False,
                  threads=1) -> np.ndarray | None:
     """Runs the reference's CFdmtCpu::process_image (None if not built)."""
