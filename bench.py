@@ -60,6 +60,9 @@ def parse_args(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--form", choices=["both", "batched"], default="both",
+                    help="batched: time only the batched form (profiling runs; no plain-form "
+                         "numbers, no FDMT roofline)")
     return ap.parse_args(argv)
 
 
@@ -292,25 +295,27 @@ def run_ours(args):
         return float(t.item())
 
     # ---- device-resident timing: plain per-beam form -------------------------
-    for _ in range(args.warmup):
-        pipe.run(inputs)
-    torch.cuda.synchronize()
-    barrier()
-    torch.cuda.synchronize()
+    plain = args.form == "both"
     clocks = ClockSampler(local).start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    fdmt_ev = []
-    launches0 = pipe.launches
-    e0.record()
-    plain_results = None
-    for _ in range(args.steps):
-        plain_results = pipe.run(inputs, fdmt_timing=fdmt_ev)
-    e1.record()
-    torch.cuda.synchronize()
-    plain_launches = (pipe.launches - launches0) // args.steps
-    barrier()
-    plain_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
-    fdmt_ms = sum(a.elapsed_time(b) for a, b in fdmt_ev) / args.steps
+    plain_results, plain_launches, plain_ms, fdmt_ms = None, None, None, None
+    if plain:
+        for _ in range(args.warmup):
+            pipe.run(inputs)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fdmt_ev = []
+        launches0 = pipe.launches
+        e0.record()
+        for _ in range(args.steps):
+            plain_results = pipe.run(inputs, fdmt_timing=fdmt_ev)
+        e1.record()
+        torch.cuda.synchronize()
+        plain_launches = (pipe.launches - launches0) // args.steps
+        barrier()
+        plain_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+        fdmt_ms = sum(a.elapsed_time(b) for a, b in fdmt_ev) / args.steps
     units = pipe.chan_samples * world
 
     # ---- device-resident timing: batched form (the headline) -----------------
@@ -332,13 +337,13 @@ def run_ours(args):
     value = units / (step_ms / 1e3)
     ncand = sum(r.n_candidates for r in results)
     launches = batch.launches_per_run(ncand)
-    same = all(a.n_candidates == b.n_candidates and np.array_equal(a.delegates, b.delegates)
-               and np.array_equal(a.group_sizes, b.group_sizes)
-               for a, b in zip(plain_results, results))
+    same = plain and all(a.n_candidates == b.n_candidates and np.array_equal(a.delegates, b.delegates)
+                         and np.array_equal(a.group_sizes, b.group_sizes)
+                         for a, b in zip(plain_results, results))
 
     peak, peak_kind = measured_peaks()
     fdmt_bytes = pipe.fdmt_alg_bytes()
-    achieved = fdmt_bytes / (fdmt_ms / 1e3) / 1e9
+    achieved = fdmt_bytes / (fdmt_ms / 1e3) / 1e9 if plain else None
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
@@ -411,14 +416,15 @@ def run_ours(args):
                        "parallelism": f"{world} independent rank(s), beams sharded, no collective"},
             "roofline": {"bound": "hbm", "kernel": "FDMT (bfs_fdmt_execute: init + level kernels)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "frac": achieved / peak if plain else None, "peak_source": peak_kind,
                          "traffic": traffic, "alg_bytes_per_step": fdmt_bytes,
                          "fdmt_ms_per_step": fdmt_ms,
                          "timed_in": "plain per-beam form (events around each beam's FDMT; "
                                      "same autotuned plans as the batched form)"},
             "plain": {"value": units / (plain_ms / 1e3), "ms_per_step": plain_ms,
                       "gpu_launches": plain_launches,
-                      "batched_speedup": plain_ms / step_ms, "same_results_as_batched": same},
+                      "batched_speedup": plain_ms / step_ms, "same_results_as_batched": same}
+                     if plain else None,
             "pipeline_balg": {"bytes_per_step": pipe_bytes,
                               "gbs": pipe_bytes / (step_ms / 1e3) / 1e9,
                               "frac_of_peak": pipe_bytes / (step_ms / 1e3) / 1e9 / peak},

@@ -1,0 +1,68 @@
+"""Time one FDMT variant on the current GPU (CUDA events, inputs resident).
+
+    python -m cpp_projects_b200.fdmt_timing --nchan 1024 --ncols 65536 \
+        [--max-dt 1024] [--fmin 1200 --fmax 1600] [--fuse -2] [--tile 0] \
+        [--precision f32|f16|bf16] [--adjoint] [--reps 10] [--warmup 3]
+
+Prints one JSON line: the plan's fused depth, milliseconds per call, the
+level-by-level algorithmic bytes of one call and the resulting GB/s.  Used
+for the autotuner's choices, for the reduced-precision and adjoint timings,
+and as the command under ncu for the per-kernel captures.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import torch
+
+from .fdmt import CFdmtGpu
+
+PRECISIONS = {"f32": 0, "f16": 1, "bf16": 2}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--nchan", type=int, default=1024)
+    ap.add_argument("--ncols", type=int, default=65536)
+    ap.add_argument("--max-dt", type=int, default=0, help="default: nchan")
+    ap.add_argument("--fmin", type=float, default=1200.0)
+    ap.add_argument("--fmax", type=float, default=1600.0)
+    ap.add_argument("--fuse", type=int, default=-2, help="-2 autotune, -1 default head, 0 none, k")
+    ap.add_argument("--tile", type=int, default=0)
+    ap.add_argument("--precision", choices=sorted(PRECISIONS), default="f32")
+    ap.add_argument("--adjoint", action="store_true")
+    ap.add_argument("--reps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    a = ap.parse_args(argv)
+    max_dt = a.max_dt or a.nchan
+    dev = torch.device("cuda", 0)
+    f = CFdmtGpu(a.fmin, a.fmax, a.nchan, a.ncols, max_dt, fuse_depth=a.fuse, head_tile=a.tile,
+                 precision=PRECISIONS[a.precision])
+    g = torch.Generator(device=dev).manual_seed(1)
+    if a.adjoint:
+        src = torch.randn((max_dt, a.ncols), device=dev, generator=g)
+        dst = torch.empty((a.nchan, a.ncols), device=dev)
+        run = lambda: f.adjoint(src, dst)  # noqa: E731
+    else:
+        src = torch.randn((a.nchan, a.ncols), device=dev, generator=g)
+        dst = torch.empty((max_dt, a.ncols), device=dev)
+        run = lambda: f.process_image(src, dst)  # noqa: E731
+    for _ in range(a.warmup):
+        run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.reps):
+        run()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.reps
+    print(json.dumps({"nchan": a.nchan, "ncols": a.ncols, "max_dt": max_dt, "precision": a.precision,
+                      "adjoint": a.adjoint, "fuse_depth": f.info.fuse_depth, "ms": ms,
+                      "alg_bytes": f.alg_bytes, "alg_gbs": f.alg_bytes / (ms / 1e3) / 1e9}))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
