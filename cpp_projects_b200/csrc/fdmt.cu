@@ -273,31 +273,52 @@ k_fdmt_level16(const S* __restrict__ in, D* __restrict__ out, const int4* __rest
 // samples u >= halo are written; the plan's look-back guarantees that every
 // value they depend on was computed from in-tile samples (u - shift >= 0), so
 // the halo columns may hold partial values.  Samples t < 0 are the zeros the
-// reference's planes hold there.  The group's row tables are staged in shared
+// reference's planes hold there.  Buffer B first stages the group's input
+// rows (it has at least `group` rows).  The group's row tables are staged in shared
 // memory (after the two planes) and merge rows are processed four at a time
 // with all loads issued before the stores.  R0C = level-0 rows per channel
 // (0: runtime value rows_per_chan).
 // grid: (ceil(ncols / tile), nchan / group)
+// Level 0 of the group.  First every thread fetches its sample of each of
+// the group's channel rows (all loads in flight at once, 8 per batch) into
+// the staging rows of shared buffer B (free until level 1); then the running
+// means read x[t - r] from there.  Local columns u - r < 0 (before the
+// window) read 0: they lie in the halo, whose values never reach a written
+// sample (the plan's look-back counts the level-0 window r).
 template <int R0C>
 __device__ __forceinline__ void head_level0(const float* __restrict__ x, float* __restrict__ bufa,
-                                            int c0, int group, int rows_per_chan, int ncols, int t,
-                                            int u, int W, int ones) {
+                                            float* __restrict__ stage, int c0, int group,
+                                            int rows_per_chan, int ncols, int t, int u, int W,
+                                            int ones) {
+    constexpr int kBatch = 8;
+    for (int cb = 0; cb < group; cb += kBatch) {
+        float xv[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            const int c = cb + k;
+            xv[k] = 0.0f;
+            if (c < group && t >= 0)
+                xv[k] = ones ? 1.0f : (t < ncols ? __ldg(x + static_cast<size_t>(c0 + c) * ncols + t) : 0.0f);
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k)
+            if (cb + k < group) stage[(cb + k) * W + u] = xv[k];
+    }
+    __syncthreads();
     const int r0c = R0C > 0 ? R0C : rows_per_chan;
 #pragma unroll 2
     for (int c = 0; c < group; ++c) {
-        const float* xr = x + static_cast<size_t>(c0 + c) * ncols;
+        const float* sx = stage + c * W + u;
         float* dst = bufa + c * r0c * W + u;
-        float v = 0.0f;
-        if (t >= 0) v = ones ? 1.0f : (t < ncols ? __ldg(xr + t) : 0.0f);
+        float v = sx[0];
         dst[0] = v;
         if constexpr (R0C > 0) {
 #pragma unroll
             for (int r = 1; r < R0C; ++r) {
                 float w = 0.0f;
                 if (t >= r) {
-                    const int tt = t - r;
-                    const float xv = ones ? 1.0f : (tt < ncols ? __ldg(xr + tt) : 0.0f);
-                    v = __fdiv_rn(__fadd_rn(__fmul_rn(v, static_cast<float>(r)), xv),
+                    const float xr = u >= r ? sx[-r] : 0.0f;
+                    v = __fdiv_rn(__fadd_rn(__fmul_rn(v, static_cast<float>(r)), xr),
                                   static_cast<float>(r + 1));
                     w = v;
                 }
@@ -308,9 +329,8 @@ __device__ __forceinline__ void head_level0(const float* __restrict__ x, float* 
             for (int r = 1; r < r0c; ++r) {
                 float w = 0.0f;
                 if (t >= r) {
-                    const int tt = t - r;
-                    const float xv = ones ? 1.0f : (tt < ncols ? __ldg(xr + tt) : 0.0f);
-                    v = __fdiv_rn(__fadd_rn(__fmul_rn(v, static_cast<float>(r)), xv),
+                    const float xr = u >= r ? sx[-r] : 0.0f;
+                    v = __fdiv_rn(__fadd_rn(__fmul_rn(v, static_cast<float>(r)), xr),
                                   static_cast<float>(r + 1));
                     w = v;
                 }
@@ -349,7 +369,7 @@ k_fdmt_head(const float* __restrict__ x, D* __restrict__ out,
     const int ntab = __ldg(&hg->tab_off[depth]) + __ldg(&hg->rows[depth]) - tab0;
     for (int i = u; i < ntab; i += W) stab[i] = __ldg(tab + tab0 + i);
 
-    head_level0<R0C>(x, bufa, blockIdx.y * group, group, rows_per_chan, ncols, t, u, W, ones);
+    head_level0<R0C>(x, bufa, bufb, blockIdx.y * group, group, rows_per_chan, ncols, t, u, W, ones);
     __syncthreads();
 
     float* src = bufa;

@@ -102,7 +102,8 @@ struct HeadPlan {
     int tile = 0;           // output samples per CTA
     int width = 0;          // tile + max halo, rounded to a warp: threads per CTA
     int rows_a = 0;         // shared rows of the even-level buffer (level 0, 2, ...)
-    int rows_b = 0;         // shared rows of the odd-level buffer
+    int rows_b = 0;         // shared rows of the odd-level buffer (>= group: it first
+                            // stages the group's input rows)
     int tab_rows = 0;       // largest per-group table (levels 1..k), staged in shared memory
     size_t smem_bytes = 0;
     std::vector<HeadGroup> groups;

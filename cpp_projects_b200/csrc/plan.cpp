@@ -201,7 +201,7 @@ bool build_head_plan(const FdmtPlanHost& p, int k, int tile, size_t smem_limit, 
             }
         }
         h.rows_a = std::max(h.rows_a, rows_a);
-        h.rows_b = std::max(h.rows_b, rows_b);
+        h.rows_b = std::max(h.rows_b, std::max(rows_b, G));  // B also stages the G input rows
         int trows = 0;
         for (int l = 1; l <= k; ++l) trows += hg.rows[l];
         h.tab_rows = std::max(h.tab_rows, trows);

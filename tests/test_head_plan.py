@@ -47,6 +47,19 @@ def level0_column(x, c, t, r0c, ncols):
     return out
 
 
+def level0_staged(xs, u, t, r0c):
+    """level0_column as the kernel computes it from the staged input window."""
+    out = np.zeros(r0c, np.float32)
+    v = np.float32(xs[u])
+    out[0] = v
+    for r in range(1, r0c):
+        if t >= r:
+            xv = np.float32(xs[u - r]) if u >= r else np.float32(0)
+            v = np.float32(np.float32(np.float32(v * np.float32(r)) + xv) / np.float32(r + 1))
+            out[r] = v
+    return out
+
+
 def emulate_head(x, params, groups, tab, r0c, ncols, rows_k):
     depth, G, tile, W, rows_a, rows_b = (int(v) for v in params[:6])
     out = np.full((rows_k, ncols), np.nan, np.float32)
@@ -61,9 +74,14 @@ def emulate_head(x, params, groups, tab, r0c, ncols, rows_k):
             a = np.zeros((rows_a, W), np.float32)
             b = np.zeros((rows_b, W), np.float32)
             assert G * r0c <= rows_a
+            assert G <= rows_b  # buffer B stages the group's input rows
             for c in range(G):
+                # the kernel reads x[t - r] from the staged window: 0 before it
+                xs = np.zeros(W, np.float32)
+                ok = (t >= 0) & (t < ncols)
+                xs[ok] = x[gi * G + c, t[ok]]
                 for ui in range(W):
-                    a[c * r0c:(c + 1) * r0c, ui] = level0_column(x, gi * G + c, int(t[ui]), r0c, ncols)
+                    a[c * r0c:(c + 1) * r0c, ui] = level0_staged(xs, ui, int(t[ui]), r0c)
             src, dst = a, b
             for lev in range(1, depth + 1):
                 e = tab[int(toff[lev]): int(toff[lev]) + int(rows[lev])]
