@@ -15,8 +15,9 @@
 //                            gather over the plan's inverse row tables, summed
 //                            in ascending g, so the FP32 result is fixed;
 //   level 0         forward  P[c,r][t] = [t >= r] mean(x[c][t-r .. t])
-//                   adjoint  gx[c][u] = sum_{r} sum_{r' >= r} [u+r >= r'][u+r < ncols]
-//                            g0[c,r'][u + r] / (r' + 1), r ascending, then r'.
+//                   adjoint  gx[c][u] = sum_{r'} RN(1/(r'+1)) *
+//                            sum_{r=0..r'} [u+r >= r'][u+r < ncols] g0[c,r'][u+r]
+//                            (inner sums r ascending, outer r' ascending).
 //
 // Boxcar S/N at a cell (row d, start t, width w) of the plane y with row mean
 // m_d and standard deviation s_d (population, as bfs_row_stats gives):
@@ -38,7 +39,6 @@ namespace {
 constexpr int kAdjThreads = 256;
 constexpr int kAdjVecs = 2;       // float4 column groups per thread
 constexpr int kAdjInitThreads = 256;
-constexpr int kAdjInitCols = 4;
 
 // words w[0..7] = the 8 floats of vectors (q+sv, q+sv+1); elements R..R+3
 template <int R>
@@ -117,29 +117,70 @@ k_fdmt_adj_level(const float* __restrict__ gout, float* __restrict__ gin, const 
     }
 }
 
-// Adjoint of level 0 (running means).  grid: (ceil(ncols / (256*4)), nchan)
+// Adjoint of level 0 (running means), one window sum and one product per
+// level-0 row:
+//   gx[c][u] = sum_{r'} RN(1/(r'+1)) * sum_{r=0..r'} [u+r >= r'][u+r < ncols] g0[c,r'][u+r]
+// (inner sums r ascending, outer r' ascending).  Thread q owns samples
+// 4q..4q+3: each row r' is read as the aligned float4 q plus the next one
+// from the lane above (warp shuffle; lane 31 loads its own), which covers
+// u + r <= 4q + 7 for up to 5 rows per channel (R0C <= 5; R0C = 0: any
+// count, scalar reads).  grid: (ceil(ceil(ncols / 4) / 256), nchan)
+template <int R0C>
 __global__ void __launch_bounds__(kAdjInitThreads)
 k_fdmt_adj_init(const float* __restrict__ g0, float* __restrict__ gx, int ncols, int in_pitch,
-                int rows_per_chan) {
+                int rows_per_chan, int vec_out) {
     const int c = blockIdx.y;
     const float* g = g0 + static_cast<size_t>(c) * rows_per_chan * in_pitch;
     float* o = gx + static_cast<size_t>(c) * ncols;
-    const int base = blockIdx.x * (kAdjInitThreads * kAdjInitCols) + threadIdx.x;
-#pragma unroll
-    for (int k = 0; k < kAdjInitCols; ++k) {
-        const int u = base + k * kAdjInitThreads;
-        if (u >= ncols) break;
-        float acc = 0.0f;
-        for (int r = 0; r < rows_per_chan; ++r) {
-            const int t = u + r;
-            if (t >= ncols) break;
-            for (int rr = r; rr < rows_per_chan; ++rr) {
-                if (t < rr) break;  // row rr is zero before sample rr
-                acc = __fadd_rn(acc, __fdiv_rn(__ldg(g + static_cast<size_t>(rr) * in_pitch + t),
-                                               static_cast<float>(rr + 1)));
-            }
+    const int nv = (ncols + 3) >> 2;
+    const int q = blockIdx.x * kAdjInitThreads + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int u = 4 * q;
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    const int R = R0C > 0 ? R0C : rows_per_chan;
+    for (int rr = 0; rr < R; ++rr) {
+        const float* row = g + static_cast<size_t>(rr) * in_pitch;
+        const float rcp = __frcp_rn(static_cast<float>(rr + 1));
+        float e[8];
+        if constexpr (R0C > 0) {
+            const float4 lo = (q < nv) ? __ldg(reinterpret_cast<const float4*>(row) + q)
+                                       : make_float4(0.f, 0.f, 0.f, 0.f);
+            float4 hi;
+            hi.x = __shfl_down_sync(0xffffffffu, lo.x, 1);
+            hi.y = __shfl_down_sync(0xffffffffu, lo.y, 1);
+            hi.z = __shfl_down_sync(0xffffffffu, lo.z, 1);
+            hi.w = __shfl_down_sync(0xffffffffu, lo.w, 1);
+            if (lane == 31)
+                hi = (q + 1 < nv) ? __ldg(reinterpret_cast<const float4*>(row) + q + 1)
+                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+            e[0] = lo.x; e[1] = lo.y; e[2] = lo.z; e[3] = lo.w;
+            e[4] = hi.x; e[5] = hi.y; e[6] = hi.z; e[7] = hi.w;
         }
-        o[u] = acc;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            float w = 0.0f;
+            const int rmax = R0C > 0 ? R0C : rows_per_chan;
+#pragma unroll
+            for (int r = 0; r < rmax; ++r) {
+                if (r > rr) break;
+                const int t = u + j + r;
+                if (t >= rr && t < ncols) {
+                    float v;
+                    if constexpr (R0C > 0) v = e[j + r];
+                    else v = __ldg(row + t);
+                    w = __fadd_rn(w, v);
+                }
+            }
+            acc[j] = __fadd_rn(acc[j], __fmul_rn(w, rcp));
+        }
+    }
+    if (q >= nv) return;
+    if (vec_out && u + 3 < ncols) {
+        reinterpret_cast<float4*>(o)[q] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (u + j < ncols) o[u + j] = acc[j];
     }
 }
 
@@ -285,9 +326,18 @@ bfs_status adjoint_run(bfs_fdmt_plan* p, const float* d_gy, float* d_gx, float* 
             k_fdmt_adj_level<false><<<grid, kAdjThreads, 0, s>>>(src, dst, off, ent, T, in_pitch, P);
         BFS_LAUNCH_CHECK("k_fdmt_adj_level");
     }
-    dim3 grid((T + kAdjInitThreads * kAdjInitCols - 1) / (kAdjInitThreads * kAdjInitCols), h.nchan);
+    dim3 grid(((T + 3) / 4 + kAdjInitThreads - 1) / kAdjInitThreads, h.nchan);
     BFS_ARG(grid.y <= 65535, "nchan too large for this build");
-    k_fdmt_adj_init<<<grid, kAdjInitThreads, 0, s>>>(bufs[0], d_gx, T, P, h.rows_per_chan0);
+    const int vec_out = (T % 4 == 0) && (reinterpret_cast<uintptr_t>(d_gx) & 15) == 0;
+    switch (h.rows_per_chan0) {
+        case 1: k_fdmt_adj_init<1><<<grid, kAdjInitThreads, 0, s>>>(bufs[0], d_gx, T, P, 1, vec_out); break;
+        case 2: k_fdmt_adj_init<2><<<grid, kAdjInitThreads, 0, s>>>(bufs[0], d_gx, T, P, 2, vec_out); break;
+        case 3: k_fdmt_adj_init<3><<<grid, kAdjInitThreads, 0, s>>>(bufs[0], d_gx, T, P, 3, vec_out); break;
+        case 4: k_fdmt_adj_init<4><<<grid, kAdjInitThreads, 0, s>>>(bufs[0], d_gx, T, P, 4, vec_out); break;
+        case 5: k_fdmt_adj_init<5><<<grid, kAdjInitThreads, 0, s>>>(bufs[0], d_gx, T, P, 5, vec_out); break;
+        default:
+            k_fdmt_adj_init<0><<<grid, kAdjInitThreads, 0, s>>>(bufs[0], d_gx, T, P, h.rows_per_chan0, vec_out);
+    }
     BFS_LAUNCH_CHECK("k_fdmt_adj_init");
     return BFS_OK;
 }

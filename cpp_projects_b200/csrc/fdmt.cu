@@ -57,6 +57,8 @@ template <> __device__ __forceinline__ __half from_f32<__half>(float v) { return
 template <> __device__ __forceinline__ __nv_bfloat16 from_f32<__nv_bfloat16>(float v) {
     return __float2bfloat16_rn(v);
 }
+__device__ __forceinline__ unsigned bits16(__half v) { return __half_as_ushort(v); }
+__device__ __forceinline__ unsigned bits16(__nv_bfloat16 v) { return __bfloat16_as_ushort(v); }
 __device__ __forceinline__ float exp2_int(int e) { return __int_as_float((127 + e) << 23); }
 // exponents packed in a table row's w: input a | input b << 8 | output << 16 (signed bytes)
 __device__ __forceinline__ int exp_field(int w, int k) {
@@ -90,6 +92,96 @@ k_fdmt_init(const float* __restrict__ x, D* __restrict__ out, int ncols, int out
             o[static_cast<size_t>(r) * out_pitch + t] = from_f32<D>(w);
         }
     }
+}
+
+// Level 0, 4 samples per thread (R0C = rows per channel, 1..5): thread q
+// owns samples t = 4q .. 4q+3, reads them as one float4 (when the rows are
+// 16-byte aligned) and the 4 before them from the lane below (warp shuffle;
+// lane 0 loads its own), runs the 4 running means side by side and stores
+// each row as one 16-byte (FP32) or 8-byte (16-bit) vector into the
+// workspace plane (128-byte pitch; samples past ncols land in the pitch
+// padding).  grid: (ceil(ceil(ncols / 4) / 256), nchan)
+__device__ __forceinline__ float init_x(const float* __restrict__ xr, int tt, int ncols, int ones) {
+    if (tt < 0 || tt >= ncols) return 0.0f;
+    return ones ? 1.0f : __ldg(xr + tt);
+}
+
+template <typename D>
+__device__ __forceinline__ void store4(D* __restrict__ p, const float (&v)[4]) {
+    if constexpr (sizeof(D) == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+        const unsigned lo = bits16(from_f32<D>(v[0])) | (bits16(from_f32<D>(v[1])) << 16);
+        const unsigned hi = bits16(from_f32<D>(v[2])) | (bits16(from_f32<D>(v[3])) << 16);
+        *reinterpret_cast<uint2*>(p) = make_uint2(lo, hi);
+    }
+}
+
+template <typename D, int R0C>
+__global__ void __launch_bounds__(kInitThreads)
+k_fdmt_init4(const float* __restrict__ x, D* __restrict__ out, int ncols, int out_pitch, int ones,
+             int vec_x) {
+    const int c = blockIdx.y;
+    const float* xr = x + static_cast<size_t>(c) * ncols;
+    D* o = out + static_cast<size_t>(c) * R0C * out_pitch;
+    const int nv = (ncols + 3) >> 2;
+    const int q = blockIdx.x * kInitThreads + threadIdx.x;
+    const int t = 4 * q;
+    const int lane = threadIdx.x & 31;
+    float4 cur;
+    if (vec_x && !ones && t + 3 < ncols)
+        cur = __ldg(reinterpret_cast<const float4*>(xr) + q);
+    else
+        cur = make_float4(init_x(xr, t, ncols, ones), init_x(xr, t + 1, ncols, ones),
+                          init_x(xr, t + 2, ncols, ones), init_x(xr, t + 3, ncols, ones));
+    float4 prev;
+    prev.x = __shfl_up_sync(0xffffffffu, cur.x, 1);
+    prev.y = __shfl_up_sync(0xffffffffu, cur.y, 1);
+    prev.z = __shfl_up_sync(0xffffffffu, cur.z, 1);
+    prev.w = __shfl_up_sync(0xffffffffu, cur.w, 1);
+    if (lane == 0)
+        prev = make_float4(init_x(xr, t - 4, ncols, ones), init_x(xr, t - 3, ncols, ones),
+                           init_x(xr, t - 2, ncols, ones), init_x(xr, t - 1, ncols, ones));
+    if (q >= nv) return;
+    const float xs[8] = {prev.x, prev.y, prev.z, prev.w, cur.x, cur.y, cur.z, cur.w};  // x[t-4 .. t+3]
+    float v[4] = {cur.x, cur.y, cur.z, cur.w};
+    store4<D>(o + t, v);
+#pragma unroll
+    for (int r = 1; r < R0C; ++r) {
+        float w[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            w[j] = 0.0f;
+            if (t + j >= r) {
+                v[j] = __fdiv_rn(__fadd_rn(__fmul_rn(v[j], static_cast<float>(r)), xs[4 + j - r]),
+                                 static_cast<float>(r + 1));
+                w[j] = v[j];
+            }
+        }
+        store4<D>(o + static_cast<size_t>(r) * out_pitch + t, w);
+    }
+}
+
+// Launches level 0 into a workspace plane (pitch P, 128-byte aligned rows).
+template <typename D>
+cudaError_t launch_init(const float* d_in, D* dst, const FdmtPlanHost& h, int P, int ones, cudaStream_t s) {
+    const int T = h.ncols;
+    const int R = h.rows_per_chan0;
+    if (R >= 1 && R <= 5) {
+        dim3 grid(((T + 3) / 4 + kInitThreads - 1) / kInitThreads, h.nchan);
+        const int vec_x = (T % 4 == 0) && d_in && (reinterpret_cast<uintptr_t>(d_in) & 15) == 0;
+        switch (R) {
+            case 1: k_fdmt_init4<D, 1><<<grid, kInitThreads, 0, s>>>(d_in, dst, T, P, ones, vec_x); break;
+            case 2: k_fdmt_init4<D, 2><<<grid, kInitThreads, 0, s>>>(d_in, dst, T, P, ones, vec_x); break;
+            case 3: k_fdmt_init4<D, 3><<<grid, kInitThreads, 0, s>>>(d_in, dst, T, P, ones, vec_x); break;
+            case 4: k_fdmt_init4<D, 4><<<grid, kInitThreads, 0, s>>>(d_in, dst, T, P, ones, vec_x); break;
+            default: k_fdmt_init4<D, 5><<<grid, kInitThreads, 0, s>>>(d_in, dst, T, P, ones, vec_x); break;
+        }
+    } else {
+        dim3 grid((T + kInitThreads * kInitCols - 1) / (kInitThreads * kInitCols), h.nchan);
+        k_fdmt_init<D><<<grid, kInitThreads, 0, s>>>(d_in, dst, T, P, R, ones);
+    }
+    return cudaGetLastError();
 }
 
 // One merge level.  The input plane is always a workspace plane (128-byte
@@ -857,11 +949,9 @@ static bfs_status fdmt_run16(bfs_fdmt_plan* plan, const float* d_in, float* d_ou
                              b_ones ? 1 : 0, s);
         if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_head: %s", cudaGetErrorString(e));
     } else {
-        dim3 grid((T + kInitThreads * kInitCols - 1) / (kInitThreads * kInitCols), h.nchan);
-        BFS_ARG(grid.y <= 65535, "nchan too large for this build");
-        k_fdmt_init<S><<<grid, kInitThreads, 0, s>>>(d_in, bufs[0], T, P, h.rows_per_chan0,
-                                                     b_ones ? 1 : 0);
-        BFS_LAUNCH_CHECK("k_fdmt_init");
+        BFS_ARG(h.nchan <= 65535, "nchan too large for this build");
+        cudaError_t e = launch_init<S>(d_in, bufs[0], h, P, b_ones ? 1 : 0, s);
+        if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_init: %s", cudaGetErrorString(e));
     }
     for (int l = k + 1; l <= h.niter; ++l) {
         const S* src = bufs[(l - 1) & 1];
@@ -898,11 +988,9 @@ static bfs_status fdmt_run(bfs_fdmt_plan* plan, const float* d_in, float* d_out,
                                            plan->d_head_groups, plan->d_head_tab, b_ones ? 1 : 0, s);
         if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_head: %s", cudaGetErrorString(e));
     } else {
-        dim3 grid((T + kInitThreads * kInitCols - 1) / (kInitThreads * kInitCols), h.nchan);
-        BFS_ARG(grid.y <= 65535, "nchan too large for this build");
-        k_fdmt_init<float><<<grid, kInitThreads, 0, s>>>(d_in, bufs[0], T, P, h.rows_per_chan0,
-                                                         b_ones ? 1 : 0);
-        BFS_LAUNCH_CHECK("k_fdmt_init");
+        BFS_ARG(h.nchan <= 65535, "nchan too large for this build");
+        cudaError_t e = launch_init<float>(d_in, bufs[0], h, P, b_ones ? 1 : 0, s);
+        if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_init: %s", cudaGetErrorString(e));
     }
     for (int l = k + 1; l <= h.niter; ++l) {
         const float* src = bufs[(l - 1) & 1];
@@ -1099,11 +1187,9 @@ extern "C" bfs_status bfs_fdmt_execute_noalloc(const bfs_fdmt_plan* plan, const 
                                            head_tab, b_ones ? 1 : 0, s);
         if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_head: %s", cudaGetErrorString(e));
     } else {
-        dim3 grid((T + kInitThreads * kInitCols - 1) / (kInitThreads * kInitCols), h.nchan);
-        BFS_ARG(grid.y <= 65535, "nchan too large for this build");
-        k_fdmt_init<float><<<grid, kInitThreads, 0, s>>>(d_in, bufs[0], T, P, h.rows_per_chan0,
-                                                         b_ones ? 1 : 0);
-        BFS_LAUNCH_CHECK("k_fdmt_init");
+        BFS_ARG(h.nchan <= 65535, "nchan too large for this build");
+        cudaError_t e = launch_init<float>(d_in, bufs[0], h, P, b_ones ? 1 : 0, s);
+        if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_init: %s", cudaGetErrorString(e));
     }
     for (int l = k + 1; l <= h.niter; ++l) {
         const float* src = bufs[(l - 1) & 1];

@@ -291,8 +291,8 @@ int orc_fdmt_run_lowp(float fmin, float fmax, int nchan, int cols, int max_dt,
  *   merge level l: gin[i][u] = sum, over the level-l rows g that read row i
  *     (as tail a_g, shift 0, or head b_g, shift s_g) in ascending g, of
  *     gout[g][u + shift] where u + shift < cols;
- *   level 0: gx[c][u] = sum_{r} sum_{r' >= r} [u+r >= r'][u+r < cols]
- *     g0[c,r'][u+r] / (r'+1), r ascending, then r'.
+ *   level 0: gx[c][u] = sum_{r'} RN(1/(r'+1)) * sum_{r=0..r'} [u+r >= r'][u+r < cols]
+ *     g0[c,r'][u+r] (inner sums r ascending, outer r' ascending).
  * With T = float the sums run in exactly that order. */
 #define DEFINE_ADJ(NAME, T)                                                              \
 int NAME(float fmin, float fmax, int nchan, int cols, int max_dt, const T* gy, T* gx) {  \
@@ -337,9 +337,14 @@ int NAME(float fmin, float fmax, int nchan, int cols, int max_dt, const T* gy, T
         const T* g0 = cur + (size_t)c * R * cols;                                        \
         for (int u = 0; u < cols; ++u) {                                                 \
             T acc = 0;                                                                   \
-            for (int r = 0; r < R && u + r < cols; ++r)                                  \
-                for (int rr = r; rr < R && u + r >= rr; ++rr)                            \
-                    acc = acc + g0[(size_t)rr * cols + u + r] / (T)(rr + 1);             \
+            for (int rr = 0; rr < R; ++rr) {                                             \
+                T w = 0;                                                                 \
+                for (int r = 0; r <= rr; ++r) {                                          \
+                    int t = u + r;                                                       \
+                    if (t >= rr && t < cols) w = w + g0[(size_t)rr * cols + t];          \
+                }                                                                        \
+                acc = acc + w * ((T)1 / (T)(rr + 1));                                    \
+            }                                                                            \
             gx[(size_t)c * cols + u] = acc;                                              \
         }                                                                                \
     }                                                                                    \
