@@ -360,9 +360,8 @@ def run_ours(args):
             h.copy_(x)
         torch.cuda.synchronize()
         h2d = sum(h.numel() * h.element_size() for h in host)
-        for h, x in zip(host, inputs):
-            x.copy_(h, non_blocking=True)
-        batch.run(inputs)
+        for _ in range(2):  # eager run, then the capture of copies + compute
+            batch.run_host(host, inputs)
         torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
@@ -371,9 +370,9 @@ def run_ours(args):
         f0.record()
         d2h = 0
         for _ in range(args.steps):
-            for h, x in zip(host, inputs):
-                x.copy_(h, non_blocking=True)
-            rs = batch.run(inputs)
+            # every beam's input copied from pinned host memory, overlapped
+            # with the search of the beams before it
+            rs = batch.run_host(host, inputs)
             # the candidate counter, then per beam the delegates and group sizes
             d2h += 4 + sum(r.delegates.nbytes + 4 * len(r.group_sizes) for r in rs)
         f1.record()

@@ -59,6 +59,11 @@ struct bfs_batch {
     cudaGraphExec_t exec = nullptr;
     std::vector<const float*> graph_inputs;
     int runs = 0;
+    // host-input form: copies + compute captured together (bfs_batch_run_host)
+    cudaGraph_t hgraph = nullptr;
+    cudaGraphExec_t hexec = nullptr;
+    std::vector<const void*> hgraph_ptrs;   // host then device pointers it was captured for
+    std::vector<cudaEvent_t> events;
     // results of the last run
     unsigned n_cands = 0, n_groups = 0;
     std::vector<bfs_cand> h_delegates;
@@ -66,6 +71,9 @@ struct bfs_batch {
     ~bfs_batch() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
+        if (hexec) cudaGraphExecDestroy(hexec);
+        if (hgraph) cudaGraphDestroy(hgraph);
+        for (cudaEvent_t e : events) cudaEventDestroy(e);
         for (auto* p : plans) bfs_fdmt_plan_destroy(p);
         for (void* p : {ws, static_cast<void*>(plane), static_cast<void*>(stats), static_cast<void*>(cands),
                         static_cast<void*>(tags), static_cast<void*>(sorted), static_cast<void*>(sorted_tags),
@@ -206,6 +214,8 @@ static bfs_status enqueue_stage1(bfs_batch* b, const float* const* d_inputs, cud
     return BFS_OK;
 }
 
+static bfs_status batch_stage2(bfs_batch* b, void* stream);
+
 extern "C" bfs_status bfs_batch_run(bfs_batch* b, const float* const* d_inputs, void* stream) {
     BFS_ARG(b && d_inputs, "null argument");
     cudaStream_t s = as_stream(stream);
@@ -238,8 +248,98 @@ extern "C" bfs_status bfs_batch_run(bfs_batch* b, const float* const* d_inputs, 
         if (st != BFS_OK) return st;
     }
     ++b->runs;
+    return batch_stage2(b, stream);
+}
 
-    // ---- stage 2: all candidates at once ----------------------------------
+// Host-input form: beam i's input is copied from pinned host memory
+// h_inputs[i] into d_inputs[i] on a copy stream while the compute stream
+// runs beam i-1 (event dependencies), so the copies overlap the FDMT and
+// search of the beams before them.  Copies and compute are captured together
+// in one CUDA graph (after one eager run), replayed while the pointers stay
+// the same.
+static bfs_status enqueue_host_stage1(bfs_batch* b, const float* const* h_inputs,
+                                      float* const* d_inputs, cudaStream_t cs, cudaStream_t cp) {
+    const int nb = static_cast<int>(b->beams.size());
+    BFS_CUDA(cudaMemsetAsync(b->d_count, 0, sizeof(unsigned), cs));
+    BFS_CUDA(cudaEventRecord(b->events[nb], cs));
+    BFS_CUDA(cudaStreamWaitEvent(cp, b->events[nb], 0));
+    for (int i = 0; i < nb; ++i) {
+        const bfs_fdmt_desc& d = b->beams[i];
+        const size_t bytes = static_cast<size_t>(d.nchan) * d.ncols * sizeof(float);
+        BFS_CUDA(cudaMemcpyAsync(d_inputs[i], h_inputs[i], bytes, cudaMemcpyHostToDevice, cp));
+        BFS_CUDA(cudaEventRecord(b->events[i], cp));
+        BFS_CUDA(cudaStreamWaitEvent(cs, b->events[i], 0));
+        bfs_status st = bfs_fdmt_execute_ws(b->plans[i], d_inputs[i], b->plane, 0, b->ws, b->ws_bytes, cs);
+        if (st != BFS_OK) return st;
+        st = launch_row_stats(b->plane, d.max_dt, d.ncols, b->stats, 0, cs);
+        if (st != BFS_OK) return st;
+        st = launch_boxcar(b->plane, d.max_dt, d.ncols, b->stats, b->thr, nullptr, b->widths_mode,
+                           b->param, 0, b->cands, b->capacity, b->d_count, cs, i, b->tags);
+        if (st != BFS_OK) return st;
+    }
+    // the copy stream joins the compute stream (required to end a capture)
+    BFS_CUDA(cudaEventRecord(b->events[nb + 1], cp));
+    BFS_CUDA(cudaStreamWaitEvent(cs, b->events[nb + 1], 0));
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_batch_run_host(bfs_batch* b, const float* const* h_inputs,
+                                         float* const* d_inputs, void* stream) {
+    BFS_ARG(b && h_inputs && d_inputs, "null argument");
+    cudaStream_t s = as_stream(stream);
+    const int nb = static_cast<int>(b->beams.size());
+    for (int i = 0; i < nb; ++i) BFS_ARG(h_inputs[i] && d_inputs[i], "beam %d: null input pointer", i);
+    if (b->events.empty()) {
+        b->events.resize(nb + 2, nullptr);
+        for (auto& e : b->events) BFS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    std::vector<const void*> ptrs;
+    for (int i = 0; i < nb; ++i) ptrs.push_back(h_inputs[i]);
+    for (int i = 0; i < nb; ++i) ptrs.push_back(d_inputs[i]);
+    const bool same = b->hexec && ptrs == b->hgraph_ptrs;
+    cudaStream_t cp;
+    BFS_CUDA(cudaStreamCreateWithFlags(&cp, cudaStreamNonBlocking));
+    bfs_status st = BFS_OK;
+    if (same) {
+        cudaError_t e = cudaGraphLaunch(b->hexec, s);
+        if (e != cudaSuccess) st = fail(BFS_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e));
+    } else if (!b->use_graph || b->runs == 0) {
+        st = enqueue_host_stage1(b, h_inputs, d_inputs, s, cp);  // eager (kernel set-up)
+    } else {
+        if (b->hexec) { cudaGraphExecDestroy(b->hexec); b->hexec = nullptr; }
+        if (b->hgraph) { cudaGraphDestroy(b->hgraph); b->hgraph = nullptr; }
+        cudaStream_t cs;
+        BFS_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        st = e == cudaSuccess ? enqueue_host_stage1(b, h_inputs, d_inputs, cs, cp)
+                              : fail(BFS_ERR_CUDA, "begin capture: %s", cudaGetErrorString(e));
+        cudaGraph_t g = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+        cudaStreamDestroy(cs);
+        if (st == BFS_OK && e2 != cudaSuccess) st = fail(BFS_ERR_CUDA, "end capture: %s", cudaGetErrorString(e2));
+        if (st == BFS_OK) {
+            b->hgraph = g;
+            g = nullptr;
+            e = cudaGraphInstantiate(&b->hexec, b->hgraph, 0);
+            if (e != cudaSuccess) st = fail(BFS_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        }
+        if (g) cudaGraphDestroy(g);
+        if (st == BFS_OK) {
+            b->hgraph_ptrs = ptrs;
+            e = cudaGraphLaunch(b->hexec, s);
+            if (e != cudaSuccess) st = fail(BFS_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e));
+        }
+    }
+    cudaStreamDestroy(cp);
+    if (st != BFS_OK) return st;
+    ++b->runs;
+    return batch_stage2(b, stream);
+}
+
+// ---- stage 2: all candidates at once --------------------------------------
+static bfs_status batch_stage2(bfs_batch* b, void* stream) {
+    cudaStream_t s = as_stream(stream);
+    const int nb = static_cast<int>(b->beams.size());
     unsigned count = 0;
     BFS_CUDA(cudaMemcpyAsync(&count, b->d_count, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     BFS_CUDA(cudaStreamSynchronize(s));

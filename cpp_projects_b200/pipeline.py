@@ -166,11 +166,33 @@ class BatchedSearch:
         return k + ((2 + 12 + 4) if n_candidates else 0)
 
     def run(self, inputs: list[torch.Tensor], stream=None) -> list[BeamResult]:
-        import ctypes
         from ._tensors import dev_ptr, stream_handle
         for i, x in enumerate(inputs):
             self._ptrs[i] = dev_ptr(x, torch.float32, "input")
         self._capi.call("bfs_batch_run", self._h, self._ptrs, stream_handle(stream))
+        return self._results()
+
+    def run_host(self, host_inputs: list[torch.Tensor], dev_inputs: list[torch.Tensor],
+                 stream=None) -> list[BeamResult]:
+        """Search beams whose inputs are in pinned host memory: each beam is
+        copied into its device buffer while the beams before it are searched."""
+        import ctypes
+        from ._tensors import dev_ptr, stream_handle
+        n = len(self.shapes)
+        hp = (ctypes.c_void_p * n)()
+        dp = (ctypes.c_void_p * n)()
+        for i, (h, d) in enumerate(zip(host_inputs, dev_inputs)):
+            if h.device.type != "cpu" or not h.is_pinned() or not h.is_contiguous() or h.dtype != torch.float32:
+                raise ValueError(f"beam {i}: host input must be a contiguous pinned float32 CPU tensor")
+            if h.numel() != self.shapes[i].nchan * self.shapes[i].nsamp or d.numel() != h.numel():
+                raise ValueError(f"beam {i}: input has the wrong size")
+            hp[i] = h.data_ptr()
+            dp[i] = dev_ptr(d, torch.float32, "device input")
+        self._capi.call("bfs_batch_run_host", self._h, hp, dp, stream_handle(stream))
+        return self._results()
+
+    def _results(self) -> list[BeamResult]:
+        import ctypes
         out = []
         for b in range(len(self.shapes)):
             nd, nc = ctypes.c_int(0), ctypes.c_uint32(0)

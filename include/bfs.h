@@ -284,6 +284,13 @@ bfs_status bfs_batch_destroy(bfs_batch* batch);
  * first run is eager; later runs replay the captured graph while the input
  * pointers are unchanged (a new set is captured again).  Synchronises. */
 bfs_status bfs_batch_run(bfs_batch* batch, const float* const* d_inputs, void* stream);
+/* The same with host inputs: h_inputs[i] (pinned host memory, nchan x ncols)
+ * is copied into d_inputs[i] (device) on an internal copy stream while the
+ * beams before it are searched, so the copies overlap the compute; copies
+ * and compute are captured in one CUDA graph after the first run.
+ * Synchronises `stream`. */
+bfs_status bfs_batch_run_host(bfs_batch* batch, const float* const* h_inputs,
+                              float* const* d_inputs, void* stream);
 bfs_status bfs_batch_counts(const bfs_batch* batch, uint32_t* n_cands, uint32_t* n_groups);
 /* Host copies of one beam's delegates (cap entries) and group sizes. */
 bfs_status bfs_batch_beam_results(const bfs_batch* batch, int beam, bfs_cand* delegates,

@@ -37,3 +37,21 @@ def test_batched_equals_plain_per_beam(cuda, use_graph):
             assert np.array_equal(g.delegates.view(np.uint32).reshape(-1), w.delegates.view(np.uint32).reshape(-1))
             assert np.array_equal(g.group_sizes, w.group_sizes)
     assert sum(r.n_candidates for r in want) > 0
+
+
+def test_host_input_form_equals_device_form(cuda):
+    beams = _beams()
+    shapes = [BeamShape(b.nchan, b.nsamp, b.fmin, b.fmax, b.max_dt) for b in beams]
+    inputs = [device_filterbank(b.nchan, b.nsamp, b.fmin, b.fmax, b.seed, b.pulses, cuda) for b in beams]
+    host = [x.cpu().pin_memory() for x in inputs]
+    batch = BatchedSearch(shapes, thr=6.0, capacity=1 << 22)
+    want = batch.run(inputs)
+    dev = [torch.full_like(x, float("nan")) for x in inputs]
+    for rep in range(3):  # eager run, then capture, then replay
+        got = batch.run_host(host, dev)
+        for w, g in zip(want, got):
+            assert g.n_candidates == w.n_candidates
+            assert np.array_equal(g.delegates.view(np.uint32).reshape(-1), w.delegates.view(np.uint32).reshape(-1))
+            assert np.array_equal(g.group_sizes, w.group_sizes)
+    assert all(torch.equal(d, x) for d, x in zip(dev, inputs))
+
