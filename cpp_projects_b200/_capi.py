@@ -20,6 +20,7 @@ BFS_WIDTHS_POW2, BFS_WIDTHS_ALL = 0, 1
 BFS_FDMT_EXTERNAL_WS = 1
 BFS_FUSE_AUTOTUNE = -2
 BFS_PREC_F32, BFS_PREC_F16, BFS_PREC_BF16 = 0, 1, 2
+BFS_PLAN_KEITH, BFS_PLAN_PRAVIR = 0, 1
 
 
 class BfsError(RuntimeError):
@@ -32,13 +33,15 @@ class FdmtDesc(ctypes.Structure):
     _fields_ = [("fmin", ctypes.c_float), ("fmax", ctypes.c_float), ("nchan", ctypes.c_int),
                 ("ncols", ctypes.c_int), ("max_dt", ctypes.c_int), ("plan_kind", ctypes.c_int),
                 ("precision", ctypes.c_int), ("fuse_depth", ctypes.c_int),
-                ("flags", ctypes.c_int), ("head_tile", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+                ("flags", ctypes.c_int), ("head_tile", ctypes.c_int), ("dt_min", ctypes.c_int),
+                ("dt_step", ctypes.c_int), ("tsamp", ctypes.c_float), ("reserved", ctypes.c_int * 3)]
 
 
 class FdmtInfo(ctypes.Structure):
     _fields_ = [("niter", ctypes.c_int), ("rows_level0", ctypes.c_int),
                 ("fuse_depth", ctypes.c_int), ("rows_total", ctypes.c_int64),
-                ("workspace_bytes", ctypes.c_size_t), ("alg_bytes", ctypes.c_double)]
+                ("workspace_bytes", ctypes.c_size_t), ("alg_bytes", ctypes.c_double),
+                ("out_rows", ctypes.c_int)]
 
 
 class ChunkDesc(ctypes.Structure):
@@ -95,6 +98,7 @@ _SIGNATURES = {
     "bfs_cluster": (_I, [_P, _U32, _P, _P, _P, _P, ctypes.POINTER(_U32), _P]),
     "bfs_select_delegates": (_I, [_P, _P, _U32, _P, _U32, _P, _P]),
     "bfs_cluster_grouped": (_I, [_P, _U32, _P, _U32, _P, _P, _P, _P, ctypes.POINTER(_U32), _P]),
+    "bfs_fdmt_plan_delays": (_I, [_P, _P, _I, _P, _P, _I]),
     "bfs_fdmt_adjoint": (_I, [_P, _P, _P, _P]),
     "bfs_fdmt_adjoint_workspace_size": (_I, [_P, ctypes.POINTER(ctypes.c_size_t)]),
     "bfs_fdmt_adjoint_ws": (_I, [_P, _P, _P, _P, ctypes.c_size_t, _P]),

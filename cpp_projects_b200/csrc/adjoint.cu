@@ -184,6 +184,32 @@ k_fdmt_adj_init(const float* __restrict__ g0, float* __restrict__ gx, int ncols,
     }
 }
 
+// Adjoint of a Pravir plan's level 0 (rows with delays dt_k per channel,
+// lvl0 = row cumsum then delays): the same window-mean transpose,
+//   gx[c][u] = sum_k RN(1/(dt_k+1)) * sum_{j=0..dt_k} [u+j >= dt_k][u+j < ncols] g0[k][u+j].
+// grid: (ceil(ncols / 256), nchan)
+__global__ void __launch_bounds__(kAdjInitThreads)
+k_fdmt_adj_init_grid(const float* __restrict__ g0, float* __restrict__ gx, const int* __restrict__ lvl0,
+                     int nchan, int ncols, int in_pitch) {
+    const int c = blockIdx.y;
+    const int u = blockIdx.x * kAdjInitThreads + threadIdx.x;
+    if (u >= ncols) return;
+    const int r0 = __ldg(lvl0 + c), nr = __ldg(lvl0 + c + 1) - r0;
+    const int* dts = lvl0 + nchan + 1 + r0;
+    float acc = 0.0f;
+    for (int k = 0; k < nr; ++k) {
+        const int d = __ldg(dts + k);
+        const float* row = g0 + static_cast<size_t>(r0 + k) * in_pitch;
+        float w = 0.0f;
+        for (int j = 0; j <= d; ++j) {
+            const int t = u + j;
+            if (t >= d && t < ncols) w = __fadd_rn(w, __ldg(row + t));
+        }
+        acc = __fadd_rn(acc, __fmul_rn(w, __frcp_rn(static_cast<float>(d + 1))));
+    }
+    gx[static_cast<size_t>(c) * ncols + u] = acc;
+}
+
 // S/N at cells: cells[3k..3k+2] = {row, start, width}.  A cell outside the
 // plane gives NaN.
 __global__ void k_snr_cells(const float* __restrict__ plane, int rows, int cols,
@@ -325,6 +351,13 @@ bfs_status adjoint_run(bfs_fdmt_plan* p, const float* d_gy, float* d_gx, float* 
         else
             k_fdmt_adj_level<false><<<grid, kAdjThreads, 0, s>>>(src, dst, off, ent, T, in_pitch, P);
         BFS_LAUNCH_CHECK("k_fdmt_adj_level");
+    }
+    if (h.kind == BFS_PLAN_PRAVIR) {
+        dim3 g2((T + kAdjInitThreads - 1) / kAdjInitThreads, h.nchan);
+        BFS_ARG(g2.y <= 65535, "nchan too large for this build");
+        k_fdmt_adj_init_grid<<<g2, kAdjInitThreads, 0, s>>>(bufs[0], d_gx, p->d_lvl0, h.nchan, T, P);
+        BFS_LAUNCH_CHECK("k_fdmt_adj_init_grid");
+        return BFS_OK;
     }
     dim3 grid(((T + 3) / 4 + kAdjInitThreads - 1) / kAdjInitThreads, h.nchan);
     BFS_ARG(grid.y <= 65535, "nchan too large for this build");

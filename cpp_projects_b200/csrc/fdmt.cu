@@ -162,12 +162,61 @@ k_fdmt_init4(const float* __restrict__ x, D* __restrict__ out, int ncols, int ou
     }
 }
 
+// Level 0 of a Pravir plan (L/FDMT_PRAVIR/fdmt_cpu.cpp:103-179): channel c
+// has rows with delays dt_0 < dt_1 < ... (lvl0 = row cumsum over channels,
+// then the delay of every row).  Row 0 at t >= dt_0 is the mean of
+// x[t-dt_0 .. t]; row k at t >= dt_k is (row_{k-1} * (dt_{k-1} + 1) + the sum
+// of x[t-dt_k .. t-dt_{k-1}-1]) / (dt_k + 1); earlier samples are 0.  Sums run
+// in index order, one rounding per operation, as the reference.
+// grid: (ceil(ncols / 256), nchan)
+template <typename D>
+__global__ void __launch_bounds__(kInitThreads)
+k_fdmt_init_grid(const float* __restrict__ x, D* __restrict__ out, const int* __restrict__ lvl0,
+                 int nchan, int ncols, int out_pitch, int ones) {
+    const int c = blockIdx.y;
+    const int t = blockIdx.x * kInitThreads + threadIdx.x;
+    if (t >= ncols) return;
+    const int r0 = __ldg(lvl0 + c), nr = __ldg(lvl0 + c + 1) - r0;
+    const int* dts = lvl0 + nchan + 1 + r0;
+    const float* xr = x + static_cast<size_t>(c) * ncols;
+    D* o = out + static_cast<size_t>(r0) * out_pitch + t;
+    float v = 0.0f;
+    int dp = __ldg(dts);
+    {
+        float w = 0.0f;
+        if (t >= dp) {
+            float sum = 0.0f;
+            for (int i = t - dp; i <= t; ++i) sum = __fadd_rn(sum, ones ? 1.0f : __ldg(xr + i));
+            v = __fdiv_rn(sum, static_cast<float>(dp + 1));
+            w = v;
+        }
+        o[0] = from_f32<D>(w);
+    }
+    for (int k = 1; k < nr; ++k) {
+        const int dc = __ldg(dts + k);
+        float w = 0.0f;
+        if (t >= dc) {
+            float sum = 0.0f;
+            for (int i = t - dc; i < t - dp; ++i) sum = __fadd_rn(sum, ones ? 1.0f : __ldg(xr + i));
+            v = __fdiv_rn(__fadd_rn(__fmul_rn(v, __fadd_rn(static_cast<float>(dp), 1.0f)), sum),
+                          __fadd_rn(static_cast<float>(dc), 1.0f));
+            w = v;
+        }
+        o[static_cast<size_t>(k) * out_pitch] = from_f32<D>(w);
+        dp = dc;
+    }
+}
+
 // Launches level 0 into a workspace plane (pitch P, 128-byte aligned rows).
 template <typename D>
-cudaError_t launch_init(const float* d_in, D* dst, const FdmtPlanHost& h, int P, int ones, cudaStream_t s) {
+cudaError_t launch_init(const float* d_in, D* dst, const FdmtPlanHost& h, int P, int ones, cudaStream_t s,
+                        const int* d_lvl0 = nullptr) {
     const int T = h.ncols;
     const int R = h.rows_per_chan0;
-    if (R >= 1 && R <= 5) {
+    if (h.kind == BFS_PLAN_PRAVIR) {
+        dim3 grid((T + kInitThreads - 1) / kInitThreads, h.nchan);
+        k_fdmt_init_grid<D><<<grid, kInitThreads, 0, s>>>(d_in, dst, d_lvl0, h.nchan, T, P, ones);
+    } else if (R >= 1 && R <= 5) {
         dim3 grid(((T + 3) / 4 + kInitThreads - 1) / kInitThreads, h.nchan);
         const int vec_x = (T % 4 == 0) && d_in && (reinterpret_cast<uintptr_t>(d_in) & 15) == 0;
         switch (R) {
@@ -627,16 +676,29 @@ static std::vector<std::vector<int>> row_exponents(const FdmtPlanHost& h) {
 
 static bfs_status plan_host_part(const bfs_fdmt_desc* desc, std::unique_ptr<bfs_fdmt_plan>& p) {
     BFS_ARG(desc != nullptr, "null argument");
-    BFS_ARG(desc->plan_kind == BFS_PLAN_KEITH, "unsupported plan_kind %d", desc->plan_kind);
+    BFS_ARG(desc->plan_kind == BFS_PLAN_KEITH || desc->plan_kind == BFS_PLAN_PRAVIR,
+            "unsupported plan_kind %d", desc->plan_kind);
     BFS_ARG(desc->precision == BFS_PREC_F32 || desc->precision == BFS_PREC_F16 ||
                 desc->precision == BFS_PREC_BF16,
             "unsupported precision %d", desc->precision);
     p.reset(new bfs_fdmt_plan);
     p->host_only = true;
     p->precision = desc->precision;
+    if (desc->plan_kind == BFS_PLAN_PRAVIR) {
+        BFS_ARG(desc->precision == BFS_PREC_F32, "16-bit planes are implemented for BFS_PLAN_KEITH only");
+        BFS_ARG(desc->fuse_depth <= 0, "BFS_PLAN_PRAVIR has no fused head (fuse_depth %d)", desc->fuse_depth);
+        bfs_status st = build_pravir_plan(desc->fmin, desc->fmax, desc->nchan, desc->ncols, desc->max_dt,
+                                          desc->dt_step > 0 ? desc->dt_step : 1, desc->dt_min, &p->host);
+        if (st != BFS_OK) return st;
+        p->fuse_depth = 0;
+        return BFS_OK;
+    }
     bfs_status st = build_fdmt_plan(desc->fmin, desc->fmax, desc->nchan, desc->ncols,
                                     desc->max_dt, &p->host);
     if (st != BFS_OK) return st;
+    FdmtPlanHost& hm = p->host;
+    hm.dt_out.resize(hm.max_dt);
+    for (int r = 0; r < hm.max_dt; ++r) hm.dt_out[r] = r;
     const FdmtPlanHost& h = p->host;
     // fused head: explicit depth, or the deepest one that keeps two CTAs per SM
     const int tile = desc->head_tile > 0 ? desc->head_tile : kHeadTile;
@@ -665,11 +727,12 @@ static inline int bfs_fdmt_plan_depth_of(int d) { return d; }
 // ---------------------------------------------------------------------------
 namespace {
 struct TuneKey {
-    int nchan, max_dt, cols_bucket, precision;
+    int nchan, max_dt, cols_bucket, precision, kind, dt_min, dt_step;
     uint32_t fmin_bits, fmax_bits;
     bool operator<(const TuneKey& o) const {
-        return std::tie(nchan, max_dt, cols_bucket, precision, fmin_bits, fmax_bits) <
-               std::tie(o.nchan, o.max_dt, o.cols_bucket, o.precision, o.fmin_bits, o.fmax_bits);
+        return std::tie(nchan, max_dt, cols_bucket, precision, kind, dt_min, dt_step, fmin_bits, fmax_bits) <
+               std::tie(o.nchan, o.max_dt, o.cols_bucket, o.precision, o.kind, o.dt_min, o.dt_step,
+                        o.fmin_bits, o.fmax_bits);
     }
 };
 struct TuneVal { int depth, tile; float ms; };
@@ -679,6 +742,7 @@ std::map<TuneKey, TuneVal> g_tune;
 TuneKey tune_key(const bfs_fdmt_desc& d) {
     TuneKey k{};
     k.nchan = d.nchan; k.max_dt = d.max_dt; k.precision = d.precision;
+    k.kind = d.plan_kind; k.dt_min = d.dt_min; k.dt_step = d.dt_step;
     int b = 0;
     while ((1 << b) < d.ncols && b < 30) ++b;
     k.cols_bucket = b;
@@ -805,6 +869,12 @@ extern "C" bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc_in, bfs_fdm
                             cudaMemcpyHostToDevice));
     }
 
+    if (h.kind == BFS_PLAN_PRAVIR) {
+        std::vector<int> l0(h.lv[0].cum.begin(), h.lv[0].cum.end());
+        l0.insert(l0.end(), h.dt0.begin(), h.dt0.end());
+        BFS_CUDA(cudaMalloc(&p->d_lvl0, l0.size() * sizeof(int)));
+        BFS_CUDA(cudaMemcpy(p->d_lvl0, l0.data(), l0.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
     // device row tables; with 16-bit planes w packs the per-row scale exponents
     const std::vector<std::vector<int>> ex = row_exponents(h);
     std::vector<int4> tab;
@@ -896,6 +966,28 @@ extern "C" bfs_status bfs_fdmt_plan_info(const bfs_fdmt_plan* plan, bfs_fdmt_inf
     info->rows_total = tot;
     info->workspace_bytes = plan->ws_bytes;
     info->alg_bytes = fdmt_alg_bytes(h, plan->precision);
+    info->out_rows = h.out_rows();
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_fdmt_plan_delays(const bfs_fdmt_plan* plan, int* out_dt, int out_cap,
+                                           int* lvl0_cum, int* lvl0_dt, int lvl0_cap) {
+    BFS_ARG(plan != nullptr, "null argument");
+    const FdmtPlanHost& h = plan->host;
+    if (out_dt) {
+        BFS_ARG(out_cap >= h.out_rows(), "out_dt needs %d entries", h.out_rows());
+        std::memcpy(out_dt, h.dt_out.data(), sizeof(int) * h.dt_out.size());
+    }
+    const int r0 = h.lv[0].total_rows();
+    if (lvl0_cum) {
+        BFS_ARG(lvl0_cap >= h.nchan + 1, "lvl0_cum needs %d entries", h.nchan + 1);
+        std::memcpy(lvl0_cum, h.lv[0].cum.data(), sizeof(int) * (h.nchan + 1));
+    }
+    if (lvl0_dt) {
+        BFS_ARG(lvl0_cap >= r0, "lvl0_dt needs %d entries", r0);
+        for (int r = 0; r < r0; ++r)
+            lvl0_dt[r] = h.kind == BFS_PLAN_PRAVIR ? h.dt0[r] : r % h.rows_per_chan0;
+    }
     return BFS_OK;
 }
 
@@ -950,7 +1042,7 @@ static bfs_status fdmt_run16(bfs_fdmt_plan* plan, const float* d_in, float* d_ou
         if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_head: %s", cudaGetErrorString(e));
     } else {
         BFS_ARG(h.nchan <= 65535, "nchan too large for this build");
-        cudaError_t e = launch_init<S>(d_in, bufs[0], h, P, b_ones ? 1 : 0, s);
+        cudaError_t e = launch_init<S>(d_in, bufs[0], h, P, b_ones ? 1 : 0, s, plan->d_lvl0);
         if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_init: %s", cudaGetErrorString(e));
     }
     for (int l = k + 1; l <= h.niter; ++l) {
@@ -989,7 +1081,7 @@ static bfs_status fdmt_run(bfs_fdmt_plan* plan, const float* d_in, float* d_out,
         if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_head: %s", cudaGetErrorString(e));
     } else {
         BFS_ARG(h.nchan <= 65535, "nchan too large for this build");
-        cudaError_t e = launch_init<float>(d_in, bufs[0], h, P, b_ones ? 1 : 0, s);
+        cudaError_t e = launch_init<float>(d_in, bufs[0], h, P, b_ones ? 1 : 0, s, plan->d_lvl0);
         if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_init: %s", cudaGetErrorString(e));
     }
     for (int l = k + 1; l <= h.niter; ++l) {
@@ -1115,6 +1207,7 @@ extern "C" bfs_status bfs_fdmt_execute_noalloc(const bfs_fdmt_plan* plan, const 
                                                float* d_out, int b_ones, void* stream) {
     BFS_ARG(plan != nullptr && d_out != nullptr, "null argument");
     BFS_ARG(plan->precision == BFS_PREC_F32, "the allocation-free entry point runs FP32 plans only");
+    BFS_ARG(plan->host.kind == BFS_PLAN_KEITH, "the allocation-free entry point runs BFS_PLAN_KEITH plans only");
     BFS_ARG(b_ones || d_in != nullptr, "d_in is null");
     size_t need = 0;
     bfs_status st = bfs_fdmt_noalloc_scratch_bytes(plan, &need, nullptr);
@@ -1188,7 +1281,7 @@ extern "C" bfs_status bfs_fdmt_execute_noalloc(const bfs_fdmt_plan* plan, const 
         if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_head: %s", cudaGetErrorString(e));
     } else {
         BFS_ARG(h.nchan <= 65535, "nchan too large for this build");
-        cudaError_t e = launch_init<float>(d_in, bufs[0], h, P, b_ones ? 1 : 0, s);
+        cudaError_t e = launch_init<float>(d_in, bufs[0], h, P, b_ones ? 1 : 0, s, plan->d_lvl0);
         if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_init: %s", cudaGetErrorString(e));
     }
     for (int l = k + 1; l <= h.niter; ++l) {

@@ -22,6 +22,7 @@ struct bfs_fdmt_plan {
     bfs::HeadPlan head;                     // fused levels 0..k (depth 0 = not used)
     bfs::HeadGroup* d_head_groups = nullptr;
     int* d_head_tab = nullptr;
+    int* d_lvl0 = nullptr;             // Pravir plans: level-0 row cumsum (nchan+1) then delays
     // adjoint (built on the first adjoint call): per level l >= 1, for every
     // row of level l-1 the level-l rows that read it, as CSR {row, shift}
     bfs::AdjointTables adj;
@@ -32,6 +33,7 @@ struct bfs_fdmt_plan {
         if (d_tab) cudaFree(d_tab);
         if (d_head_groups) cudaFree(d_head_groups);
         if (d_head_tab) cudaFree(d_head_tab);
+        if (d_lvl0) cudaFree(d_lvl0);
         for (void* b : d_buf)
             if (b) cudaFree(b);
         if (d_adj_off) cudaFree(d_adj_off);

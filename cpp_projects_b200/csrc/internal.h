@@ -58,17 +58,27 @@ struct FdmtLevel {
 };
 
 struct FdmtPlanHost {
+    int kind = BFS_PLAN_KEITH;
     float fmin = 0, fmax = 0;
     int nchan = 0, ncols = 0, max_dt = 0;
     int niter = 0;
-    int rows_per_chan0 = 0;  // level-0 rows of every channel (d0 + 1)
+    int rows_per_chan0 = 0;  // level-0 rows of every channel (d0 + 1); Pravir plans: 0
+                             // (per channel: lv[0].rows, delays dt0)
+    std::vector<int> dt0;    // Pravir plans: the delay of every level-0 row
+    std::vector<int> dt_out; // delay of every output row
     std::vector<FdmtLevel> lv;  // niter + 1 levels
+    int out_rows() const { return lv.empty() ? 0 : lv.back().total_rows(); }
 };
 
 // Builds the plan exactly as the reference's CFdmtB/CFdmtCpu do.  Returns
 // BFS_OK or BFS_ERR_ARG (with the message set).
 bfs_status build_fdmt_plan(float fmin, float fmax, int nchan, int ncols, int max_dt,
                            FdmtPlanHost* out);
+// The reference's second FDMT variant (FDMT_PRAVIR): delay grids dt_min ..
+// dt_max step dt_step per sub-band, window-mean level 0, rounded mid-band
+// mappings.  BFS_ERR_ARG where the reference throws.
+bfs_status build_pravir_plan(float fmin, float fmax, int nchan, int ncols, int dt_max, int dt_step,
+                             int dt_min, FdmtPlanHost* out);
 
 // Inverse row tables of the adjoint: for level l >= 1 and every row i of the
 // level-(l-1) plane, the level-l rows g that read row i, with the shift of

@@ -253,4 +253,157 @@ void build_adjoint_tables(const FdmtPlanHost& p, AdjointTables* out) {
     out->built = true;
 }
 
+// ---------------------------------------------------------------------------
+// Pravir plan.  Restates MyVSLib_C++/FDMT_PRAVIR/fdmt_base.cpp:86-278 with
+// fdmtUtils.cpp:36-45,92-108, keeping the reference's float arithmetic: the
+// dispersion coefficient of a sub-band is a float quotient of float powers
+// (std::pow(float, float)), delays are float products rounded with
+// std::round, the nearest grid index prefers the upper neighbour on ties.
+// ---------------------------------------------------------------------------
+namespace {
+
+float pravir_cff(float f1s, float f1e, float f2s, float f2e) {
+    const float e = -2.0f;
+    return (std::pow(f1s, e) - std::pow(f1e, e)) / (std::pow(f2s, e) - std::pow(f2e, e));
+}
+
+long pravir_round(float v) { return static_cast<long>(std::round(v)); }
+
+std::vector<int> pravir_grid(float fs, float fe, float fmin, float fmax, int dt_max, int dt_min, int step) {
+    const float r = pravir_cff(fs, fe, fmin, fmax);
+    const long hi = pravir_round(static_cast<float>(dt_max) * r);
+    const long lo = pravir_round(static_cast<float>(dt_min) * r);
+    std::vector<int> g;
+    for (long d = lo; d <= hi; d += step) g.push_back(static_cast<int>(d));
+    return g;
+}
+
+int pravir_closest(const std::vector<int>& g, long v) {
+    const auto it = std::lower_bound(g.begin(), g.end(), v);
+    int idx = static_cast<int>(it - g.begin());
+    if (it != g.end()) {
+        if (it != g.begin() && v - *(it - 1) < *it - v) --idx;
+    } else {
+        idx = static_cast<int>(g.size()) - 1;
+    }
+    return idx;
+}
+
+}  // namespace
+
+bfs_status build_pravir_plan(float fmin, float fmax, int nchan, int ncols, int dt_max, int dt_step,
+                             int dt_min, FdmtPlanHost* out) {
+    BFS_ARG(out != nullptr, "plan output is null");
+    BFS_ARG(nchan >= 2, "nchan must be >= 2 (got %d)", nchan);
+    BFS_ARG(ncols >= 1, "ncols must be >= 1 (got %d)", ncols);
+    BFS_ARG(dt_step >= 1 && dt_min >= 0 && dt_max >= dt_min, "need dt_step >= 1, 0 <= dt_min <= dt_max");
+    BFS_ARG(std::isfinite(fmin) && std::isfinite(fmax) && fmin > 0.0f && fmax > fmin,
+            "need 0 < fmin < fmax (got %g, %g)", fmin, fmax);
+    FdmtPlanHost& p = *out;
+    p = FdmtPlanHost{};
+    p.kind = BFS_PLAN_PRAVIR;
+    p.fmin = fmin; p.fmax = fmax; p.nchan = nchan; p.ncols = ncols;
+    int n = 0;
+    while ((1 << n) < nchan) ++n;
+    p.niter = n;
+    p.lv.resize(n + 1);
+    const float df = (fmax - fmin) / static_cast<float>(nchan);
+    const float corr = df / 2;
+
+    // level 0: one sub-band per channel, rows = its delay grid
+    std::vector<std::vector<int>> grids(nchan);
+    {
+        FdmtLevel& L = p.lv[0];
+        L.nsub = nchan;
+        L.rows.resize(nchan);
+        for (int i = 0; i < nchan; ++i) {
+            const float fs = df * static_cast<float>(i) + fmin;
+            const float fe = fs + df;
+            grids[i] = pravir_grid(fs, fe, fmin, fmax, dt_max, dt_min, dt_step);
+            BFS_ARG(!grids[i].empty(), "channel %d has an empty delay grid", i);
+            L.rows[i] = static_cast<int>(grids[i].size());
+            for (int d : grids[i]) p.dt0.push_back(d);
+        }
+    }
+    std::vector<int> top = grids[nchan - 1];
+    float df_top = df, df_bot = df;
+    for (int l = 1; l <= n; ++l) {
+        const FdmtLevel& P = p.lv[l - 1];
+        FdmtLevel& L = p.lv[l];
+        const int nprev = P.nsub;
+        const int ncur = nprev / 2 + nprev % 2;
+        const bool do_copy = nprev % 2 == 1;
+        const float dtop = do_copy ? df_top : df_top + df_bot;
+        const float dbot = df_bot * 2;
+        std::vector<std::vector<int>> cur(ncur);
+        std::vector<float> fst(ncur), fen(ncur), fmd(ncur);
+        for (int i = 0; i < ncur; ++i) {
+            const float fs = dbot * static_cast<float>(i) + fmin;
+            float fe, fm;
+            if (i == ncur - 1) {
+                if (do_copy) {
+                    fe = fs + dtop * 2;
+                    fm = fs + dtop;
+                    cur[i] = top;
+                } else {
+                    fe = fs + dtop;
+                    fm = fs + dbot / 2;
+                    cur[i] = pravir_grid(fs, fe, fmin, fmax, dt_max, dt_min, dt_step);
+                    top = cur[i];
+                }
+            } else {
+                fe = fs + dbot;
+                fm = fs + dbot / 2;
+                cur[i] = pravir_grid(fs, fe, fmin, fmax, dt_max, dt_min, dt_step);
+            }
+            BFS_ARG(!cur[i].empty(), "level %d sub-band %d has an empty delay grid", l, i);
+            fst[i] = fs; fen[i] = fe; fmd[i] = fm;
+        }
+        L.nsub = ncur;
+        L.rows.resize(ncur);
+        for (int i = 0; i < ncur; ++i) L.rows[i] = static_cast<int>(cur[i].size());
+        L.cum.assign(ncur + 1, 0);
+        for (int i = 0; i < ncur; ++i) L.cum[i + 1] = L.cum[i] + L.rows[i];
+        std::vector<int> pcum(nprev + 1, 0);
+        for (int i = 0; i < nprev; ++i) pcum[i + 1] = pcum[i] + P.rows[i];
+        const int R = L.cum[ncur];
+        L.a_row.resize(R); L.b_row.resize(R); L.shift.resize(R); L.lookback.assign(R, 0);
+        for (int i = 0; i < ncur; ++i) {
+            const int tail = 2 * i, head = 2 * i + 1;
+            const float fs = fst[i], fe = fen[i];
+            const float fm1 = fmd[i] - corr, fm2 = fmd[i] + corr;
+            for (int j = 0; j < L.rows[i]; ++j) {
+                const long dt = cur[i][j];
+                const long m1 = pravir_round(static_cast<float>(dt) * pravir_cff(fs, fm1, fs, fe));
+                const long m2 = pravir_round(static_cast<float>(dt) * pravir_cff(fs, fm2, fs, fe));
+                BFS_ARG(m1 <= dt && m2 <= dt, "level %d: mid-band delay above the delay", l);
+                const int row = L.cum[i] + j;
+                if (i == ncur - 1 && do_copy) {
+                    L.a_row[row] = pcum[tail] + pravir_closest(grids[tail], dt);
+                    L.b_row[row] = -1;
+                    L.shift[row] = 0;
+                } else {
+                    BFS_ARG(m2 < ncols, "level %d: offset %ld >= ncols %d", l, m2, ncols);
+                    L.a_row[row] = pcum[tail] + pravir_closest(grids[tail], m1);
+                    L.b_row[row] = pcum[head] + pravir_closest(grids[head], dt - m2);
+                    L.shift[row] = static_cast<int>(m2);
+                }
+            }
+        }
+        grids = std::move(cur);
+        df_top = dtop;
+        df_bot = dbot;
+    }
+    for (auto& L : p.lv) {
+        if (L.cum.size() != static_cast<size_t>(L.nsub + 1)) {
+            L.cum.assign(L.nsub + 1, 0);
+            for (int i = 0; i < L.nsub; ++i) L.cum[i + 1] = L.cum[i] + L.rows[i];
+        }
+    }
+    p.dt_out = grids[0];
+    p.max_dt = p.out_rows();
+    p.rows_per_chan0 = 0;
+    return BFS_OK;
+}
+
 }  // namespace bfs

@@ -140,3 +140,99 @@ class CFdmtGpu:
         out = torch.empty((self.m_imaxDt, self.m_cols), dtype=torch.float32, device=d_in.device)
         self.process_image(d_in, out, b_ones)
         return out
+
+
+# Dispersion constant of the reference's DM grid (TEMPO2 / Manchester & Taylor
+# 1972, L/FDMT_PRAVIR/fdmtUtils.hpp:7-11), MHz^2 pc^-1 cm^3 s.
+K_DISP_MT = np.float32(4.1493774e3)
+
+
+class FDMTGPU:
+    """The reference's second FDMT variant (``FDMT`` / ``FDMTGPU``,
+    MyVSLib_C++/FDMT_PRAVIR/fdmt_base.hpp:37-84, fdmt_gpu.cuh) on the
+    library's kernels: delay grids ``dt_min .. dt_max`` step ``dt_step``,
+    window-mean level 0, rounded mid-band mappings (``BFS_PLAN_PRAVIR``).
+    ``execute`` takes device tensors and raises ``ValueError`` on a size
+    mismatch (the reference throws ``std::invalid_argument``)."""
+
+    def __init__(self, f_min: float, f_max: float, nchans: int, nsamps: int, tsamp: float,
+                 dt_max: int, dt_step: int = 1, dt_min: int = 0, external_ws: bool = False):
+        self.m_f_min, self.m_f_max = float(f_min), float(f_max)
+        self.m_nchans, self.m_nsamps = int(nchans), int(nsamps)
+        self.m_tsamp = float(tsamp)
+        self.m_dt_max, self.m_dt_step, self.m_dt_min = int(dt_max), int(dt_step), int(dt_min)
+        desc = _capi.FdmtDesc(fmin=self.m_f_min, fmax=self.m_f_max, nchan=self.m_nchans,
+                              ncols=self.m_nsamps, max_dt=self.m_dt_max, plan_kind=_capi.BFS_PLAN_PRAVIR,
+                              fuse_depth=0, dt_min=self.m_dt_min, dt_step=self.m_dt_step,
+                              tsamp=self.m_tsamp,
+                              flags=_capi.BFS_FDMT_EXTERNAL_WS if external_ws else 0)
+        self._plan = ctypes.c_void_p()
+        _capi.call("bfs_fdmt_plan_create", ctypes.byref(desc), ctypes.byref(self._plan))
+        self.info = _capi.FdmtInfo()
+        _capi.call("bfs_fdmt_plan_info", self._plan, ctypes.byref(self.info))
+
+    def __del__(self):
+        p = getattr(self, "_plan", None)
+        if p is not None and p.value:
+            try:
+                _capi.lib().bfs_fdmt_plan_destroy(p)
+            except Exception:
+                pass
+            self._plan = None
+
+    # --- the reference's getters --------------------------------------------
+    def get_df(self) -> float:
+        return float(np.float32(np.float32(self.m_f_max) - np.float32(self.m_f_min)) / np.float32(self.m_nchans))
+
+    def get_correction(self) -> float:
+        return float(np.float32(self.get_df()) / np.float32(2))
+
+    def get_niters(self) -> int:
+        return int(self.info.niter)
+
+    def get_dt_grid_final(self) -> list[int]:
+        n = int(self.info.out_rows)
+        dt = np.zeros(n, np.int32)
+        _capi.call("bfs_fdmt_plan_delays", self._plan, dt.ctypes.data_as(ctypes.c_void_p), n, None, None, 0)
+        return [int(v) for v in dt]
+
+    def get_dm_grid_final(self) -> list[float]:
+        """dt * tsamp / (K (f_min^-2 - f_max^-2)) in float32
+        (L/FDMT_PRAVIR/fdmt_base.cpp:64-74)."""
+        f32 = np.float32
+        conv = f32(K_DISP_MT * (np.power(f32(self.m_f_min), f32(-2.0)) - np.power(f32(self.m_f_max), f32(-2.0))))
+        step = f32(f32(self.m_tsamp) / conv)
+        return [float(f32(f32(dt) * step)) for dt in self.get_dt_grid_final()]
+
+    @property
+    def out_rows(self) -> int:
+        return int(self.info.out_rows)
+
+    @property
+    def alg_bytes(self) -> float:
+        return float(self.info.alg_bytes)
+
+    # --- transform --------------------------------------------------------------
+    def execute(self, waterfall: torch.Tensor, waterfall_size: int, dmt: torch.Tensor, dmt_size: int,
+                stream: torch.cuda.Stream | None = None) -> None:
+        if waterfall_size != self.m_nchans * self.m_nsamps or waterfall.numel() != waterfall_size:
+            raise ValueError("Invalid size of waterfall")
+        if dmt_size != self.out_rows * self.m_nsamps or dmt.numel() != dmt_size:
+            raise ValueError("Invalid size of dmt")
+        _capi.call("bfs_fdmt_execute", self._plan, dev_ptr(waterfall, torch.float32, "waterfall"),
+                   dev_ptr(dmt, torch.float32, "dmt"), 0, stream_handle(stream))
+
+    def __call__(self, waterfall: torch.Tensor) -> torch.Tensor:
+        out = torch.empty((self.out_rows, self.m_nsamps), dtype=torch.float32, device=waterfall.device)
+        self.execute(waterfall, waterfall.numel(), out, out.numel())
+        return out
+
+    def adjoint(self, d_grad_out: torch.Tensor, d_grad_in: torch.Tensor | None = None,
+                stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+        if d_grad_in is None:
+            d_grad_in = torch.empty((self.m_nchans, self.m_nsamps), dtype=torch.float32,
+                                    device=d_grad_out.device)
+        _capi.call("bfs_fdmt_adjoint", self._plan, dev_ptr(d_grad_out, torch.float32, "d_grad_out"),
+                   dev_ptr(d_grad_in, torch.float32, "d_grad_in"), stream_handle(stream))
+        return d_grad_in
+

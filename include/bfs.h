@@ -56,7 +56,12 @@ bfs_status bfs_trim_scratch(void);
  * Input: nchan x ncols float32, row 0 = fmin channel.  Output: max_dt x ncols,
  * row d = delay d samples across the band.
  * ---------------------------------------------------------------------- */
-enum { BFS_PLAN_KEITH = 0 };
+/* Plan kinds: BFS_PLAN_KEITH — the reference's CFdmtCpu/CFdmtGpu plan
+ * (L/FDMT/FdmtB.cpp, FdmtCpu.cpp); BFS_PLAN_PRAVIR — its second FDMT variant
+ * (L/FDMT_PRAVIR/fdmt_base.cpp:118-278, fdmt_cpu.cpp:28-301): delay grids
+ * dt_min..max_dt step dt_step, window-mean level 0, output rows = the final
+ * grid's length (max_dt - dt_min)/dt_step + 1, no fused head. */
+enum { BFS_PLAN_KEITH = 0, BFS_PLAN_PRAVIR = 1 };
 /* Storage of the FDMT planes between levels (no reference counterpart: the
  * reference is FP32 throughout).  F16 / BF16 store those planes as 16-bit
  * values, row g scaled by 2^-ceil(log2(channels summed into g)); sums are
@@ -78,7 +83,10 @@ typedef struct bfs_fdmt_desc {
                           head keeping 2 CTAs/SM; 0: level-by-level; k: fuse levels 0..k */
     int flags;         /* BFS_FDMT_EXTERNAL_WS: the plan allocates no planes; use _execute_ws */
     int head_tile;     /* samples per CTA of the fused head (0 = 256)                  */
-    int reserved[6];
+    int dt_min;        /* BFS_PLAN_PRAVIR: smallest delay of the grid (0)              */
+    int dt_step;       /* BFS_PLAN_PRAVIR: grid step (0 is taken as 1)                 */
+    float tsamp;       /* BFS_PLAN_PRAVIR: sample time (s), for the DM grid only       */
+    int reserved[3];
 } bfs_fdmt_desc;
 
 typedef struct bfs_fdmt_plan bfs_fdmt_plan;
@@ -90,6 +98,7 @@ typedef struct bfs_fdmt_info {
     int64_t rows_total;     /* sum of rows over levels 0..niter               */
     size_t workspace_bytes; /* device scratch the plan owns                   */
     double alg_bytes;       /* level-by-level algorithmic bytes of one call   */
+    int out_rows;           /* output rows (max_dt; Pravir: the grid length)  */
 } bfs_fdmt_info;
 
 bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc, bfs_fdmt_plan** plan);
@@ -104,6 +113,12 @@ bfs_status bfs_fdmt_plan_destroy(bfs_fdmt_plan* plan);
 bfs_status bfs_fdmt_plan_info(const bfs_fdmt_plan* plan, bfs_fdmt_info* info);
 /* rows_per_level[0..niter] (cap entries at most); returns BFS_ERR_ARG if cap too small */
 bfs_status bfs_fdmt_plan_rows(const bfs_fdmt_plan* plan, int* rows_per_level, int cap);
+/* Delays of the output rows (out_cap >= out_rows; the reference's
+ * FDMT::get_dt_grid_final, L/FDMT_PRAVIR/fdmt_base.cpp:61-63) and of the
+ * level-0 rows with the level-0 row cumsum over channels (nchan + 1).  Any
+ * pointer may be null. */
+bfs_status bfs_fdmt_plan_delays(const bfs_fdmt_plan* plan, int* out_dt, int out_cap, int* lvl0_cum,
+                                int* lvl0_dt, int lvl0_cap);
 /* Host copies of level `level`'s (>= 1) row tables: tail row, head row (-1 = copied row), head shift. */
 bfs_status bfs_fdmt_plan_tables(const bfs_fdmt_plan* plan, int level, int* a_row, int* b_row,
                                 int* shift, int cap);

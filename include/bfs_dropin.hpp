@@ -4,6 +4,7 @@
 // Statistical_preprocessing.cuh and Clusterization.cuh, and link libbfs_b200.
 //
 //   CFdmtGpu                      L/FDMT/FdmtGpu.cuh:5-53
+//   FDMTGPU (Pravir plan)         L/FDMT_PRAVIR/fdmt_base.hpp:37-84, fdmt_gpu.cuh
 //   statistical_preprocessing::   L/CDMT/Statistical_preprocessing.cuh:9-10
 //   clusterization::              L/Clusterization/Clusterization.cuh:10-67
 //   select_delegates::write_log   L/Clusterization/select_delegates.cu:127-177
@@ -14,9 +15,11 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <fstream>
 #include <iomanip>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -78,6 +81,61 @@ public:
 private:
     bfs_fdmt_plan* m_plan = nullptr;
     bfs_status m_status = BFS_OK;
+};
+
+// The reference's second FDMT variant (L/FDMT_PRAVIR/fdmt_base.hpp:37-84,
+// fdmt_gpu.cuh): FDMTGPU(f_min, f_max, nchans, nsamps, tsamp, dt_max,
+// dt_step, dt_min), execute(waterfall, waterfall_size, dmt, dmt_size) on
+// device pointers, throwing std::invalid_argument on a size mismatch (as
+// FDMT::check_inputs, fdmt_base.cpp:106-116) and std::runtime_error where the
+// library reports an error.
+class FDMTGPU {
+public:
+    FDMTGPU(float f_min, float f_max, size_t nchans, size_t nsamps, float tsamp, size_t dt_max,
+            size_t dt_step = 1, size_t dt_min = 0)
+        : m_nchans(nchans), m_nsamps(nsamps), m_tsamp(tsamp), m_f_min(f_min), m_f_max(f_max) {
+        bfs_fdmt_desc d{};
+        d.fmin = f_min; d.fmax = f_max; d.nchan = static_cast<int>(nchans);
+        d.ncols = static_cast<int>(nsamps); d.max_dt = static_cast<int>(dt_max);
+        d.plan_kind = BFS_PLAN_PRAVIR; d.precision = BFS_PREC_F32; d.fuse_depth = 0;
+        d.dt_step = static_cast<int>(dt_step); d.dt_min = static_cast<int>(dt_min); d.tsamp = tsamp;
+        if (bfs_fdmt_plan_create(&d, &m_plan) != BFS_OK) throw std::runtime_error(bfs_last_error());
+        bfs_fdmt_info info{};
+        bfs_fdmt_plan_info(m_plan, &info);
+        m_niters = static_cast<size_t>(info.niter);
+        m_dt_grid.resize(static_cast<size_t>(info.out_rows));
+        std::vector<int> dt(m_dt_grid.size());
+        bfs_fdmt_plan_delays(m_plan, dt.data(), static_cast<int>(dt.size()), nullptr, nullptr, 0);
+        for (size_t i = 0; i < dt.size(); ++i) m_dt_grid[i] = static_cast<size_t>(dt[i]);
+    }
+    FDMTGPU(const FDMTGPU&) = delete;
+    FDMTGPU& operator=(const FDMTGPU&) = delete;
+    ~FDMTGPU() { if (m_plan) bfs_fdmt_plan_destroy(m_plan); }
+
+    float get_df() const { return (m_f_max - m_f_min) / static_cast<float>(m_nchans); }
+    float get_correction() const { return get_df() / 2; }
+    size_t get_niters() const { return m_niters; }
+    const std::vector<size_t>& get_dt_grid_final() const { return m_dt_grid; }
+    std::vector<float> get_dm_grid_final() const {
+        const float k = 4.1493774e3f;  // L/FDMT_PRAVIR/fdmtUtils.hpp:9,11
+        const float conv = k * (std::pow(m_f_min, -2.0f) - std::pow(m_f_max, -2.0f));
+        const float step = m_tsamp / conv;
+        std::vector<float> dm(m_dt_grid.size());
+        for (size_t i = 0; i < dm.size(); ++i) dm[i] = static_cast<float>(m_dt_grid[i]) * step;
+        return dm;
+    }
+    void execute(const float* waterfall, size_t waterfall_size, float* dmt, size_t dmt_size) {
+        if (waterfall_size != m_nchans * m_nsamps) throw std::invalid_argument("Invalid size of waterfall");
+        if (dmt_size != m_dt_grid.size() * m_nsamps) throw std::invalid_argument("Invalid size of dmt");
+        if (bfs_fdmt_execute(m_plan, waterfall, dmt, 0, nullptr) != BFS_OK)
+            throw std::runtime_error(bfs_last_error());
+    }
+
+private:
+    bfs_fdmt_plan* m_plan = nullptr;
+    size_t m_nchans, m_nsamps, m_niters = 0;
+    float m_tsamp, m_f_min, m_f_max;
+    std::vector<size_t> m_dt_grid;
 };
 
 namespace statistical_preprocessing {

@@ -51,6 +51,24 @@ int orc_fdmt_adjoint_f32(float fmin, float fmax, int nchan, int cols, int max_dt
 int orc_fdmt_adjoint_f64(float fmin, float fmax, int nchan, int cols, int max_dt,
                          const double* gy, double* gx);
 
+/* --- Pravir-plan FDMT (reference: MyVSLib_C++/FDMT_PRAVIR/) -------------
+ * All return < 0 where the reference throws.  rows_per_level[0..niter];
+ * orc_pravir_level: sub-band row cumsum (nsub+1), dt of every row and, for
+ * level >= 1, tail row, head row (-1: copied) and offset; returns the rows. */
+int orc_pravir_rows(float fmin, float fmax, int nchans, int nsamps, long dt_max, long dt_step,
+                    long dt_min, int* rows_per_level, int cap);
+int orc_pravir_level(float fmin, float fmax, int nchans, int nsamps, long dt_max, long dt_step,
+                     long dt_min, int level, int* cum, int* dt, int* a_row, int* b_row, int* shift,
+                     int cap);
+int orc_pravir_run_f32(float fmin, float fmax, int nchans, int nsamps, long dt_max, long dt_step,
+                       long dt_min, const float* in, float* out);
+int orc_pravir_run_f64(float fmin, float fmax, int nchans, int nsamps, long dt_max, long dt_step,
+                       long dt_min, const double* in, double* out);
+int orc_pravir_adjoint_f32(float fmin, float fmax, int nchans, int nsamps, long dt_max, long dt_step,
+                           long dt_min, const float* gy, float* gx);
+int orc_pravir_adjoint_f64(float fmin, float fmax, int nchans, int nsamps, long dt_max, long dt_step,
+                           long dt_min, const double* gy, double* gx);
+
 /* --- search (reference: MyVSLib_C++/Clusterization/ sources) --------------- */
 int64_t orc_boxcar(const float* plane, int rows, int cols, float thr, int mode,
                    int param, orc_cand* out, int64_t cap);

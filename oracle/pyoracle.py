@@ -58,6 +58,28 @@ def ref_lib() -> ctypes.CDLL | None:
     return _ref
 
 
+_ref_pravir = None
+
+
+def ref_pravir_lib() -> ctypes.CDLL | None:
+    """The reference's own FDMTCPU (Pravir plan, oracle/_ref), or None."""
+    global _ref_pravir
+    if _ref_pravir is None:
+        path = HERE / "_ref" / "libref_pravir.so"
+        if not path.exists():
+            return None
+        l = ctypes.CDLL(str(path))
+        L = ctypes.c_long
+        l.ref_pravir_rows.restype = L
+        l.ref_pravir_rows.argtypes = [_F, _F, L, L, _F, L, L, L]
+        l.ref_pravir_dt_grid.restype = L
+        l.ref_pravir_dt_grid.argtypes = [_F, _F, L, L, _F, L, L, L, _P, L]
+        l.ref_pravir_execute.restype = ctypes.c_int
+        l.ref_pravir_execute.argtypes = [_F, _F, L, L, _F, L, L, L, _P, _P, L, ctypes.c_int]
+        _ref_pravir = l
+    return _ref_pravir
+
+
 def ref_gpu_lib() -> ctypes.CDLL | None:
     """The reference's own GPU classes (oracle/_ref/libref_gpu.so), or None."""
     global _ref_gpu
@@ -207,6 +229,79 @@ def snr_cells_f64(y: np.ndarray, cells: np.ndarray):
         win[t:t + w] = 1.0
         grads.append((win - w / n) / (sd * np.sqrt(w)) - snr[k] * (row - m) / (n * sd * sd))
     return snr, grads
+
+
+# ---- Pravir plan kind -----------------------------------------------------------
+def _pravir_lib():
+    l = lib()
+    L = ctypes.c_long
+    for n in ("orc_pravir_rows", "orc_pravir_level", "orc_pravir_run_f32", "orc_pravir_run_f64",
+              "orc_pravir_adjoint_f32", "orc_pravir_adjoint_f64"):
+        getattr(l, n).restype = ctypes.c_int
+    l.orc_pravir_rows.argtypes = [_F, _F, ctypes.c_int, ctypes.c_int, L, L, L, _P, ctypes.c_int]
+    l.orc_pravir_level.argtypes = [_F, _F, ctypes.c_int, ctypes.c_int, L, L, L, ctypes.c_int,
+                                   _P, _P, _P, _P, _P, ctypes.c_int]
+    for n in ("orc_pravir_run_f32", "orc_pravir_run_f64", "orc_pravir_adjoint_f32", "orc_pravir_adjoint_f64"):
+        getattr(l, n).argtypes = [_F, _F, ctypes.c_int, ctypes.c_int, L, L, L, _P, _P]
+    return l
+
+
+def pravir_rows(fmin, fmax, nchans, nsamps, dt_max, dt_step=1, dt_min=0) -> np.ndarray:
+    rows = np.zeros(64, np.int32)
+    n = _pravir_lib().orc_pravir_rows(_F(fmin), _F(fmax), nchans, nsamps, dt_max, dt_step, dt_min,
+                                      _ptr(rows), rows.size)
+    if n < 0:
+        raise ValueError(f"plan rejected ({n})")
+    return rows[: n + 1].copy()
+
+
+def pravir_level(fmin, fmax, nchans, nsamps, dt_max, dt_step, dt_min, level):
+    """(cum, dt, a, b, s) of one level of the Pravir plan (a, b, s empty at level 0)."""
+    rows = int(pravir_rows(fmin, fmax, nchans, nsamps, dt_max, dt_step, dt_min)[level])
+    cap = max(rows, nchans) + 1
+    cum = np.zeros(cap, np.int32); dt = np.zeros(cap, np.int32)
+    a = np.zeros(cap, np.int32); b = np.zeros(cap, np.int32); s = np.zeros(cap, np.int32)
+    _pravir_lib().orc_pravir_level(_F(fmin), _F(fmax), nchans, nsamps, dt_max, dt_step, dt_min, level,
+                                   _ptr(cum), _ptr(dt), _ptr(a), _ptr(b), _ptr(s), cap)
+    return cum, dt[:rows], a[:rows], b[:rows], s[:rows]
+
+
+def pravir_fdmt(fmin, fmax, x: np.ndarray, nchans, nsamps, dt_max, dt_step=1, dt_min=0,
+                dtype=np.float32) -> np.ndarray:
+    nout = int(pravir_rows(fmin, fmax, nchans, nsamps, dt_max, dt_step, dt_min)[-1])
+    out = np.zeros((nout, nsamps), dtype)
+    xin = np.ascontiguousarray(x, dtype)
+    fn = _pravir_lib().orc_pravir_run_f32 if dtype == np.float32 else _pravir_lib().orc_pravir_run_f64
+    if fn(_F(fmin), _F(fmax), nchans, nsamps, dt_max, dt_step, dt_min, _ptr(xin), _ptr(out)) != 0:
+        raise ValueError("oracle Pravir FDMT failed")
+    return out
+
+
+def pravir_adjoint(fmin, fmax, gy: np.ndarray, nchans, nsamps, dt_max, dt_step=1, dt_min=0,
+                   dtype=np.float32) -> np.ndarray:
+    gx = np.zeros((nchans, nsamps), dtype)
+    g = np.ascontiguousarray(gy, dtype)
+    fn = _pravir_lib().orc_pravir_adjoint_f32 if dtype == np.float32 else _pravir_lib().orc_pravir_adjoint_f64
+    if fn(_F(fmin), _F(fmax), nchans, nsamps, dt_max, dt_step, dt_min, _ptr(g), _ptr(gx)) != 0:
+        raise ValueError("oracle Pravir adjoint failed")
+    return gx
+
+
+def ref_pravir_cpu(fmin, fmax, x: np.ndarray, nchans, nsamps, dt_max, dt_step=1, dt_min=0,
+                   tsamp=1.0, threads=1) -> np.ndarray | None:
+    """A fresh reference FDMTCPU(...).execute() (None if not built or it throws)."""
+    r = ref_pravir_lib()
+    if r is None:
+        return None
+    n = r.ref_pravir_rows(fmin, fmax, nchans, nsamps, tsamp, dt_max, dt_step, dt_min)
+    if n < 0:
+        return None
+    out = np.zeros((n, nsamps), np.float32)
+    xin = np.ascontiguousarray(x, np.float32)
+    if r.ref_pravir_execute(fmin, fmax, nchans, nsamps, tsamp, dt_max, dt_step, dt_min, _ptr(xin), _ptr(out),
+                            out.size, threads) != 0:
+        return None
+    return out
 
 
 def ref_fdmt_cpu(fmin, fmax, x: np.ndarray | None, nchan, ncols, max_dt, b_ones=False,

@@ -1,18 +1,20 @@
 // A reference-style driver written against the reference's own names
 // (CFdmtGpu, clusterization::clusterization_main), compiled with
 // include/bfs_dropin.hpp instead of the reference headers.
-//   dropin_demo <fdmt_in.bin> <fdmt_out.bin> <log file>
+//   dropin_demo <fdmt_in.bin> <fdmt_out.bin> <log file> <pravir_out.bin>
 // Reads a 64 x 1024 float32 filterbank, writes its FDMT (1200-1600 MHz,
 // max delay 64), then runs clusterization_main on the reference's 3 x 16 test
 // plane (clusterization_forpravir/clusterization_test.cu:63-112) with W = 2,
-// threshold 4 and metrics {2, 1, 2}.
+// threshold 4 and metrics {2, 1, 2}; also runs the Pravir-plan FDMTGPU
+// (tsamp 1 ms, dt_max 64) on the same filterbank and checks that a size
+// mismatch throws std::invalid_argument.
 #include <cstdio>
 #include <vector>
 
 #include "bfs_dropin.hpp"
 
 int main(int argc, char** argv) {
-    if (argc != 4) { std::fprintf(stderr, "usage: %s in.bin out.bin log\n", argv[0]); return 2; }
+    if (argc != 5) { std::fprintf(stderr, "usage: %s in.bin out.bin log pravir.bin\n", argv[0]); return 2; }
     const int nchan = 64, cols = 1024, maxdt = 64;
     std::vector<float> in(nchan * cols), out(maxdt * cols);
     FILE* f = std::fopen(argv[1], "rb");
@@ -29,6 +31,27 @@ int main(int argc, char** argv) {
     f = std::fopen(argv[2], "wb");
     std::fwrite(out.data(), sizeof(float), out.size(), f);
     std::fclose(f);
+
+    {
+        FDMTGPU pravir(1200.0f, 1600.0f, nchan, cols, 0.001f, maxdt);
+        const size_t nout = pravir.get_dt_grid_final().size() * cols;
+        float* d_pout = nullptr;
+        cudaMalloc(reinterpret_cast<void**>(&d_pout), nout * sizeof(float));
+        bool threw = false;
+        try {
+            pravir.execute(d_in, in.size() - 1, d_pout, nout);
+        } catch (const std::invalid_argument&) {
+            threw = true;
+        }
+        if (!threw) return 6;
+        pravir.execute(d_in, in.size(), d_pout, nout);
+        std::vector<float> pout(nout);
+        cudaMemcpy(pout.data(), d_pout, nout * sizeof(float), cudaMemcpyDeviceToHost);
+        cudaFree(d_pout);
+        f = std::fopen(argv[4], "wb");
+        std::fwrite(pout.data(), sizeof(float), pout.size(), f);
+        std::fclose(f);
+    }
 
     const int rows = 3, pc = 16;
     std::vector<float> plane(rows * pc, 2.0f);

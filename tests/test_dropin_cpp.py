@@ -1,6 +1,7 @@
 """The C++ drop-in header (include/bfs_dropin.hpp) compiles a reference-style
-driver unchanged (CPU) and, on the GPU, gives the same FDMT as the oracle and
-the expected delegate log for the reference's clustering test plane."""
+driver unchanged (CPU) and, on the GPU, gives the same FDMT (both plan kinds)
+as the oracle and the expected delegate log for the reference's clustering
+test plane."""
 import subprocess
 from pathlib import Path
 
@@ -35,11 +36,15 @@ def test_dropin_driver_runs_and_matches(cuda, tmp_path):
     x = np.random.default_rng(5).standard_normal((64, 1024)).astype(np.float32)
     x.tofile(tmp_path / "in.bin")
     r = subprocess.run([str(exe), str(tmp_path / "in.bin"), str(tmp_path / "out.bin"),
-                        str(tmp_path / "ouput.log")], capture_output=True, text=True)
+                        str(tmp_path / "ouput.log"), str(tmp_path / "pravir.bin")],
+                       capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     got = np.fromfile(tmp_path / "out.bin", np.float32).reshape(64, 1024)
     want = pyoracle.fdmt_f32(1200.0, 1600.0, x, 64, 1024, 64)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    pr = np.fromfile(tmp_path / "pravir.bin", np.float32).reshape(-1, 1024)
+    pwant = pyoracle.pravir_fdmt(1200.0, 1600.0, x, 64, 1024, 64)
+    assert pr.shape == pwant.shape and np.array_equal(pr.view(np.uint32), pwant.view(np.uint32))
     body = [ln.split() for ln in (tmp_path / "ouput.log").read_text().splitlines()[1:]]
     assert body == [["1", "4", "4e-05", "0", "1", "140", "3"],
                     ["2", "4", "4e-05", "2", "1", "100", "3"],
