@@ -55,8 +55,8 @@ def parse_args(argv=None):
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["config2", "config0", "config4fwd", "config3", "config4"],
-                    default="config2")
+    ap.add_argument("--workload", choices=["config2", "config0", "config4fwd", "config3", "config4",
+                                           "config1"], default="config2")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
@@ -687,10 +687,123 @@ def run_config4(args):
     return 0
 
 
+def run_config1(args):
+    """Full pipeline from raw voltages: one GUPPI-like chunk (32 coarse
+    channels x 2 pols x 4 128 768 int8 samples, 1200-1328 MHz, a pulse at
+    DM 56.8) through unpack -> forward FFT (2^20) -> FP64 chirp at DM 56.8 ->
+    inverse FFTs (1024 fine channels) -> detection + transpose + dedispersion
+    shifts -> calc_fdmt_inputs -> FDMT of data and mask (max delay 1024) ->
+    fdmt_normalization -> per-row normalisation + boxcar (widths 1..32, S/N
+    > 7) + clustering (+-16 samples, +-8 rows, any width).  value: fine
+    channel-samples (1024 x 129 024) per second of the device-timed step;
+    e2e: the same with the raw chunk copied from pinned host memory and the
+    delegates read back."""
+    import torch
+
+    from cpp_projects_b200 import search, synth
+    from cpp_projects_b200.chunk import CChunk_gpu
+    from cpp_projects_b200.cluster import complete_clusterization
+
+    if not torch.cuda.is_available():
+        print(json.dumps({"metric": METRIC, "error": "no CUDA device"}))
+        return 1
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    args.warmup = max(args.warmup, 3)
+    vc = synth.config1()
+    raw = synth.voltage_chunk(vc, dev)
+    ch = CChunk_gpu(vc.fmin, vc.fmax, vc.npol, vc.nchan, vc.len_sft, 0, 0, vc.dm, 0.0, 1, 7.0, 1, vc.nbin,
+                    vc.nfft, vc.noverlap, vc.tsamp, max_dt=vc.max_dt, dms=[vc.dm])
+    cplx = ch.complex_buffer(dev)
+    cands_buf = torch.empty((1 << 24, 4), dtype=torch.int32, device=dev)
+    units = ch.rows * ch.msamp
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+
+    def step(src):
+        ev[0].record()
+        ch.unpack(src, cplx)
+        ev[1].record()
+        planes = ch.process(cplx)
+        ev[2].record()
+        y = planes[0]
+        st = search.row_stats(y)
+        cands, n = search.boxcar_gather(y, 7.0, 0, 5, stats=st, out=cands_buf)
+        cl = complete_clusterization(cands, (16, 8, 1 << 30)) if n else None
+        ev[3].record()
+        return n, cl
+
+    for _ in range(args.warmup):
+        step(raw)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0).start()
+    t = {"unpack": 0.0, "coherent+fdmt": 0.0, "search": 0.0}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        n, cl = step(raw)
+        torch.cuda.synchronize()
+        t["unpack"] += ev[0].elapsed_time(ev[1])
+        t["coherent+fdmt"] += ev[1].elapsed_time(ev[2])
+        t["search"] += ev[2].elapsed_time(ev[3])
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    step_ms = sum(t.values()) / args.steps
+    dl = cl.delegate_records() if cl is not None else np.zeros(0)
+    top = dl[np.argmax(dl["msnr"])] if len(dl) else None
+    # e2e: the raw chunk from pinned host memory every step, delegates back
+    host = raw.cpu().pin_memory()
+    draw = torch.empty_like(raw)
+    for _ in range(2):
+        draw.copy_(host, non_blocking=True)
+        step(draw)
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    d2h = 0
+    for _ in range(args.steps):
+        draw.copy_(host, non_blocking=True)
+        n2, cl2 = step(draw)
+        recs = cl2.delegate_records() if cl2 is not None else np.zeros(0)
+        d2h += 4 + recs.nbytes
+    f1.record()
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1) / args.steps
+    peak, peak_kind = measured_peaks()
+    line = {
+        "metric": METRIC, "value": units / (step_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int8 in, FP64 chirp phase, f32",
+        "data": "synthetic GUPPI-like int8 voltages (uniform [-8, 7] + a pulse at DM 56.8), generated on device",
+        "config": {"workload": "config1", "coarse_channels": vc.nchan, "pols": vc.npol // 2,
+                   "samples_per_channel": vc.len_chunk, "band_mhz": [vc.fmin, vc.fmax], "nbin": vc.nbin,
+                   "nfft": vc.nfft, "noverlap": vc.noverlap, "fine_channels": ch.rows, "msamp": ch.msamp,
+                   "coherent_dms": [vc.dm], "max_dt": vc.max_dt,
+                   "search": "pow2 widths 1..32, S/N > 7, clusters +-16/+-8/any",
+                   "l2": "no flush: 512 MiB raw chunk and 2 GiB spectra exceed L2"},
+        "stages_ms": {k: v / args.steps for k, v in t.items()},
+        "roofline": None,
+        "e2e": {"value": units / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(host.numel()),
+                "d2h_bytes_per_step": d2h // args.steps, "ms_per_step": e2e_ms},
+        "candidates": int(n), "delegates": int(len(dl)),
+        "brightest": None if top is None else {"mt": int(top["mt"]), "mdt": int(top["mdt"]),
+                                               "mwidth": int(top["mwidth"]), "snr": float(top["msnr"])},
+        # the chunk's dedispersion shifts align every fine channel to the
+        # bottom of the band: t0 (top of band) plus the cross-band delay
+        "pulse_expected_mt": int((vc.t0 + 4.148808e3 * vc.dm * (vc.fmin ** -2 - vc.fmax ** -2) / vc.tsamp)
+                                 // vc.len_sft),
+        "cpu_baseline": None, "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None):
     args = parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "config1":
+        return run_config1(args)
     if args.workload == "config3":
         return run_config3(args)
     if args.workload == "config4":

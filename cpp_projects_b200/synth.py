@@ -108,6 +108,68 @@ def config3(seed: int = 3) -> Beam:
     return Beam(nchan, nsamp, 1100.0, 1500.0, nchan, seed, pulses, gain.astype(np.float32))
 
 
+@dataclass
+class VoltageChunk:
+    """A GUPPI-like voltage chunk and the coherent-dedispersion geometry the
+    reference's CChunkB derives from it (MyVSLib_C++/CDMT/ChunkB.h:77-98)."""
+    fmin: float
+    fmax: float
+    npol: int          # 4 = two complex polarisations (the reference's count)
+    nchan: int         # coarse channels
+    len_sft: int       # fine channels per coarse channel
+    nbin: int          # forward FFT length
+    nfft: int          # FFTs per chunk
+    noverlap: int      # overlap-save samples on each side
+    tsamp: float       # coarse sample time (s) = 1 / channel bandwidth
+    max_dt: int
+    dm: float          # DM of the injected pulse (pc cm^-3)
+    t0: int            # arrival sample of the pulse at the top of the band
+    amp: float         # impulse amplitude before dispersion
+    seed: int
+
+    @property
+    def len_chunk(self) -> int:
+        return (self.nbin - 2 * self.noverlap) * self.nfft
+
+
+def config1(seed: int = 1) -> VoltageChunk:
+    """32 coarse channels of 4 MHz (1200-1328 MHz), 2 polarisations, one chunk
+    of 4 x (2^20 - 2 x 8192) = 4 128 768 samples per channel (2^22 less the
+    overlap), int8 uniform in [-8, 7] plus a pulse at DM 56.8; FFT length 2^20
+    with 8192 samples of overlap-save on each side (the intra-channel smear at
+    DM 56.8 is ~4300 samples), 32 fine channels per coarse channel (1024 in
+    all), FDMT max delay 1024."""
+    return VoltageChunk(1200.0, 1328.0, 4, 32, 32, 1 << 20, 4, 8192, 0.25e-6, 1024, 56.8, 1_000_000,
+                        200.0, seed)
+
+
+def voltage_chunk(vc: VoltageChunk, device):
+    """Raw int8 chunk [nchan][len_chunk][npol] generated on the device: an
+    impulse in every coarse channel at t0 plus the cold-plasma delay of the
+    channel centre relative to the top of the band, dispersed inside the
+    channel by the transfer function exp(2 pi i k DM f^2 / (f0^2 (f0 + f)))
+    (k = 4.148808e9 MHz^2 s / (pc cm^-3) in these units), plus uniform integer
+    noise in [-8, 7], rounded and clipped to int8."""
+    import torch
+    n = vc.len_chunk
+    g = torch.Generator(device=device).manual_seed(int(vc.seed))
+    raw = torch.randint(-8, 8, (vc.nchan, n, vc.npol), generator=g, device=device, dtype=torch.int16)
+    bw_sub = (vc.fmax - vc.fmin) / vc.nchan
+    fb = torch.fft.fftfreq(n, d=1.0, device=device, dtype=torch.float64) * bw_sub  # MHz offsets
+    for c in range(vc.nchan):
+        f0 = vc.fmin + bw_sub * (0.5 + c)
+        delay = 4.148808e3 * vc.dm * (f0 ** -2 - vc.fmax ** -2) / vc.tsamp
+        x = torch.zeros(n, dtype=torch.complex128, device=device)
+        x[(vc.t0 + int(round(delay))) % n] = vc.amp
+        r = fb / f0
+        phase = vc.dm * r * r / (f0 + fb) * 4.148808e9
+        x = torch.fft.ifft(torch.fft.fft(x) * torch.exp(2j * np.pi * phase))
+        for p in range(vc.npol // 2):
+            raw[c, :, 2 * p] += torch.round(x.real).to(torch.int16)
+            raw[c, :, 2 * p + 1] += torch.round(x.imag).to(torch.int16)
+    return raw.clamp_(-8, 7).to(torch.int8)
+
+
 CONFIG0_SEARCH = dict(widths_mode=0, param=5, thr=7.0, metrics=(16, 8, 1 << 30))
 
 
