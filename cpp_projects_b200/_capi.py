@@ -58,6 +58,15 @@ class BatchDesc(ctypes.Structure):
                 ("use_graph", ctypes.c_int), ("reserved", ctypes.c_int * 8)]
 
 
+class GuppiHeader(ctypes.Structure):
+    _fields_ = [("nbits", ctypes.c_int), ("chan_bw", ctypes.c_float), ("npol", ctypes.c_int),
+                ("directio", ctypes.c_int), ("obsfreq", ctypes.c_float), ("nchan", ctypes.c_int),
+                ("obsbw", ctypes.c_float), ("blocsize", ctypes.c_int64), ("telescope", ctypes.c_int),
+                ("tbin", ctypes.c_float), ("straight_order", ctypes.c_int), ("data_offset", ctypes.c_int64),
+                ("nsamp", ctypes.c_int64), ("fmin", ctypes.c_float), ("fmax", ctypes.c_float),
+                ("reserved", ctypes.c_int * 4)]
+
+
 class Cand(ctypes.Structure):
     _fields_ = [("mt", ctypes.c_int), ("mdt", ctypes.c_int), ("mwidth", ctypes.c_int),
                 ("msnr", ctypes.c_float)]
@@ -104,6 +113,17 @@ _SIGNATURES = {
     "bfs_fdmt_adjoint_ws": (_I, [_P, _P, _P, _P, ctypes.c_size_t, _P]),
     "bfs_boxcar_snr_cells": (_I, [_P, _I, _I, _P, _P, _I, _P, _P]),
     "bfs_boxcar_snr_cells_adjoint": (_I, [_P, _I, _I, _P, _P, _I, _P, _P, _P, _P]),
+    "bfs_guppi_parse_header": (_I, [_P, ctypes.c_size_t, _P]),
+    "bfs_guppi_open": (_I, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+    "bfs_guppi_close": (_I, [_P]),
+    "bfs_guppi_blocks": (_I, [_P, ctypes.POINTER(_I)]),
+    "bfs_guppi_block_header": (_I, [_P, _I, _P]),
+    "bfs_guppi_chunk_count": (_I, [_P, _I, ctypes.c_int64, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
+    "bfs_guppi_read_chunk": (_I, [_P, _I, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, _P, ctypes.c_size_t]),
+    "bfs_guppi_reader_create": (_I, [_P, ctypes.c_int64, ctypes.c_int64, _I, _I, ctypes.POINTER(_P)]),
+    "bfs_guppi_reader_next": (_I, [_P, _P, _P, ctypes.POINTER(_P), ctypes.POINTER(_I),
+                                   ctypes.POINTER(ctypes.c_int64)]),
+    "bfs_guppi_reader_destroy": (_I, [_P]),
     "bfs_batch_create": (_I, [ctypes.POINTER(BatchDesc), ctypes.POINTER(_P)]),
     "bfs_batch_destroy": (_I, [_P]),
     "bfs_batch_run": (_I, [_P, _P, _P]),

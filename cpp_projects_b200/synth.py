@@ -170,6 +170,47 @@ def voltage_chunk(vc: VoltageChunk, device):
     return raw.clamp_(-8, 7).to(torch.int8)
 
 
+def guppi_header(nchan: int, npol: int, nsamp: int, obsfreq: float, obsbw: float, tbin: float,
+                 directio: int = 0, telescope: str = "GBT", chan_bw: float | None = None) -> bytes:
+    """A GUPPI RAW header: 80-byte "KEY     = value" cards ending with an END
+    card (BACKEND and OBSEND carry the two "END"s that precede it, so the
+    data start after the third, as the reference's reader expects).  The
+    reader puts the data right after the letters "END"; with DIRECTIO the
+    512-byte alignment covers the rest of the card, without it the card is
+    written as the bare "END"."""
+    chan_bw = obsbw / nchan if chan_bw is None else chan_bw
+
+    def card(k, v):
+        return f"{k:<8}= {v}".ljust(80)[:80]
+
+    cards = [card("BACKEND", "'GUPPI   '"), card("TELESCOP", f"'{telescope}'"),
+             card("OBS_MODE", "'RAW     '"), card("OBSFREQ", f"{obsfreq:.6f}"),
+             card("OBSBW", f"{obsbw:.6f}"), card("OBSNCHAN", f"{nchan}"), card("CHAN_BW", f"{chan_bw:.6f}"),
+             card("NPOL", f"{npol}"), card("NBITS", "8"), card("TBIN", f"{tbin:.12e}"),
+             card("BLOCSIZE", f"{nchan * npol * nsamp}"), card("DIRECTIO", f"{directio}"),
+             card("OBSEND", "0"), "END".ljust(80) if directio else "END"]
+    return "".join(cards).encode()
+
+
+def write_guppi(path, blocks: list[np.ndarray], obsfreq: float, obsbw: float, tbin: float,
+                directio: int = 0, telescope: str = "GBT", descending: bool = False) -> None:
+    """Writes int8 blocks [nchan][nsamp][npol] (ascending frequency) as a
+    GUPPI RAW file; with ``descending`` the channels are stored from the top
+    of the band down and CHAN_BW is negative."""
+    with open(path, "wb") as f:
+        for b in blocks:
+            nchan, nsamp, npol = b.shape
+            hdr = guppi_header(nchan, npol, nsamp, obsfreq, obsbw, tbin, directio, telescope,
+                               -obsbw / nchan if descending else None)
+            f.write(hdr)
+            if directio:
+                f.write(b"\0" * ((-len(hdr)) % 512))
+            data = (b[::-1] if descending else b).astype(np.int8).tobytes()
+            f.write(data)
+            if directio:
+                f.write(b"\0" * ((-len(data)) % 512))
+
+
 CONFIG0_SEARCH = dict(widths_mode=0, param=5, thr=7.0, metrics=(16, 8, 1 << 30))
 
 

@@ -313,6 +313,63 @@ bfs_status bfs_batch_beam_results(const bfs_batch* batch, int beam, bfs_cand* de
                                   uint32_t* n_candidates);
 
 /* ------------------------------------------------------------------------
+ * GUPPI RAW input (replaces CSession_guppi's file handling,
+ * L/CDMT/Session_guppi.cpp:31-85,111-283,336-369 and
+ * L/TelescopeHeader.cpp:88-124,175-347).  Header keys as the reference reads
+ * them (DIRECTIO, NBITS, CHAN_BW, OBSFREQ, OBSNCHAN, OBSBW, BLOCSIZE,
+ * TELESCOP, NPOL, TBIN; data after the third "END", 512-byte aligned with
+ * DIRECTIO).  8-bit samples.  Chunks are [nchan][len_chunk][npol] int8 in
+ * ascending frequency (a negative CHAN_BW reverses the stored order); chunk j
+ * of a block starts at sample j*(len_chunk - 2*noverlap), the last ends at
+ * the block's last sample (the reference's session loop; its rewind before
+ * the last chunk of a block is not reproduced).
+ * ---------------------------------------------------------------------- */
+enum { BFS_GUPPI_GBT = 0, BFS_GUPPI_PARKES = 1 };
+typedef struct bfs_guppi_header {
+    int nbits;
+    float chan_bw;        /* |CHAN_BW| (MHz)                                     */
+    int npol;             /* bytes per sample per channel at 8 bits (NPOL)       */
+    int directio;
+    float obsfreq;        /* |OBSFREQ| (MHz), band centre                        */
+    int nchan;            /* OBSNCHAN                                            */
+    float obsbw;          /* |OBSBW| (MHz)                                       */
+    int64_t blocsize;     /* data bytes of the block                             */
+    int telescope;        /* BFS_GUPPI_GBT / BFS_GUPPI_PARKES                    */
+    float tbin;           /* sample time (s)                                     */
+    int straight_order;   /* 1: ascending frequency in the file (CHAN_BW >= 0)   */
+    int64_t data_offset;  /* byte offset of the block's data                     */
+    int64_t nsamp;        /* samples per channel in the block                    */
+    float fmin, fmax;     /* obsfreq -/+ obsbw / 2                               */
+    int reserved[4];
+} bfs_guppi_header;
+typedef struct bfs_guppi_file bfs_guppi_file;
+typedef struct bfs_guppi_reader bfs_guppi_reader;
+
+/* Parses one header held in text[0..len) (data_offset relative to text). */
+bfs_status bfs_guppi_parse_header(const char* text, size_t len, bfs_guppi_header* out);
+/* Opens a file and indexes its blocks (CSession_guppi::calcQuantBlocks). */
+bfs_status bfs_guppi_open(const char* path, bfs_guppi_file** out);
+bfs_status bfs_guppi_close(bfs_guppi_file* file);
+bfs_status bfs_guppi_blocks(const bfs_guppi_file* file, int* nblocks);
+bfs_status bfs_guppi_block_header(const bfs_guppi_file* file, int block, bfs_guppi_header* out);
+bfs_status bfs_guppi_chunk_count(const bfs_guppi_file* file, int block, int64_t len_chunk,
+                                 int64_t noverlap, int64_t* nchunks);
+/* One chunk into host memory dst (CSession_guppi::download_chunk). */
+bfs_status bfs_guppi_read_chunk(const bfs_guppi_file* file, int block, int64_t chunk, int64_t len_chunk,
+                                int64_t noverlap, int8_t* dst, size_t dst_bytes);
+/* Streaming reader (no reference counterpart): a background thread reads
+ * every chunk of every block in order into `nbuffers` host buffers (pinned
+ * when `pinned`); _next hands out the next one and, given d_dst (device,
+ * chunk-sized), copies it there asynchronously on `stream`, so file reads,
+ * copies and the caller's kernels overlap.  *block = -1 at the end.  The
+ * host buffer (h_src) stays valid until the next call. */
+bfs_status bfs_guppi_reader_create(const bfs_guppi_file* file, int64_t len_chunk, int64_t noverlap,
+                                   int nbuffers, int pinned, bfs_guppi_reader** out);
+bfs_status bfs_guppi_reader_next(bfs_guppi_reader* reader, void* d_dst, void* stream,
+                                 const int8_t** h_src, int* block, int64_t* chunk);
+bfs_status bfs_guppi_reader_destroy(bfs_guppi_reader* reader);
+
+/* ------------------------------------------------------------------------
  * Coherent-dedispersion chunk stage.
  * Replaces CSession_guppi_gpu::unpack_chunk (L/CDMT/Session_guppi_gpu.cu:53-60,
  * 117-141) and CChunk_gpu / CChunk_fly_gpu::process (L/CDMT/Chunk_gpu.cu:134-460,

@@ -58,6 +58,33 @@ def ref_lib() -> ctypes.CDLL | None:
     return _ref
 
 
+_ref_guppi = None
+
+
+def ref_guppi_header(path, offset: int = 0) -> dict | None:
+    """The reference's CTelescopeHeader::readGuppiHeader on the block starting
+    at `offset` (None if oracle/_ref was not built; {'ok': False} if it
+    rejects the header)."""
+    global _ref_guppi
+    if _ref_guppi is None:
+        p = HERE / "_ref" / "libref_guppi.so"
+        if not p.exists():
+            return None
+        _ref_guppi = ctypes.CDLL(str(p))
+        _ref_guppi.ref_guppi_read_header.restype = ctypes.c_int
+    i = [ctypes.c_int(0) for _ in range(5)]
+    f = [ctypes.c_float(0) for _ in range(4)]
+    blk = ctypes.c_longlong(0)
+    pos = ctypes.c_long(0)
+    ok = _ref_guppi.ref_guppi_read_header(
+        str(path).encode(), ctypes.c_long(offset), ctypes.byref(i[0]), ctypes.byref(f[0]), ctypes.byref(i[1]),
+        ctypes.byref(i[2]), ctypes.byref(f[1]), ctypes.byref(i[3]), ctypes.byref(f[2]), ctypes.byref(blk),
+        ctypes.byref(i[4]), ctypes.byref(f[3]), ctypes.byref(pos))
+    return {"ok": ok == 1, "nbits": i[0].value, "chan_bw": f[0].value, "npol": i[1].value,
+            "directio": i[2].value, "obsfreq": f[1].value, "nchan": i[3].value, "obsbw": f[2].value,
+            "blocsize": blk.value, "telescope": i[4].value, "tbin": f[3].value, "data_pos": pos.value}
+
+
 _ref_pravir = None
 
 
