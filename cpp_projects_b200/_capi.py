@@ -113,6 +113,8 @@ _SIGNATURES = {
     "bfs_fdmt_adjoint_ws": (_I, [_P, _P, _P, _P, ctypes.c_size_t, _P]),
     "bfs_boxcar_snr_cells": (_I, [_P, _I, _I, _P, _P, _I, _P, _P]),
     "bfs_boxcar_snr_cells_adjoint": (_I, [_P, _I, _I, _P, _P, _I, _P, _P, _P, _P]),
+    "bfs_cut_fragment": (_I, [_P, _I, _I, _I, _I, _P, ctypes.POINTER(_I), ctypes.POINTER(_I),
+                              ctypes.POINTER(_I), _P]),
     "bfs_guppi_parse_header": (_I, [_P, ctypes.c_size_t, _P]),
     "bfs_guppi_open": (_I, [ctypes.c_char_p, ctypes.POINTER(_P)]),
     "bfs_guppi_close": (_I, [_P]),

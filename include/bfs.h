@@ -312,6 +312,16 @@ bfs_status bfs_batch_beam_results(const bfs_batch* batch, int beam, bfs_cand* de
                                   int* group_sizes, int cap, int* n_delegates,
                                   uint32_t* n_candidates);
 
+/* Square fragment of a DM-time plane around (target_row, target_col) for
+ * vetting (CChunkB::cutQuadraticFragment, L/CDMT/ChunkB.cpp:255-275, and
+ * CFragment, L/Fragment.h:3-28): dim = min(rows, cols); with rows < cols the
+ * rows x rows block from column (target_col / rows) * rows, else the
+ * cols x cols block at the top; read at the reference's flat row-major
+ * positions, 0 past the end of the plane.  d_out (device, dim*dim) may be
+ * null to get the geometry only. */
+bfs_status bfs_cut_fragment(const float* d_plane, int rows, int cols, int target_row, int target_col,
+                            float* d_out, int* row_begin, int* col_begin, int* dim, void* stream);
+
 /* ------------------------------------------------------------------------
  * GUPPI RAW input (replaces CSession_guppi's file handling,
  * L/CDMT/Session_guppi.cpp:31-85,111-283,336-369 and

@@ -5,6 +5,8 @@
 //
 //   CFdmtGpu                      L/FDMT/FdmtGpu.cuh:5-53
 //   FDMTGPU (Pravir plan)         L/FDMT_PRAVIR/fdmt_base.hpp:37-84, fdmt_gpu.cuh
+//   COutChunkHeader               L/OutChunkHeader.h, OutChunkHeader.cpp:89-227
+//   CFragment, cutQuadraticFragment  L/Fragment.h:3-28, L/CDMT/ChunkB.cpp:255-275
 //   statistical_preprocessing::   L/CDMT/Statistical_preprocessing.cuh:9-10
 //   clusterization::              L/Clusterization/Clusterization.cuh:10-67
 //   select_delegates::write_log   L/Clusterization/select_delegates.cu:127-177
@@ -137,6 +139,62 @@ private:
     float m_tsamp, m_f_min, m_f_max;
     std::vector<size_t> m_dt_grid;
 };
+
+// Candidate report line and writer (L/OutChunkHeader.h, OutChunkHeader.cpp:89-227).
+class COutChunkHeader {
+public:
+    COutChunkHeader() = default;
+    COutChunkHeader(int nrows, int ncols, int nSucessRow, int nSucessCol, int width, float SNR,
+                    float coherentDedisp, int numBlock, int numChunk)
+        : m_nrows(nrows), m_ncols(ncols), m_nSucessRow(nSucessRow), m_nSucessCol(nSucessCol),
+          m_SNR(SNR), m_coherentDedisp(coherentDedisp), m_numBlock(numBlock), m_numChunk(numChunk),
+          m_wnd_width(width) {}
+    int m_nrows = 0, m_ncols = 0, m_nSucessRow = 0, m_nSucessCol = 0;
+    float m_SNR = 0, m_coherentDedisp = 0;
+    int m_numBlock = 0, m_numChunk = 0, m_wnd_width = 0;
+
+    void createOutStr(char* pstr) const {
+        std::sprintf(pstr, "Block=  %d,Chunk=  %d,Rows=  %d,Cols=  %d, SucRow=  %d,SucCol=  %d, SNR=  %.4f, "
+                     "CohDisp=  %.4f, windWidth=  %d", m_numBlock + 1, m_numChunk + 1, m_nrows, m_ncols,
+                     m_nSucessRow, m_nSucessCol, m_SNR, m_coherentDedisp, m_wnd_width);
+    }
+    static void writeReport(const char* path, std::vector<COutChunkHeader>* headers, const float pulse_length) {
+        FILE* f = std::fopen(path, "wb");
+        if (!f) { std::printf("Can not open output file for writing"); return; }
+        for (const COutChunkHeader& h : *headers) {
+            char line[400] = {0};
+            h.createOutStr(line);
+            std::fprintf(f, "%s, Length of pulse= %.10e\n", line, pulse_length);
+        }
+        std::fclose(f);
+    }
+};
+
+// Square cut-out around a detection (L/Fragment.h:3-28) and the cut rule of
+// CChunkB::cutQuadraticFragment (L/CDMT/ChunkB.cpp:255-275) on a device plane.
+class CFragment {
+public:
+    CFragment() = default;
+    CFragment(const float* parr, int IDim, int NBeginRow, int NBeginCol, int NWidth, float VAlsnr, float cohDisp)
+        : m_nBeginRow(NBeginRow), m_nBeginCol(NBeginCol), m_dim(IDim),
+          m_vctData(parr, parr + static_cast<size_t>(IDim) * IDim), m_width(NWidth), m_snr(VAlsnr),
+          m_cohDisp(cohDisp) {}
+    int m_nBeginRow = 0, m_nBeginCol = 0, m_dim = 0;
+    std::vector<float> m_vctData = std::vector<float>(1);
+    int m_width = 0;
+    float m_snr = 0, m_cohDisp = 0;
+};
+
+// parrFragment: device buffer of min(rows, cols)^2 floats; parrInpImage: device plane.
+inline void cutQuadraticFragment(float* parrFragment, float* parrInpImage, int* piRowBegin, int* piColBegin,
+                                 const int QInpImageRows, const int QInpImageCols, const int NUmTargetRow,
+                                 const int NUmTargetCol) {
+    int dim = 0;
+    bfs_dropin_detail::report(bfs_cut_fragment(parrInpImage, QInpImageRows, QInpImageCols, NUmTargetRow,
+                                               NUmTargetCol, parrFragment, piRowBegin, piColBegin, &dim,
+                                               nullptr),
+                              "cutQuadraticFragment");
+}
 
 namespace statistical_preprocessing {
 inline void calc_fdmt_inputs(float* d_parr_inp, const int NRows, const int NCols, float* d_buff,

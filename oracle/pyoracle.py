@@ -58,6 +58,73 @@ def ref_lib() -> ctypes.CDLL | None:
     return _ref
 
 
+_ref_report = None
+
+
+def _report_lib():
+    global _ref_report
+    if _ref_report is None:
+        p = HERE / "_ref" / "libref_report.so"
+        if not p.exists():
+            return None
+        _ref_report = ctypes.CDLL(str(p))
+        _ref_report.ref_write_report.argtypes = [ctypes.c_char_p, ctypes.c_int, _P, _P, _P, _F]
+        _ref_report.ref_read_report_line.restype = ctypes.c_int
+        _ref_report.ref_read_report_line.argtypes = [ctypes.c_char_p, ctypes.c_int, _P, _P]
+    return _ref_report
+
+
+def ref_write_report(path, records, pulse_length) -> bool:
+    """The reference's COutChunkHeader::writeReport; records are tuples
+    (nrows, ncols, suc_row, suc_col, width, snr, cohdisp, block, chunk)."""
+    lib_ = _report_lib()
+    if lib_ is None:
+        return False
+    ints = np.zeros((max(len(records), 1), 9), np.int32)
+    snr = np.zeros(max(len(records), 1), np.float32)
+    coh = np.zeros(max(len(records), 1), np.float32)
+    for i, r in enumerate(records):
+        ints[i, :5] = r[:5]
+        snr[i], coh[i] = r[5], r[6]
+        ints[i, 5], ints[i, 6] = r[7], r[8]
+    lib_.ref_write_report(str(path).encode(), len(records), _ptr(ints), _ptr(snr), _ptr(coh), pulse_length)
+    return True
+
+
+def ref_read_report_line(path, line) -> dict | None:
+    lib_ = _report_lib()
+    if lib_ is None:
+        return None
+    ints = np.zeros(7, np.int32)
+    fl = np.zeros(2, np.float32)
+    if not lib_.ref_read_report_line(str(path).encode(), int(line), _ptr(ints), _ptr(fl)):
+        return {"ok": False}
+    return {"ok": True, "numBlock": int(ints[0]), "numChunk": int(ints[1]), "nrows": int(ints[2]),
+            "ncols": int(ints[3]), "sucRow": int(ints[4]), "sucCol": int(ints[5]), "width": int(ints[6]),
+            "cohDisp": float(fl[0]), "snr": float(fl[1])}
+
+
+def cut_quadratic_fragment(plane: np.ndarray, target_row: int, target_col: int):
+    """Restates CChunkB::cutQuadraticFragment (MyVSLib_C++/CDMT/ChunkB.cpp:
+    255-275) on the flat row-major plane; positions past its end read 0
+    (the reference's memcpy would read outside the array there)."""
+    rows, cols = plane.shape
+    flat = np.ascontiguousarray(plane, np.float32).reshape(-1)
+    if rows < cols:
+        d, cb, rb = rows, (target_col // rows) * rows, 0
+        start = cb
+    else:
+        part = target_row // rows
+        d, cb, rb = cols, 0, part
+        start = part * cols
+    out = np.zeros((d, d), np.float32)
+    for i in range(d):
+        a = i * cols + start
+        n = max(0, min(d, flat.size - a))
+        out[i, :n] = flat[a:a + n]
+    return out, rb, cb
+
+
 _ref_guppi = None
 
 

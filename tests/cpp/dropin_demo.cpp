@@ -9,6 +9,7 @@
 // (tsamp 1 ms, dt_max 64) on the same filterbank and checks that a size
 // mismatch throws std::invalid_argument.
 #include <cstdio>
+#include <string>
 #include <vector>
 
 #include "bfs_dropin.hpp"
@@ -66,6 +67,20 @@ int main(int argc, char** argv) {
     cudaMemcpy(d_metrics, metrics, sizeof(metrics), cudaMemcpyHostToDevice);
     const bool found = clusterization::clusterization_main(d_plane, rows, pc, *d_thr, 2, d_metrics,
                                                            argv[3], 0.00001f, 0.0f);
+    {
+        // a report line for the brightest cell and its square fragment
+        std::vector<COutChunkHeader> hdrs{COutChunkHeader(rows, pc, 0, 4, 1, 140.0f, 56.8f, 0, 0)};
+        COutChunkHeader::writeReport((std::string(argv[3]) + ".report").c_str(), &hdrs, 1.25e-3f);
+        float* d_frag = nullptr;
+        cudaMalloc(reinterpret_cast<void**>(&d_frag), rows * rows * sizeof(float));
+        int rb = -1, cb = -1;
+        cutQuadraticFragment(d_frag, d_plane, &rb, &cb, rows, pc, 0, 4);
+        std::vector<float> frag(rows * rows);
+        cudaMemcpy(frag.data(), d_frag, frag.size() * sizeof(float), cudaMemcpyDeviceToHost);
+        cudaFree(d_frag);
+        const CFragment fr(frag.data(), rows, rb, cb, 1, 140.0f, 56.8f);
+        if (fr.m_nBeginCol != 3 || fr.m_vctData[1] != 140.0f) return 7;
+    }
     cudaFree(d_in); cudaFree(d_out); cudaFree(d_plane); cudaFree(d_thr); cudaFree(d_metrics);
     return found ? 0 : 5;
 }

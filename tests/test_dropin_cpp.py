@@ -45,6 +45,10 @@ def test_dropin_driver_runs_and_matches(cuda, tmp_path):
     pr = np.fromfile(tmp_path / "pravir.bin", np.float32).reshape(-1, 1024)
     pwant = pyoracle.pravir_fdmt(1200.0, 1600.0, x, 64, 1024, 64)
     assert pr.shape == pwant.shape and np.array_equal(pr.view(np.uint32), pwant.view(np.uint32))
+    from cpp_projects_b200 import reports
+    want_rep = tmp_path / "want.report"
+    reports.write_report(want_rep, [reports.COutChunkHeader(3, 16, 0, 4, 1, 140.0, 56.8, 0, 0)], 1.25e-3)
+    assert (tmp_path / "ouput.log.report").read_bytes() == want_rep.read_bytes()
     body = [ln.split() for ln in (tmp_path / "ouput.log").read_text().splitlines()[1:]]
     assert body == [["1", "4", "4e-05", "0", "1", "140", "3"],
                     ["2", "4", "4e-05", "2", "1", "100", "3"],
