@@ -108,6 +108,7 @@ _SIGNATURES = {
     "bfs_select_delegates": (_I, [_P, _P, _U32, _P, _U32, _P, _P]),
     "bfs_cluster_grouped": (_I, [_P, _U32, _P, _U32, _P, _P, _P, _P, ctypes.POINTER(_U32), _P]),
     "bfs_fdmt_plan_delays": (_I, [_P, _P, _I, _P, _P, _I]),
+    "bfs_fdmt_execute_row_mask": (_I, [_P, _P, _I, _P, _P]),
     "bfs_fdmt_adjoint": (_I, [_P, _P, _P, _P]),
     "bfs_fdmt_adjoint_workspace_size": (_I, [_P, ctypes.POINTER(ctypes.c_size_t)]),
     "bfs_fdmt_adjoint_ws": (_I, [_P, _P, _P, _P, ctypes.c_size_t, _P]),

@@ -322,7 +322,9 @@ extern "C" bfs_status bfs_chunk_process(bfs_chunk* c, void* d_cplx, const double
         if (st != BFS_OK) return st;
         st = bfs_preproc_calc_fdmt_inputs(c->plane, c->rows, c->msamp, c->buff, c->mask, stream);
         if (st != BFS_OK) return st;
-        st = bfs_fdmt_execute(c->fdmt, c->mask, c->norm, 0, stream);
+        // FDMT of the mask: its rows are all 0 or all 1 (calc_fdmt_inputs zaps
+        // whole rows), so the channel-count form gives the same bits in one pass
+        st = bfs_fdmt_execute_row_mask(c->fdmt, c->mask, c->msamp, c->norm, stream);
         if (st != BFS_OK) return st;
         float* out = d_out + i * plane_out;
         st = bfs_fdmt_execute(c->fdmt, c->plane, out, 0, stream);

@@ -233,6 +233,52 @@ cudaError_t launch_init(const float* d_in, D* dst, const FdmtPlanHost& h, int P,
     return cudaGetLastError();
 }
 
+// FDMT of 0/1 rows (b_ones mode, or a plane whose row c is all w_c in {0,1}):
+// output row d at sample t is exactly the number of channels c with w_c != 0
+// and tau(d, c) <= t (the level-0 means of a 0/1 row are exactly 0 or 1 and
+// every merge adds integers, so the level-by-level FDMT gives the same
+// bits).  One CTA per output row: a shared histogram of tau over the row's
+// channels (integer counts, exact in FP32), its inclusive prefix sum, then
+// the row written once.  L = max tau + 1 histogram entries.
+constexpr int kOnesThreads = 256;
+
+__global__ void __launch_bounds__(kOnesThreads)
+k_fdmt_ones(float* __restrict__ out, int out_pitch, const int* __restrict__ tau,
+            const float* __restrict__ w, int w_stride, int nchan, int ncols, int L) {
+    extern __shared__ float hist[];
+    const int d = blockIdx.x;
+    for (int i = threadIdx.x; i < L; i += blockDim.x) hist[i] = 0.0f;
+    __syncthreads();
+    const int* tr = tau + static_cast<size_t>(d) * nchan;
+    for (int c = threadIdx.x; c < nchan; c += blockDim.x) {
+        const bool on = w ? (__ldg(w + static_cast<size_t>(c) * w_stride) != 0.0f) : true;
+        if (on) atomicAdd(&hist[__ldg(tr + c)], 1.0f);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {  // inclusive scan by one warp: a segment per lane
+        const int lane = threadIdx.x;
+        const int seg = (L + 31) / 32;
+        const int b0 = min(L, lane * seg), b1 = min(L, b0 + seg);
+        float sum = 0.0f;
+        for (int i = b0; i < b1; ++i) sum += hist[i];
+        float pre = sum;  // inclusive scan of the segment totals
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const float v = __shfl_up_sync(0xffffffffu, pre, o);
+            if (lane >= o) pre += v;
+        }
+        float run = pre - sum;
+        for (int i = b0; i < b1; ++i) {
+            run += hist[i];
+            hist[i] = run;
+        }
+    }
+    __syncthreads();
+    float* o = out + static_cast<size_t>(d) * out_pitch;
+    const float last = hist[L - 1];
+    for (int t = threadIdx.x; t < ncols; t += blockDim.x) o[t] = t < L ? hist[t] : last;
+}
+
 // One merge level.  The input plane is always a workspace plane (128-byte
 // row pitch), so the tail row moves as float4; the shifted head row moves as
 // 4 scalar loads (its alignment depends on the row's shift); the output is
@@ -1022,6 +1068,36 @@ extern "C" bfs_status bfs_fdmt_workspace_size(const bfs_fdmt_plan* plan, size_t*
     return BFS_OK;
 }
 
+constexpr int kOnesMaxHist = 12 * 1024;  // shared-memory histogram entries (48 KB)
+
+// Uploads the plan's delay table for 0/1 rows on first use; false when the
+// fast path does not apply (histogram too long).
+static bfs_status ensure_ones(bfs_fdmt_plan* plan, bool* usable) {
+    *usable = false;
+    if (plan->ones_max_tau < 0) {
+        std::vector<int> tau;
+        int mx = 0;
+        build_ones_delays(plan->host, &tau, &mx);
+        plan->ones_max_tau = mx;
+        if (mx + 1 <= kOnesMaxHist) {
+            BFS_CUDA(cudaMalloc(&plan->d_ones_tau, tau.size() * sizeof(int)));
+            BFS_CUDA(cudaMemcpy(plan->d_ones_tau, tau.data(), tau.size() * sizeof(int), cudaMemcpyHostToDevice));
+        }
+    }
+    *usable = plan->d_ones_tau != nullptr;
+    return BFS_OK;
+}
+
+static bfs_status launch_ones(bfs_fdmt_plan* plan, const float* d_w, int w_stride, float* d_out,
+                              cudaStream_t s) {
+    const FdmtPlanHost& h = plan->host;
+    const int L = plan->ones_max_tau + 1;
+    k_fdmt_ones<<<h.out_rows(), kOnesThreads, L * sizeof(float), s>>>(d_out, h.ncols, plan->d_ones_tau, d_w,
+                                                                      w_stride, h.nchan, h.ncols, L);
+    BFS_LAUNCH_CHECK("k_fdmt_ones");
+    return BFS_OK;
+}
+
 // The same schedule over 16-bit planes (storage type S).
 template <typename S>
 static bfs_status fdmt_run16(bfs_fdmt_plan* plan, const float* d_in, float* d_out, int b_ones,
@@ -1065,6 +1141,12 @@ static bfs_status fdmt_run(bfs_fdmt_plan* plan, const float* d_in, float* d_out,
     if (plan->precision == BFS_PREC_BF16)
         return fdmt_run16<__nv_bfloat16>(plan, d_in, d_out, b_ones, static_cast<__nv_bfloat16*>(buf0_),
                                          static_cast<__nv_bfloat16*>(buf1_), s);
+    if (b_ones) {
+        bool usable = false;
+        bfs_status st = ensure_ones(plan, &usable);
+        if (st != BFS_OK) return st;
+        if (usable) return launch_ones(plan, nullptr, 0, d_out, s);
+    }
     float* buf0 = static_cast<float*>(buf0_);
     float* buf1 = static_cast<float*>(buf1_);
     const FdmtPlanHost& h = plan->host;
@@ -1115,6 +1197,18 @@ extern "C" bfs_status bfs_fdmt_execute_ws(bfs_fdmt_plan* plan, const float* d_in
     BFS_ARG((reinterpret_cast<uintptr_t>(d_workspace) & 255) == 0, "workspace must be 256-byte aligned");
     char* w = static_cast<char*>(d_workspace);
     return fdmt_run(plan, d_in, d_out, b_ones, w, w + plane_bytes(plan, 0), as_stream(stream));
+}
+
+extern "C" bfs_status bfs_fdmt_execute_row_mask(bfs_fdmt_plan* plan, const float* d_mask, int mask_pitch,
+                                                float* d_out, void* stream) {
+    BFS_ARG(plan != nullptr && d_mask != nullptr && d_out != nullptr, "null argument");
+    BFS_ARG(!plan->host_only, "plan was created with bfs_fdmt_plan_create_host");
+    BFS_ARG(plan->precision == BFS_PREC_F32, "the row-mask FDMT is implemented for FP32 plans");
+    bool usable = false;
+    bfs_status st = ensure_ones(plan, &usable);
+    if (st != BFS_OK) return st;
+    BFS_ARG(usable, "the plan's delays exceed the row-mask histogram (%d)", kOnesMaxHist);
+    return launch_ones(plan, d_mask, mask_pitch, d_out, as_stream(stream));
 }
 
 // ---------------------------------------------------------------------------

@@ -23,6 +23,8 @@ struct bfs_fdmt_plan {
     bfs::HeadGroup* d_head_groups = nullptr;
     int* d_head_tab = nullptr;
     int* d_lvl0 = nullptr;             // Pravir plans: level-0 row cumsum (nchan+1) then delays
+    int* d_ones_tau = nullptr;         // FDMT of 0/1 rows: tau [out_row][channel] (first use)
+    int ones_max_tau = -1;
     // adjoint (built on the first adjoint call): per level l >= 1, for every
     // row of level l-1 the level-l rows that read it, as CSR {row, shift}
     bfs::AdjointTables adj;
@@ -34,6 +36,7 @@ struct bfs_fdmt_plan {
         if (d_head_groups) cudaFree(d_head_groups);
         if (d_head_tab) cudaFree(d_head_tab);
         if (d_lvl0) cudaFree(d_lvl0);
+        if (d_ones_tau) cudaFree(d_ones_tau);
         for (void* b : d_buf)
             if (b) cudaFree(b);
         if (d_adj_off) cudaFree(d_adj_off);

@@ -92,6 +92,13 @@ struct AdjointTables {
 };
 void build_adjoint_tables(const FdmtPlanHost& p, AdjointTables* out);
 
+// FDMT of 0/1 rows: every level-0 value of a 0/1 row is exactly 0 or 1 and
+// every merge adds integers, so output row d at sample t is exactly the
+// number of channels c with weight 1 whose total delay along the merge tree,
+// tau(d, c) (the level-0 row plus every head shift on the path), is <= t.
+// tau is row-major [out_row][channel]; max_tau its largest value.
+void build_ones_delays(const FdmtPlanHost& p, std::vector<int>* tau, int* max_tau);
+
 // ---------------------------------------------------------------------------
 // Fused "head" of the FDMT: levels 0..k of one group of 2^k adjacent channels
 // computed by one CTA over a time tile, all intermediate levels in shared

@@ -406,4 +406,39 @@ bfs_status build_pravir_plan(float fmin, float fmax, int nchan, int ncols, int d
     return BFS_OK;
 }
 
+void build_ones_delays(const FdmtPlanHost& p, std::vector<int>* tau, int* max_tau) {
+    // channel and delay of every level-0 row
+    const int r0 = p.lv[0].total_rows();
+    std::vector<int> chan(r0), delay(r0);
+    for (int c = 0; c < p.nchan; ++c)
+        for (int r = p.lv[0].cum[c]; r < p.lv[0].cum[c + 1]; ++r) {
+            chan[r] = c;
+            delay[r] = p.kind == BFS_PLAN_PRAVIR ? p.dt0[r] : r - p.lv[0].cum[c];
+        }
+    const int nout = p.out_rows();
+    tau->assign(static_cast<size_t>(nout) * p.nchan, 0);
+    *max_tau = 0;
+    // depth-first walk from every output row down to its level-0 rows
+    struct Node { int level, row, acc; };
+    std::vector<Node> stack;
+    for (int d = 0; d < nout; ++d) {
+        int* t = tau->data() + static_cast<size_t>(d) * p.nchan;
+        stack.clear();
+        stack.push_back({p.niter, d, 0});
+        while (!stack.empty()) {
+            const Node n = stack.back();
+            stack.pop_back();
+            if (n.level == 0) {
+                const int v = n.acc + delay[n.row];
+                t[chan[n.row]] = v;
+                *max_tau = std::max(*max_tau, v);
+                continue;
+            }
+            const FdmtLevel& L = p.lv[n.level];
+            stack.push_back({n.level - 1, L.a_row[n.row], n.acc});
+            if (L.b_row[n.row] >= 0) stack.push_back({n.level - 1, L.b_row[n.row], n.acc + L.shift[n.row]});
+        }
+    }
+}
+
 }  // namespace bfs

@@ -140,6 +140,16 @@ bfs_status bfs_fdmt_workspace_size(const bfs_fdmt_plan* plan, size_t* bytes);
 bfs_status bfs_fdmt_execute_ws(bfs_fdmt_plan* plan, const float* d_in, float* d_out, int b_ones,
                                void* d_workspace, size_t workspace_bytes, void* stream);
 
+/* FDMT of a plane whose row c is all 1 where d_mask[c * mask_pitch] != 0 and
+ * all 0 elsewhere (a row mask such as calc_fdmt_inputs' zapping mask): the
+ * output is exactly what bfs_fdmt_execute gives on that plane (b_ones mode
+ * is the all-1 case and uses the same path) — every value is an integer
+ * count of channels, formed from the plan's per-channel delays in one pass
+ * over the output instead of the level-by-level transform.  FP32 plans; the
+ * first call uploads the delay table (allocates, synchronous). */
+bfs_status bfs_fdmt_execute_row_mask(bfs_fdmt_plan* plan, const float* d_mask, int mask_pitch,
+                                     float* d_out, void* stream);
+
 /* Allocation-free FDMT.  No counterpart in the reference: it exists for
  * callers that cannot allocate device memory where they run the transform
  * (a real-time receiver whose GPU memory is all reserved at start-up, a

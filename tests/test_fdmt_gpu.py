@@ -110,3 +110,35 @@ def test_fdmt_rejects_bad_sizes(cuda):
     f = CFdmtGpu(1200.0, 1600.0, 64, 128, 64)
     with pytest.raises(ValueError):
         f.process_image(torch.zeros(10, device=cuda), torch.zeros((64, 128), device=cuda))
+
+
+@pytest.mark.parametrize("case", CASES[:5] + CASES[7:])
+@pytest.mark.parametrize("kind", ["keith", "pravir"])
+def test_row_mask_fdmt_equals_the_transform(cuda, case, kind):
+    """The channel-count form of the FDMT of a 0/1 row mask gives exactly the
+    level-by-level transform of that plane (and b_ones is its all-1 case)."""
+    import ctypes
+    from cpp_projects_b200 import FDMTGPU, _capi
+    from cpp_projects_b200._tensors import dev_ptr
+    fmin, fmax, nchan, ncols, max_dt = case
+    if kind == "pravir":
+        if ncols <= max_dt:
+            pytest.skip("Pravir plans need offsets below ncols")
+        f = FDMTGPU(fmin, fmax, nchan, ncols, 1e-3, max_dt)
+        rows = f.out_rows
+    else:
+        f = CFdmtGpu(fmin, fmax, nchan, ncols, max_dt, fuse_depth=0)
+        rows = max_dt
+    m = (np.random.default_rng(nchan).random(nchan) > 0.2).astype(np.float32)
+    plane = torch.from_numpy(np.repeat(m[:, None], ncols, 1)).to(cuda)
+    want = torch.empty((rows, ncols), device=cuda)
+    _capi.call("bfs_fdmt_execute", f._plan, dev_ptr(plane), dev_ptr(want), 0, None)
+    got = torch.full((rows, ncols), float("nan"), device=cuda)
+    _capi.call("bfs_fdmt_execute_row_mask", f._plan, dev_ptr(plane), ncols, dev_ptr(got), None)
+    assert torch.equal(got, want)
+    if kind == "keith":
+        ones = torch.full((rows, ncols), float("nan"), device=cuda)
+        f.process_image(None, ones, True)
+        oracle_ones = pyoracle.fdmt_f32(fmin, fmax, None, nchan, ncols, max_dt, b_ones=True)
+        assert np.array_equal(ones.cpu().numpy(), oracle_ones)
+
