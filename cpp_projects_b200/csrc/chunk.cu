@@ -113,30 +113,39 @@ __global__ void k_chirp(const float2* __restrict__ in, float2* __restrict__ out,
 // Power detection + roll by nbin/2 + unpadding + frequency reversal +
 // dedispersion shift, as one gather: output row r (fine channel, highest
 // frequency first), column c of the dedispersed plane.
-__global__ void k_detect(const float2* __restrict__ volt, float* __restrict__ plane, int nchan,
-                         int len_sft, int mbin, int nbin, int nfft, int npol2, int nov_pc,
-                         int mbin_adj, int msamp, const int* __restrict__ shift) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= msamp) return;
+__global__ void __launch_bounds__(256)
+k_detect(const float2* __restrict__ volt, float* __restrict__ plane, int nchan, int len_sft, int mbin,
+         int nbin, int nfft, int npol2, int nov_pc, int mbin_adj, int msamp, const int* __restrict__ shift,
+         double inv_nbin2) {
     const int r = blockIdx.y;
-    int idx = (c - shift[r]) % msamp;     // dedisperse: out[(idx + s) % msamp] = in[idx]
+    const int c0 = blockIdx.x * blockDim.x;
+    if (c0 + static_cast<int>(threadIdx.x) >= msamp) return;
+    // the CTA's first column, then this thread's by single-step carries
+    // (msamp, mbin_adj and nbin wrap at most once over a CTA's span when they
+    // are >= the CTA width; smaller ones are reduced by a short loop)
+    int idx = (c0 - __ldg(shift + r)) % msamp;  // dedisperse: out[(idx + s) % msamp] = in[idx]
     if (idx < 0) idx += msamp;
+    idx += threadIdx.x;
+    while (idx >= msamp) idx -= msamp;
     const int isub = r / len_sft;
     const int ifine = len_sft - 1 - (r % len_sft);
     const int coarse = nchan - 1 - isub;
-    const int ifft = idx / mbin_adj;
-    const int ibin = idx % mbin_adj;
-    const int p = ifine * mbin + ibin + nov_pc;          // position in the rolled row
-    const int q = (p + nbin / 2) % nbin;                 // position before the roll
+    int ifft = idx / mbin_adj;
+    const int ibin = idx - ifft * mbin_adj;
+    int q = ifine * mbin + ibin + nov_pc + nbin / 2;     // position before the roll
+    if (q >= nbin) q -= nbin;
     const size_t pol_stride = static_cast<size_t>(nfft) * nchan * nbin;
     const size_t base = (static_cast<size_t>(ifft) * nchan + coarse) * nbin + q;
     float acc = 0.0f;
     for (int ipol = 0; ipol < npol2; ++ipol) {
-        const float2 v = volt[base + ipol * pol_stride];
+        const float2 v = __ldg(volt + base + ipol * pol_stride);
         const double x = v.x, y = v.y;
-        acc = __fadd_rn(acc, static_cast<float>((x * x + y * y) / nbin / nbin));
+        // |v|^2 / nbin / nbin in FP64 (the reference's roll kernel); with nbin a
+        // power of two the two divides are an exact scaling by 2^-2k
+        const double pw = inv_nbin2 > 0.0 ? (x * x + y * y) * inv_nbin2 : (x * x + y * y) / nbin / nbin;
+        acc = __fadd_rn(acc, static_cast<float>(pw));
     }
-    plane[static_cast<size_t>(r) * msamp + c] = acc;
+    plane[static_cast<size_t>(r) * msamp + c0 + threadIdx.x] = acc;
 }
 
 bfs_status cufft_check(cufftResult r, const char* what) {
@@ -294,8 +303,10 @@ static bfs_status chunk_detect(bfs_chunk* c, const float2* d_volt, double dm, fl
     const bfs_chunk_desc& d = c->d;
     dim3 grid((c->msamp + 255) / 256, c->rows);
     BFS_ARG(grid.y <= 65535, "too many fine channels");
+    const bool pow2 = (d.nbin & (d.nbin - 1)) == 0;
+    const double inv_nbin2 = pow2 ? 1.0 / (static_cast<double>(d.nbin) * d.nbin) : 0.0;  // exact for 2^k
     k_detect<<<grid, 256, 0, s>>>(d_volt, d_plane, d.nchan, d.len_sft, c->mbin, d.nbin, d.nfft,
-                                  d.npol / 2, c->nov_pc, c->mbin_adj, c->msamp, c->d_shift);
+                                  d.npol / 2, c->nov_pc, c->mbin_adj, c->msamp, c->d_shift, inv_nbin2);
     BFS_LAUNCH_CHECK("k_detect");
     // the host vector must outlive the (pageable, staged) copy: wait for it
     BFS_CUDA(cudaStreamSynchronize(s));
