@@ -96,6 +96,7 @@ _SIGNATURES = {
     "bfs_fdmt_workspace_size": (_I, [_P, ctypes.POINTER(ctypes.c_size_t)]),
     "bfs_fdmt_execute_ws": (_I, [_P, _P, _P, _I, _P, ctypes.c_size_t, _P]),
     "bfs_fdmt_execute_noalloc": (_I, [_P, _P, _P, _I, _P]),
+    "bfs_selftest_divide": (_I, [_I, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint32), _P]),
     "bfs_fdmt_noalloc_scratch_bytes": (_I, [_P, ctypes.POINTER(ctypes.c_size_t),
                                             ctypes.POINTER(ctypes.c_size_t)]),
     "bfs_preproc_calc_fdmt_inputs": (_I, [_P, _I, _I, _P, _P, _P]),

@@ -36,8 +36,8 @@
 #include <mutex>
 #include <tuple>
 
+#include "divide.cuh"
 #include "internal.h"
-
 #include "fdmt_plan.h"
 
 namespace bfs {
@@ -153,8 +153,7 @@ k_fdmt_init4(const float* __restrict__ x, D* __restrict__ out, int ncols, int ou
         for (int j = 0; j < 4; ++j) {
             w[j] = 0.0f;
             if (t + j >= r) {
-                v[j] = __fdiv_rn(__fadd_rn(__fmul_rn(v[j], static_cast<float>(r)), xs[4 + j - r]),
-                                 static_cast<float>(r + 1));
+                v[j] = div_small(__fadd_rn(__fmul_rn(v[j], static_cast<float>(r)), xs[4 + j - r]), r + 1);
                 w[j] = v[j];
             }
         }
@@ -505,8 +504,7 @@ __device__ __forceinline__ void head_level0(const float* __restrict__ x, float* 
                 float w = 0.0f;
                 if (t >= r) {
                     const float xr = u >= r ? sx[-r] : 0.0f;
-                    v = __fdiv_rn(__fadd_rn(__fmul_rn(v, static_cast<float>(r)), xr),
-                                  static_cast<float>(r + 1));
+                    v = div_small(__fadd_rn(__fmul_rn(v, static_cast<float>(r)), xr), r + 1);
                     w = v;
                 }
                 dst[r * W] = w;

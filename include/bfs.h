@@ -445,6 +445,16 @@ bfs_status bfs_chunk_detect(bfs_chunk* chunk, const void* d_volt, double dm, flo
 bfs_status bfs_chunk_process(bfs_chunk* chunk, void* d_cplx, const double* dms, int ndm,
                              float* d_out, void* stream);
 
+/* ---- self-tests (no reference counterpart) ---- */
+
+/* Compares the level-0 kernels' division by the constant d (a multiply and a
+ * fused multiply-add for d = 2..8, __fdiv_rn otherwise) with __fdiv_rn(x, d)
+ * for all 2^32 float bit patterns x on the current device; *mismatches = how
+ * many differ (0 means the FDMT's level 0 is bit-exact for that divisor),
+ * *first_bad (may be NULL) = the lowest differing bit pattern.  Synchronises
+ * `stream`. */
+bfs_status bfs_selftest_divide(int d, uint64_t* mismatches, uint32_t* first_bad, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,6 +58,37 @@ def test_fdmt_autotuned_and_wide_tiles_bit_exact(cuda, case, fuse, tile):
     assert np.array_equal(_bits(d_out.cpu().numpy()), _bits(want))
 
 
+@pytest.mark.parametrize("d", range(2, 9))
+def test_level0_constant_division_matches_ieee_divide_for_every_float(cuda, d):
+    """The level-0 running means divide by r + 1 with a multiply / fused
+    multiply-add split; all 2^32 bit patterns must give __fdiv_rn's bits."""
+    import ctypes
+    from cpp_projects_b200 import _capi
+    bad, first = ctypes.c_uint64(), ctypes.c_uint32()
+    _capi.call("bfs_selftest_divide", d, ctypes.byref(bad), ctypes.byref(first), None)
+    assert bad.value == 0, f"d={d}: {bad.value} mismatches, first bits {first.value:#010x}"
+
+
+@pytest.mark.parametrize("shape", [(64, 2048, 64), (64, 2048, 96), (64, 2048, 128)])
+@pytest.mark.parametrize("fuse", [0, -1])
+def test_fdmt_bit_exact_on_special_values(cuda, shape, fuse):
+    """Signed zeros, subnormals, tiny and huge magnitudes reach the level-0
+    divisions on both sides of the split-division guard (|x| >= 2^-64)."""
+    nchan, ncols, max_dt = shape
+    rng = np.random.default_rng(13)
+    x = rng.standard_normal((nchan, ncols)).astype(np.float32)
+    specials = np.array([0.0, -0.0, 1e-40, -1e-40, 1e-30, -1e-30, 2.0 ** -64, -(2.0 ** -65),
+                         1e-20, 1e30, -1e30, 3.0e38 / 256], np.float32)
+    idx = rng.integers(0, x.size, size=x.size // 4)
+    x.reshape(-1)[idx] = specials[rng.integers(0, specials.size, size=idx.size)]
+    x[:, :64] = -0.0  # whole runs of negative zeros: -0 sums stay -0
+    f = CFdmtGpu(1200.0, 1600.0, nchan, ncols, max_dt, fuse_depth=fuse)
+    d_out = torch.full((max_dt, ncols), float("nan"), device=cuda)
+    f.process_image(torch.from_numpy(x).to(cuda), d_out, False)
+    want = pyoracle.fdmt_f32(1200.0, 1600.0, x, nchan, ncols, max_dt)
+    assert np.array_equal(_bits(d_out.cpu().numpy()), _bits(want))
+
+
 def test_autotune_returns_a_valid_choice(cuda):
     from cpp_projects_b200.fdmt import autotune
     depth, tile, ms = autotune(1200.0, 1600.0, 1024, 65536, 1024)
