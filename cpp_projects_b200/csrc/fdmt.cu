@@ -504,7 +504,9 @@ __device__ __forceinline__ void head_level0(const float* __restrict__ x, float* 
                 float w = 0.0f;
                 if (t >= r) {
                     const float xr = u >= r ? sx[-r] : 0.0f;
-                    v = div_small(__fadd_rn(__fmul_rn(v, static_cast<float>(r)), xr), r + 1);
+                    // v * 1 is v: the first step needs no multiply
+                    const float m = r == 1 ? v : __fmul_rn(v, static_cast<float>(r));
+                    v = div_small(__fadd_rn(m, xr), r + 1);
                     w = v;
                 }
                 dst[r * W] = w;
@@ -525,14 +527,19 @@ __device__ __forceinline__ void head_level0(const float* __restrict__ x, float* 
     }
 }
 
-__device__ __forceinline__ float head_merge(const float* __restrict__ src, int4 e, int u, int t, int W) {
-    const float a = src[e.x * W + u];
-    const float b = src[e.y * W + max(u - e.z, 0)];
-    return (t >= e.z && u >= e.z) ? __fadd_rn(a, b) : a;
+// One merge row of the head, from its staged entry {a, b, thr, d}: a = byte
+// offset of the tail row in the source buffer, b = byte offset of the head
+// row minus the shift (so b + 4u addresses sample u - shift), thr = the first
+// local column that adds the head row (shift, raised by the samples t < 0 in
+// the first tile), d = the destination offset.  `sb` = source buffer + u.
+__device__ __forceinline__ float head_merge(const char* __restrict__ sb, int4 e, int u) {
+    float a = *reinterpret_cast<const float*>(sb + e.x);
+    if (u >= e.z) a = __fadd_rn(a, *reinterpret_cast<const float*>(sb + e.y));
+    return a;
 }
 
 template <int R0C, typename D>
-__global__ void __launch_bounds__(1024)
+__global__ void __launch_bounds__(1024, 1)
 k_fdmt_head(const float* __restrict__ x, D* __restrict__ out,
             const HeadGroup* __restrict__ groups, const int4* __restrict__ tab, int ncols,
             int out_pitch, int depth, int group, int rows_per_chan, int tile, int rows_a,
@@ -544,15 +551,30 @@ k_fdmt_head(const float* __restrict__ x, D* __restrict__ out,
     const int u = threadIdx.x;
     const HeadGroup* hg = groups + blockIdx.y;
     const int halo = __ldg(&hg->halo);
-    const int t = blockIdx.x * tile - halo + u;
+    const int t0 = blockIdx.x * tile - halo;  // sample of local column 0
+    const int t = t0 + u;
     float* bufa = sm;
     float* bufb = sm + rows_a * W;
     int4* stab = reinterpret_cast<int4*>(sm + (rows_a + rows_b) * W);
 
-    // stage this group's tables (levels 1..depth are contiguous)
+    // stage this group's tables (levels 1..depth are contiguous) as offsets:
+    // t >= shift and u >= shift  <=>  u >= shift + max(0, -t0)
     const int tab0 = __ldg(&hg->tab_off[1]);
-    const int ntab = __ldg(&hg->tab_off[depth]) + __ldg(&hg->rows[depth]) - tab0;
-    for (int i = u; i < ntab; i += W) stab[i] = __ldg(tab + tab0 + i);
+    const int last0 = __ldg(&hg->tab_off[depth]) - tab0;
+    const int ntab = last0 + __ldg(&hg->rows[depth]);
+    const int neg0 = max(0, -t0);
+    for (int i = u; i < ntab; i += W) {
+        const int4 e = __ldg(tab + tab0 + i);
+        int l = 1;
+        while (l < depth && i >= __ldg(&hg->tab_off[l + 1]) - tab0) ++l;
+        const int j = i - (__ldg(&hg->tab_off[l]) - tab0);  // row within its level
+        int4 f;
+        f.x = e.x * W * 4;
+        f.y = (e.y * W - e.z) * 4;
+        f.z = e.z + neg0;
+        f.w = l < depth ? j * W * 4 : j;
+        stab[i] = f;
+    }
 
     head_level0<R0C>(x, bufa, bufb, blockIdx.y * group, group, rows_per_chan, ncols, t, u, W, ones);
     __syncthreads();
@@ -560,22 +582,24 @@ k_fdmt_head(const float* __restrict__ x, D* __restrict__ out,
     float* src = bufa;
     float* dst = bufb;
     const bool writer = (u >= halo) && (u < halo + tile) && (t < ncols);
+    const int4* tb = stab;
     for (int l = 1; l <= depth; ++l) {
         const int rows = __ldg(&hg->rows[l]);
-        const int4* tb = stab + (__ldg(&hg->tab_off[l]) - tab0);
+        const char* sb = reinterpret_cast<const char*>(src + u);
         if (l < depth) {
+            char* db = reinterpret_cast<char*>(dst + u);
             int j = 0;
             for (; j + 4 <= rows; j += 4) {
-                const float v0 = head_merge(src, tb[j], u, t, W);
-                const float v1 = head_merge(src, tb[j + 1], u, t, W);
-                const float v2 = head_merge(src, tb[j + 2], u, t, W);
-                const float v3 = head_merge(src, tb[j + 3], u, t, W);
-                dst[j * W + u] = v0;
-                dst[(j + 1) * W + u] = v1;
-                dst[(j + 2) * W + u] = v2;
-                dst[(j + 3) * W + u] = v3;
+                float v[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) v[k] = head_merge(sb, tb[j + k], u);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) *reinterpret_cast<float*>(db + tb[j + k].w) = v[k];
             }
-            for (; j < rows; ++j) dst[j * W + u] = head_merge(src, tb[j], u, t, W);
+            for (; j < rows; ++j) {
+                const int4 e = tb[j];
+                *reinterpret_cast<float*>(db + e.w) = head_merge(sb, e, u);
+            }
             __syncthreads();
             float* tmp = src; src = dst; dst = tmp;
         } else {
@@ -584,24 +608,15 @@ k_fdmt_head(const float* __restrict__ x, D* __restrict__ out,
                 if constexpr (sizeof(D) == 4) o[static_cast<size_t>(row) * out_pitch] = from_f32<D>(v);
                 else o[static_cast<size_t>(row) * out_pitch] = from_f32<D>(__fmul_rn(v, oscale));
             };
-            int j = 0;
-            for (; j + 4 <= rows; j += 4) {
-                const float v0 = head_merge(src, tb[j], u, t, W);
-                const float v1 = head_merge(src, tb[j + 1], u, t, W);
-                const float v2 = head_merge(src, tb[j + 2], u, t, W);
-                const float v3 = head_merge(src, tb[j + 3], u, t, W);
-                if (writer) {
-                    put(j, v0);
-                    put(j + 1, v1);
-                    put(j + 2, v2);
-                    put(j + 3, v3);
-                }
-            }
-            for (; j < rows; ++j) {
-                const float v = head_merge(src, tb[j], u, t, W);
+            // shared-memory reads and global stores do not alias: the
+            // compiler may hoist the loads of later rows above the stores
+#pragma unroll 4
+            for (int j = 0; j < rows; ++j) {
+                const float v = head_merge(sb, tb[j], u);
                 if (writer) put(j, v);
             }
         }
+        tb += rows;
     }
 }
 

@@ -82,21 +82,33 @@ def emulate_head(x, params, groups, tab, r0c, ncols, rows_k):
                 xs[ok] = x[gi * G + c, t[ok]]
                 for ui in range(W):
                     a[c * r0c:(c + 1) * r0c, ui] = level0_staged(xs, ui, int(t[ui]), r0c)
-            src, dst = a, b
+            # the staged entries as the kernel forms them: byte offsets of the
+            # tail row and of the head row minus its shift, the first local
+            # column that adds the head row, the destination offset
+            t0 = tb * tile - halo
+            neg0 = max(0, -t0)
+            src, dst = a.reshape(-1), b.reshape(-1)
             for lev in range(1, depth + 1):
                 e = tab[int(toff[lev]): int(toff[lev]) + int(rows[lev])]
                 res = np.zeros((int(rows[lev]), W), np.float32)
                 for j, (ea, eb, es, _) in enumerate(e):
-                    assert 0 <= ea < src.shape[0] and 0 <= eb < src.shape[0] and es >= 0
-                    v = src[ea].copy()
-                    ok = (t >= es) & (u >= es)
-                    sh = np.zeros(W, np.float32)
-                    sh[es:] = src[eb, : W - es] if es < W else 0
-                    v[ok] = (v[ok] + sh[ok]).astype(np.float32)
+                    fx, fy, fz = ea * W * 4, (eb * W - es) * 4, es + neg0
+                    fw = j * W * 4 if lev < depth else j
+                    ia = fx // 4 + u
+                    assert ia.min() >= 0 and ia.max() < src.size
+                    v = src[ia].copy()
+                    ok = u >= fz
+                    assert np.array_equal(ok, (t >= es) & (u >= es))
+                    ib = fy // 4 + u[ok]
+                    if ib.size:
+                        assert ib.min() >= eb * W and ib.max() < (eb + 1) * W <= src.size
+                        v[ok] = (v[ok] + src[ib]).astype(np.float32)
+                    if lev < depth:
+                        idst = fw // 4 + u
+                        assert idst.min() >= 0 and idst.max() < dst.size
+                        dst[idst] = v
                     res[j] = v
                 if lev < depth:
-                    assert res.shape[0] <= dst.shape[0]
-                    dst[: res.shape[0]] = res
                     src, dst = dst, src
                 else:
                     wr = (u >= halo) & (u < halo + tile) & (t < ncols)

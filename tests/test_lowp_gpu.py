@@ -47,9 +47,14 @@ def test_lowp_ones_mode_and_external_workspace(cuda, prec):
     f.process_image_ws(None, d_out, True, ws)
     want = pyoracle.fdmt_lowp(fmin, fmax, None, nchan, ncols, max_dt, prec, 0, b_ones=True)
     assert np.array_equal(d_out.cpu().numpy(), want)
-    # the 16-bit planes take half the workspace of the FP32 ones
-    f32 = CFdmtGpu(fmin, fmax, nchan, ncols, max_dt, fuse_depth=0, external_ws=True)
-    assert f.workspace_size() <= f32.workspace_size() // 2 + 512
+    # two 16-bit ping-pong planes (2 bytes per value, 128-byte row pitch):
+    # even levels below the last in one, odd levels in the other
+    rows = f.rows_per_level()[:-1]
+    pitch = (ncols + 63) // 64 * 64
+
+    def plane(r):
+        return (int(r) * pitch * 2 + 255) // 256 * 256
+    assert f.workspace_size() == plane(rows[0::2].max()) + plane(rows[1::2].max())
 
 
 def test_lowp_error_against_fp64_on_device(cuda):
