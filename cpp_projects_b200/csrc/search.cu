@@ -136,91 +136,79 @@ k_boxcar(const float* __restrict__ plane, int rows, int cols, const float* __res
 }
 
 // Register-blocked boxcar for a width set fixed at compile time
-// (MODE 0: 1, 2, 4 .. WMAX; MODE 1: 1 .. WMAX).  Each thread owns kRegStarts
-// adjacent start samples; their window x[t .. t + kRegStarts + WMAX - 2] is
-// read once from shared memory with 128-bit loads and the running sums
-// advance from registers.  sqrtf(w) and RN(1/sqrtf(w)) come from the host
-// (IEEE there too).  The exact quotient sum / sqrtf(w) is only evaluated when
-// a one-multiply estimate cannot rule the window out: the estimate
-// qa = RN(sum * RN(1/sqrtf(w))) is within 2^-22 of the true quotient, so for
-// thr > 0 a window with qa <= thr * (1 - 1e-5) (thr_lo) cannot have
-// RN(sum / sqrtf(w)) > thr.  One warp vote per width skips the emission code
-// when no lane has a window above thr_lo.
-constexpr int kRegStarts = 4;
-constexpr int kRegTile = kBoxThreads * kRegStarts;
+// (MODE 0: 1, 2, 4 .. WMAX; MODE 1: 1 .. WMAX).  The CTA's row tile (starts
+// t0 .. t0 + kRegTile - 1 plus the WMAX - 1 samples after them) is read once,
+// normalised once and kept in shared memory.  Each thread owns kRegStarts
+// adjacent starts and runs their running sums side by side (independent add
+// chains, each in the reference's sequential order); it reads its window as
+// float4s just before the width step that first needs them, so only about
+// kRegStarts + 4 window values are live at a time.  sqrtf(w) and RN(1/sqrtf(w))
+// come from the host (IEEE there too).  The exact quotient sum / sqrtf(w) is
+// only evaluated when a one-multiply estimate cannot rule the window out: the
+// estimate qa = RN(sum * RN(1/sqrtf(w))) is within 2^-22 of the true quotient,
+// so for thr > 0 a window with qa <= thr * (1 - 1e-5) (thr_lo) cannot have
+// RN(sum / sqrtf(w)) > thr.  Per width the warp ORs the lanes' masks of such
+// windows and visits only the start offsets some lane has set.  Interior
+// tiles (every window inside the row) take a copy with no bounds tests.
+constexpr int kRegStarts = 16;
+constexpr int kRegThreads = 128;
+constexpr int kRegTile = kRegThreads * kRegStarts;
 
 struct WidthConsts {
     float sq[33];  // sqrtf(w), w = 1..32 (index w)
     float rs[33];  // RN(1 / sqrtf(w))
 };
 
-template <int MODE, int WMAX>
-__global__ void __launch_bounds__(kBoxThreads)
-k_boxcar_reg(const float* __restrict__ plane, int rows, int cols, const float* __restrict__ stats,
-             const float* __restrict__ d_thr, float thr_host, float thr_lo_host, int snr_fast,
-             bfs_cand* __restrict__ out, unsigned capacity, unsigned* __restrict__ d_count,
-             const WidthConsts wc, int tag, int* __restrict__ tags) {
-    constexpr int kWin = kRegStarts + WMAX - 1;
-    constexpr int kVec = (kWin + 3) / 4;
-    __shared__ float4 tile4[(kRegTile + 4 * kVec + 3) / 4];
-    float* tile = reinterpret_cast<float*>(tile4);
-    const int row = blockIdx.y;
-    const int t0 = blockIdx.x * kRegTile;
-    const float* x = plane + static_cast<size_t>(row) * cols;
-    constexpr int kSpan = kRegTile + 4 * kVec;
-    // interior tile: every window of every start lies inside the row
-    const bool interior = (t0 + kSpan) <= cols;
-    if (stats) {
-        const float m = stats[row], sd = stats[rows + row];
-        for (int i = threadIdx.x; i < kSpan; i += kBoxThreads) {
-            const int t = t0 + i;
-            tile[i] = (interior || t < cols) ? norm_sample(__ldg(x + t), m, sd) : 0.0f;
-        }
-    } else {
-        for (int i = threadIdx.x; i < kSpan; i += kBoxThreads) {
-            const int t = t0 + i;
-            tile[i] = (interior || t < cols) ? __ldg(x + t) : 0.0f;
-        }
-    }
-    __syncthreads();
-    float thr = thr_host, thr_lo = thr_lo_host;
-    if (d_thr) {
-        thr = __ldg(d_thr);
-        thr_lo = thr > 0.0f ? thr * 0.99999f : -INFINITY;
-    }
+template <int MODE, int WMAX, bool INTERIOR>
+__device__ __forceinline__ void boxcar_starts(const float4* __restrict__ win4, int tb, int cols, int row,
+                                              float thr, float thr_lo, int snr_fast, const WidthConsts& wc,
+                                              bfs_cand* __restrict__ out, unsigned capacity,
+                                              unsigned* __restrict__ d_count, int tag, int* __restrict__ tags) {
+    constexpr int S = kRegStarts;
+    constexpr int kVec = (S + WMAX - 1 + 3) / 4;
+    const int lane = threadIdx.x & 31;
     float win[4 * kVec];
+    float sum[S];
 #pragma unroll
-    for (int v = 0; v < kVec; ++v) {
-        const float4 q = tile4[threadIdx.x + v];
+    for (int v = 0; v < S / 4; ++v) {
+        const float4 q = win4[v];
         win[4 * v] = q.x; win[4 * v + 1] = q.y; win[4 * v + 2] = q.z; win[4 * v + 3] = q.w;
     }
-    const int tb = t0 + threadIdx.x * kRegStarts;
-    const int lane = threadIdx.x & 31;
-    float sum[kRegStarts];
 #pragma unroll
-    for (int j = 0; j < kRegStarts; ++j) sum[j] = 0.0f;
+    for (int j = 0; j < S; ++j) sum[j] = 0.0f;
 #pragma unroll
     for (int w = 1; w <= WMAX; ++w) {
+        // step w reads window values w - 1 .. w + S - 2: fetch the vector
+        // that starts at value w + S - 2 when the step first reaches it
+        constexpr int kFirst = S / 4;
+        if (((w + S - 2) & 3) == 0 && (w + S - 2) / 4 >= kFirst && (w + S - 2) / 4 < kVec) {
+            const float4 q = win4[(w + S - 2) / 4];
+            const int b = w + S - 2;
+            win[b] = q.x; win[b + 1] = q.y; win[b + 2] = q.z; win[b + 3] = q.w;
+        }
 #pragma unroll
-        for (int j = 0; j < kRegStarts; ++j) sum[j] = __fadd_rn(sum[j], win[j + w - 1]);
+        for (int j = 0; j < S; ++j) sum[j] = __fadd_rn(sum[j], win[j + w - 1]);
         if (MODE == 0 && (w & (w - 1)) != 0) continue;
         const float rs = wc.rs[w];
-        bool maybe[kRegStarts];
-        bool anyp = false;
+        unsigned maybe = 0;
 #pragma unroll
-        for (int j = 0; j < kRegStarts; ++j) {
-            maybe[j] = __fmul_rn(sum[j], rs) > thr_lo && (interior || (tb + j + w - 1) < cols);
-            anyp |= maybe[j];
-        }
-        if (!__any_sync(0xffffffffu, anyp)) continue;
+        for (int j = 0; j < S; ++j)
+            if (__fmul_rn(sum[j], rs) > thr_lo && (INTERIOR || tb + j + w - 1 < cols)) maybe |= 1u << j;
+        unsigned todo = __reduce_or_sync(0xffffffffu, maybe);
+        if (!todo) continue;
         const float sq = wc.sq[w];
         const int code = (MODE == 1) ? w : (31 - __clz(w));
+        while (todo) {  // warp-uniform: the start offsets some lane may emit
+            const int j = __ffs(todo) - 1;
+            todo &= todo - 1;
+            float sj = sum[0];
 #pragma unroll
-        for (int j = 0; j < kRegStarts; ++j) {
+            for (int k = 1; k < S; ++k)
+                if (k == j) sj = sum[k];
             float snr = 0.0f;
             bool pass = false;
-            if (maybe[j]) {
-                snr = snr_fast ? __fdividef(sum[j], sq) : __fdiv_rn(sum[j], sq);
+            if ((maybe >> j) & 1u) {
+                snr = snr_fast ? __fdividef(sj, sq) : __fdiv_rn(sj, sq);
                 pass = snr > thr;
             }
             const unsigned ballot = __ballot_sync(0xffffffffu, pass);
@@ -241,6 +229,58 @@ k_boxcar_reg(const float* __restrict__ plane, int rows, int cols, const float* _
             }
         }
     }
+}
+
+template <int MODE, int WMAX>
+__global__ void __launch_bounds__(kRegThreads)
+k_boxcar_reg(const float* __restrict__ plane, int rows, int cols, const float* __restrict__ stats,
+             const float* __restrict__ d_thr, float thr_host, float thr_lo_host, int snr_fast,
+             bfs_cand* __restrict__ out, unsigned capacity, unsigned* __restrict__ d_count,
+             const WidthConsts wc, int tag, int* __restrict__ tags) {
+    constexpr int kSpan = kRegTile + 4 * ((WMAX - 1 + 3) / 4);
+    __shared__ float4 tile4[kSpan / 4];
+    float* tile = reinterpret_cast<float*>(tile4);
+    const int row = blockIdx.y;
+    const int t0 = blockIdx.x * kRegTile;
+    const float* x = plane + static_cast<size_t>(row) * cols;
+    // interior tile: every window of every start lies inside the row
+    const bool interior = (t0 + kSpan) <= cols;
+    if (stats) {
+        const float m = stats[row], sd = stats[rows + row];
+        if (interior) {
+#pragma unroll 4
+            for (int i = threadIdx.x; i < kSpan; i += kRegThreads) tile[i] = norm_sample(__ldg(x + t0 + i), m, sd);
+        } else {
+            for (int i = threadIdx.x; i < kSpan; i += kRegThreads) {
+                const int t = t0 + i;
+                tile[i] = t < cols ? norm_sample(__ldg(x + t), m, sd) : 0.0f;
+            }
+        }
+    } else {
+        if (interior) {
+#pragma unroll 4
+            for (int i = threadIdx.x; i < kSpan; i += kRegThreads) tile[i] = __ldg(x + t0 + i);
+        } else {
+            for (int i = threadIdx.x; i < kSpan; i += kRegThreads) {
+                const int t = t0 + i;
+                tile[i] = t < cols ? __ldg(x + t) : 0.0f;
+            }
+        }
+    }
+    __syncthreads();
+    float thr = thr_host, thr_lo = thr_lo_host;
+    if (d_thr) {
+        thr = __ldg(d_thr);
+        thr_lo = thr > 0.0f ? thr * 0.99999f : -INFINITY;
+    }
+    const float4* win4 = tile4 + threadIdx.x * (kRegStarts / 4);
+    const int tb = t0 + threadIdx.x * kRegStarts;
+    if (interior)
+        boxcar_starts<MODE, WMAX, true>(win4, tb, cols, row, thr, thr_lo, snr_fast, wc, out, capacity, d_count,
+                                        tag, tags);
+    else
+        boxcar_starts<MODE, WMAX, false>(win4, tb, cols, row, thr, thr_lo, snr_fast, wc, out, capacity,
+                                         d_count, tag, tags);
 }
 
 // Canonical key of a candidate: (row * cols + start) << wbits | width code,
@@ -441,13 +481,14 @@ bfs_status launch_boxcar(const float* d_plane, int rows, int cols, const float* 
         // compile-time width sets: pow2 up to 32, every width up to 8
         const float thr_lo = thr > 0.0f ? thr * 0.99999f : -INFINITY;
         dim3 grid_r((cols + kRegTile - 1) / kRegTile, rows);
+        static_assert(kRegStarts % 4 == 0 && kRegStarts <= 32, "starts per thread: a multiple of 4, at most 32");
         WidthConsts wc;
         for (int w = 0; w <= 32; ++w) {
             wc.sq[w] = std::sqrt(static_cast<float>(w));  // IEEE-correct on the host
             wc.rs[w] = w ? 1.0f / wc.sq[w] : 0.0f;
         }
         bool launched = true;
-#define BFS_BOX_REG(M, W) k_boxcar_reg<M, W><<<grid_r, kBoxThreads, 0, s>>>(                  \
+#define BFS_BOX_REG(M, W) k_boxcar_reg<M, W><<<grid_r, kRegThreads, 0, s>>>(                  \
             d_plane, rows, cols, d_stats, d_thr, thr, thr_lo, snr_fast, d_out, capacity, d_count, wc, \
             tag, d_tags)
         if (mode == BFS_WIDTHS_POW2) {
