@@ -142,13 +142,12 @@ k_boxcar(const float* __restrict__ plane, int rows, int cols, const float* __res
 // adjacent starts and runs their running sums side by side (independent add
 // chains, each in the reference's sequential order); it reads its window as
 // float4s just before the width step that first needs them, so only about
-// kRegStarts + 4 window values are live at a time.  sqrtf(w) and RN(1/sqrtf(w))
-// come from the host (IEEE there too).  The exact quotient sum / sqrtf(w) is
-// only evaluated when a one-multiply estimate cannot rule the window out: the
-// estimate qa = RN(sum * RN(1/sqrtf(w))) is within 2^-22 of the true quotient,
-// so for thr > 0 a window with qa <= thr * (1 - 1e-5) (thr_lo) cannot have
-// RN(sum / sqrtf(w)) > thr.  Per width the warp ORs the lanes' masks of such
-// windows and visits only the start offsets some lane has set.  Interior
+// kRegStarts + 4 window values are live at a time.  sqrtf(w) comes from the
+// host (IEEE there too).  The exact quotient sum / sqrtf(w) is
+// only evaluated for windows whose sum exceeds a per-width lower bound of the
+// sums that can pass (thr > 0; every window when thr <= 0).  Per width the
+// warp ORs the lanes' masks of such windows and visits only the start offsets
+// some lane has set.  Interior
 // tiles (every window inside the row) take a copy with no bounds tests.
 constexpr int kRegStarts = 16;
 constexpr int kRegThreads = 128;
@@ -156,7 +155,6 @@ constexpr int kRegTile = kRegThreads * kRegStarts;
 
 struct WidthConsts {
     float sq[33];  // sqrtf(w), w = 1..32 (index w)
-    float rs[33];  // RN(1 / sqrtf(w))
 };
 
 template <int MODE, int WMAX, bool INTERIOR>
@@ -189,14 +187,17 @@ __device__ __forceinline__ void boxcar_starts(const float4* __restrict__ win4, i
 #pragma unroll
         for (int j = 0; j < S; ++j) sum[j] = __fadd_rn(sum[j], win[j + w - 1]);
         if (MODE == 0 && (w & (w - 1)) != 0) continue;
-        const float rs = wc.rs[w];
+        // RN(sum / sq) > thr needs sum / sq > thr (1 - 2^-24), so for thr > 0
+        // every passing window has sum > RN(RN(thr sq) (1 - 1e-5)) (the two
+        // roundings add at most 2^-23 relative): one compare per window
+        const float sq = wc.sq[w];
+        const float lim = thr_lo > -INFINITY ? __fmul_rn(__fmul_rn(thr, sq), 0.99999f) : -INFINITY;
         unsigned maybe = 0;
 #pragma unroll
         for (int j = 0; j < S; ++j)
-            if (__fmul_rn(sum[j], rs) > thr_lo && (INTERIOR || tb + j + w - 1 < cols)) maybe |= 1u << j;
+            if (sum[j] > lim && (INTERIOR || tb + j + w - 1 < cols)) maybe |= 1u << j;
         unsigned todo = __reduce_or_sync(0xffffffffu, maybe);
         if (!todo) continue;
-        const float sq = wc.sq[w];
         const int code = (MODE == 1) ? w : (31 - __clz(w));
         while (todo) {  // warp-uniform: the start offsets some lane may emit
             const int j = __ffs(todo) - 1;
@@ -248,8 +249,19 @@ k_boxcar_reg(const float* __restrict__ plane, int rows, int cols, const float* _
     if (stats) {
         const float m = stats[row], sd = stats[rows + row];
         if (interior) {
-#pragma unroll 4
-            for (int i = threadIdx.x; i < kSpan; i += kRegThreads) tile[i] = norm_sample(__ldg(x + t0 + i), m, sd);
+            // every load in flight before the first use
+            constexpr int kPer = (kSpan + kRegThreads - 1) / kRegThreads;
+            float v[kPer];
+#pragma unroll
+            for (int k = 0; k < kPer; ++k) {
+                const int i = threadIdx.x + k * kRegThreads;
+                v[k] = (k < kPer - 1 || i < kSpan) ? __ldg(x + t0 + i) : 0.0f;
+            }
+#pragma unroll
+            for (int k = 0; k < kPer; ++k) {
+                const int i = threadIdx.x + k * kRegThreads;
+                if (k < kPer - 1 || i < kSpan) tile[i] = norm_sample(v[k], m, sd);
+            }
         } else {
             for (int i = threadIdx.x; i < kSpan; i += kRegThreads) {
                 const int t = t0 + i;
@@ -258,8 +270,18 @@ k_boxcar_reg(const float* __restrict__ plane, int rows, int cols, const float* _
         }
     } else {
         if (interior) {
-#pragma unroll 4
-            for (int i = threadIdx.x; i < kSpan; i += kRegThreads) tile[i] = __ldg(x + t0 + i);
+            constexpr int kPer = (kSpan + kRegThreads - 1) / kRegThreads;
+            float v[kPer];
+#pragma unroll
+            for (int k = 0; k < kPer; ++k) {
+                const int i = threadIdx.x + k * kRegThreads;
+                v[k] = (k < kPer - 1 || i < kSpan) ? __ldg(x + t0 + i) : 0.0f;
+            }
+#pragma unroll
+            for (int k = 0; k < kPer; ++k) {
+                const int i = threadIdx.x + k * kRegThreads;
+                if (k < kPer - 1 || i < kSpan) tile[i] = v[k];
+            }
         } else {
             for (int i = threadIdx.x; i < kSpan; i += kRegThreads) {
                 const int t = t0 + i;
@@ -483,10 +505,7 @@ bfs_status launch_boxcar(const float* d_plane, int rows, int cols, const float* 
         dim3 grid_r((cols + kRegTile - 1) / kRegTile, rows);
         static_assert(kRegStarts % 4 == 0 && kRegStarts <= 32, "starts per thread: a multiple of 4, at most 32");
         WidthConsts wc;
-        for (int w = 0; w <= 32; ++w) {
-            wc.sq[w] = std::sqrt(static_cast<float>(w));  // IEEE-correct on the host
-            wc.rs[w] = w ? 1.0f / wc.sq[w] : 0.0f;
-        }
+        for (int w = 0; w <= 32; ++w) wc.sq[w] = std::sqrt(static_cast<float>(w));  // IEEE-correct on the host
         bool launched = true;
 #define BFS_BOX_REG(M, W) k_boxcar_reg<M, W><<<grid_r, kRegThreads, 0, s>>>(                  \
             d_plane, rows, cols, d_stats, d_thr, thr, thr_lo, snr_fast, d_out, capacity, d_count, wc, \
