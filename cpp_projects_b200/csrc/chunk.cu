@@ -112,40 +112,69 @@ __global__ void k_chirp(const float2* __restrict__ in, float2* __restrict__ out,
 
 // Power detection + roll by nbin/2 + unpadding + frequency reversal +
 // dedispersion shift, as one gather: output row r (fine channel, highest
-// frequency first), column c of the dedispersed plane.
-__global__ void __launch_bounds__(256)
+// frequency first), columns c .. c + kDetectCols - 1 of the dedispersed plane
+// per thread, so that every thread has kDetectCols x npol2 independent
+// voltage loads in flight and stores one 16-byte vector when the row allows.
+constexpr int kDetectThreads = 256;
+constexpr int kDetectCols = 4;
+
+__global__ void __launch_bounds__(kDetectThreads)
 k_detect(const float2* __restrict__ volt, float* __restrict__ plane, int nchan, int len_sft, int mbin,
          int nbin, int nfft, int npol2, int nov_pc, int mbin_adj, int msamp, const int* __restrict__ shift,
          double inv_nbin2) {
     const int r = blockIdx.y;
-    const int c0 = blockIdx.x * blockDim.x;
-    if (c0 + static_cast<int>(threadIdx.x) >= msamp) return;
-    // the CTA's first column, then this thread's by single-step carries
-    // (msamp, mbin_adj and nbin wrap at most once over a CTA's span when they
-    // are >= the CTA width; smaller ones are reduced by a short loop)
-    int idx = (c0 - __ldg(shift + r)) % msamp;  // dedisperse: out[(idx + s) % msamp] = in[idx]
+    const int c = (blockIdx.x * kDetectThreads + threadIdx.x) * kDetectCols;
+    if (c >= msamp) return;
+    // source column of output column c: dedisperse writes out[(idx + s) % msamp] = in[idx]
+    int idx = (c - __ldg(shift + r)) % msamp;
     if (idx < 0) idx += msamp;
-    idx += threadIdx.x;
-    while (idx >= msamp) idx -= msamp;
     const int isub = r / len_sft;
     const int ifine = len_sft - 1 - (r % len_sft);
     const int coarse = nchan - 1 - isub;
     int ifft = idx / mbin_adj;
-    const int ibin = idx - ifft * mbin_adj;
-    int q = ifine * mbin + ibin + nov_pc + nbin / 2;     // position before the roll
-    if (q >= nbin) q -= nbin;
+    int ibin = idx - ifft * mbin_adj;
+    int q0 = ifine * mbin + nov_pc + nbin / 2;   // position of ibin 0 before the roll
+    if (q0 >= nbin) q0 -= nbin;
     const size_t pol_stride = static_cast<size_t>(nfft) * nchan * nbin;
-    const size_t base = (static_cast<size_t>(ifft) * nchan + coarse) * nbin + q;
-    float acc = 0.0f;
-    for (int ipol = 0; ipol < npol2; ++ipol) {
-        const float2 v = __ldg(volt + base + ipol * pol_stride);
-        const double x = v.x, y = v.y;
-        // |v|^2 / nbin / nbin in FP64 (the reference's roll kernel); with nbin a
-        // power of two the two divides are an exact scaling by 2^-2k
-        const double pw = inv_nbin2 > 0.0 ? (x * x + y * y) * inv_nbin2 : (x * x + y * y) / nbin / nbin;
-        acc = __fadd_rn(acc, static_cast<float>(pw));
+    float2 v[kDetectCols][2];
+#pragma unroll
+    for (int j = 0; j < kDetectCols; ++j) {
+        int q = q0 + ibin;
+        if (q >= nbin) q -= nbin;
+        const size_t base = (static_cast<size_t>(ifft) * nchan + coarse) * nbin + q;
+        const bool live = c + j < msamp;
+#pragma unroll
+        for (int ipol = 0; ipol < 2; ++ipol)
+            v[j][ipol] = (live && ipol < npol2) ? __ldg(volt + base + ipol * pol_stride) : make_float2(0.f, 0.f);
+        // next source column: idx + 1, wrapping at msamp, carried into (ifft, ibin)
+        if (++idx == msamp) {
+            idx = 0; ifft = 0; ibin = 0;
+        } else if (++ibin == mbin_adj) {
+            ibin = 0; ++ifft;
+        }
     }
-    plane[static_cast<size_t>(r) * msamp + c0 + threadIdx.x] = acc;
+    float acc[kDetectCols];
+#pragma unroll
+    for (int j = 0; j < kDetectCols; ++j) {
+        acc[j] = 0.0f;
+#pragma unroll
+        for (int ipol = 0; ipol < 2; ++ipol) {
+            if (ipol >= npol2) break;
+            const double x = v[j][ipol].x, y = v[j][ipol].y;
+            // |v|^2 / nbin / nbin in FP64 (the reference's roll kernel); with nbin a
+            // power of two the two divides are an exact scaling by 2^-2k
+            const double pw = inv_nbin2 > 0.0 ? (x * x + y * y) * inv_nbin2 : (x * x + y * y) / nbin / nbin;
+            acc[j] = __fadd_rn(acc[j], static_cast<float>(pw));
+        }
+    }
+    float* o = plane + static_cast<size_t>(r) * msamp + c;
+    if ((msamp & 3) == 0) {   // c is a multiple of 4: the row offset keeps 16-byte alignment
+        *reinterpret_cast<float4*>(o) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < kDetectCols; ++j)
+            if (c + j < msamp) o[j] = acc[j];
+    }
 }
 
 bfs_status cufft_check(cufftResult r, const char* what) {
@@ -301,11 +330,13 @@ static bfs_status chunk_detect(bfs_chunk* c, const float2* d_volt, double dm, fl
     chunk_shifts(c, dm, sh);
     BFS_CUDA(cudaMemcpyAsync(c->d_shift, sh.data(), sizeof(int) * sh.size(), cudaMemcpyHostToDevice, s));
     const bfs_chunk_desc& d = c->d;
-    dim3 grid((c->msamp + 255) / 256, c->rows);
+    const int span = kDetectThreads * kDetectCols;
+    dim3 grid((c->msamp + span - 1) / span, c->rows);
     BFS_ARG(grid.y <= 65535, "too many fine channels");
+    BFS_ARG(d.npol / 2 <= 2, "at most two polarisations");
     const bool pow2 = (d.nbin & (d.nbin - 1)) == 0;
     const double inv_nbin2 = pow2 ? 1.0 / (static_cast<double>(d.nbin) * d.nbin) : 0.0;  // exact for 2^k
-    k_detect<<<grid, 256, 0, s>>>(d_volt, d_plane, d.nchan, d.len_sft, c->mbin, d.nbin, d.nfft,
+    k_detect<<<grid, kDetectThreads, 0, s>>>(d_volt, d_plane, d.nchan, d.len_sft, c->mbin, d.nbin, d.nfft,
                                   d.npol / 2, c->nov_pc, c->mbin_adj, c->msamp, c->d_shift, inv_nbin2);
     BFS_LAUNCH_CHECK("k_detect");
     // the host vector must outlive the (pageable, staged) copy: wait for it
