@@ -153,8 +153,10 @@ constexpr int kRegStarts = 16;
 constexpr int kRegThreads = 128;
 constexpr int kRegTile = kRegThreads * kRegStarts;
 
+constexpr int kRegMaxW = 128;  // widest window of the register-blocked kernel
+
 struct WidthConsts {
-    float sq[33];  // sqrtf(w), w = 1..32 (index w)
+    float sq[kRegMaxW + 1];  // sqrtf(w), w = 1..kRegMaxW (index w)
 };
 
 template <int MODE, int WMAX, bool INTERIOR>
@@ -500,12 +502,12 @@ bfs_status launch_boxcar(const float* d_plane, int rows, int cols, const float* 
         return fail(BFS_ERR_ARG, "unknown widths_mode %d", mode);
     }
     {
-        // compile-time width sets: pow2 up to 32, every width up to 8
+        // compile-time width sets: pow2 up to 128, every width up to 8
         const float thr_lo = thr > 0.0f ? thr * 0.99999f : -INFINITY;
         dim3 grid_r((cols + kRegTile - 1) / kRegTile, rows);
         static_assert(kRegStarts % 4 == 0 && kRegStarts <= 32, "starts per thread: a multiple of 4, at most 32");
         WidthConsts wc;
-        for (int w = 0; w <= 32; ++w) wc.sq[w] = std::sqrt(static_cast<float>(w));  // IEEE-correct on the host
+        for (int w = 0; w <= kRegMaxW; ++w) wc.sq[w] = std::sqrt(static_cast<float>(w));  // IEEE-correct on the host
         bool launched = true;
 #define BFS_BOX_REG(M, W) k_boxcar_reg<M, W><<<grid_r, kRegThreads, 0, s>>>(                  \
             d_plane, rows, cols, d_stats, d_thr, thr, thr_lo, snr_fast, d_out, capacity, d_count, wc, \
@@ -518,6 +520,8 @@ bfs_status launch_boxcar(const float* d_plane, int rows, int cols, const float* 
                 case 8: BFS_BOX_REG(0, 8); break;
                 case 16: BFS_BOX_REG(0, 16); break;
                 case 32: BFS_BOX_REG(0, 32); break;
+                case 64: BFS_BOX_REG(0, 64); break;
+                case 128: BFS_BOX_REG(0, 128); break;
                 default: launched = false;
             }
         } else {

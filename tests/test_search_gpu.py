@@ -67,7 +67,7 @@ PLANES = [(8, 5000), (3, 1024), (1, 37), (17, 2049), (64, 3000)]
 
 
 @pytest.mark.parametrize("shape", PLANES)
-@pytest.mark.parametrize("mode,param", [(0, 5), (0, 0), (1, 4), (1, 33)])
+@pytest.mark.parametrize("mode,param", [(0, 5), (0, 0), (0, 6), (0, 7), (0, 8), (1, 4), (1, 33)])
 def test_boxcar_matches_oracle(cuda, shape, mode, param):
     rng = np.random.default_rng(hash((shape, mode, param)) % 2**32)
     x = rng.standard_normal(shape).astype(np.float32)
