@@ -82,6 +82,15 @@ class CChunk_gpu:
     def forward_fft(self, d_cplx, stream=None):
         _capi.call("bfs_chunk_forward_fft", self._h, dev_ptr(d_cplx, torch.float32), stream_handle(stream))
 
+    def unpack_fft(self, d_raw: torch.Tensor, d_spec: torch.Tensor, stream=None) -> None:
+        """unpack + forward FFT in one step: the spectra of every segment of the
+        GUPPI int8 chunk (for nbin = 2^20 a fused four-step transform that reads
+        the int8 samples directly; other sizes unpack and call cuFFT)."""
+        if d_raw.numel() != self.m_nchan * self.len_chunk * self.m_npol:
+            raise ValueError("raw chunk has the wrong size")
+        _capi.call("bfs_chunk_unpack_fft", self._h, dev_ptr(d_raw, torch.int8, "d_raw"),
+                   dev_ptr(d_spec, torch.float32, "d_spec"), stream_handle(stream))
+
     def voltages(self, d_spec, dm: float, d_volt, stream=None):
         _capi.call("bfs_chunk_voltages", self._h, dev_ptr(d_spec, torch.float32), ctypes.c_double(dm),
                    dev_ptr(d_volt, torch.float32), stream_handle(stream))
@@ -97,6 +106,27 @@ class CChunk_gpu:
                           device=pcmparrRawSignalCur.device)
         _capi.call("bfs_chunk_process", self._h, dev_ptr(pcmparrRawSignalCur, torch.float32),
                    dms.ctypes.data_as(ctypes.c_void_p), len(dms), dev_ptr(out), stream_handle(stream))
+        return out
+
+    def process_spectrum(self, d_spec: torch.Tensor, stream=None) -> torch.Tensor:
+        """The per-DM part of process on spectra from unpack_fft / forward_fft
+        (d_spec is not modified): (ndm, max_dt, msamp) planes."""
+        dms = np.ascontiguousarray(self.m_coh_dm_Vector, np.float64)
+        out = torch.empty((len(dms), self.max_dt, self.msamp), dtype=torch.float32, device=d_spec.device)
+        _capi.call("bfs_chunk_process_spectrum", self._h, dev_ptr(d_spec, torch.float32),
+                   dms.ctypes.data_as(ctypes.c_void_p), len(dms), dev_ptr(out), stream_handle(stream))
+        return out
+
+    def process_raw(self, d_raw: torch.Tensor, d_spec: torch.Tensor, stream=None) -> torch.Tensor:
+        """unpack_fft + the per-DM part of process: (ndm, max_dt, msamp) planes
+        straight from the int8 chunk; d_spec receives the spectra."""
+        if d_raw.numel() != self.m_nchan * self.len_chunk * self.m_npol:
+            raise ValueError("raw chunk has the wrong size")
+        dms = np.ascontiguousarray(self.m_coh_dm_Vector, np.float64)
+        out = torch.empty((len(dms), self.max_dt, self.msamp), dtype=torch.float32, device=d_raw.device)
+        _capi.call("bfs_chunk_process_raw", self._h, dev_ptr(d_raw, torch.int8, "d_raw"),
+                   dev_ptr(d_spec, torch.float32, "d_spec"), dms.ctypes.data_as(ctypes.c_void_p), len(dms),
+                   dev_ptr(out), stream_handle(stream))
         return out
 
     def search(self, planes: torch.Tensor, logfile: str | None = "candidates.log",

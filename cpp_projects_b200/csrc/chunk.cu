@@ -54,6 +54,9 @@ struct bfs_chunk {
 };
 
 namespace bfs {
+bool fft_fused_supported(int nbin, int npol);
+bfs_status fft_forward_guppi(const signed char* raw, float2* tmp, float2* x, long long nsamp, int noverlap,
+                             int nfft, int nchan, int npol, cudaStream_t s);
 namespace {
 
 constexpr double kDispersionConstant = 4.148808e9;  // MHz^2 pc^-1 cm^3 us (Chunk_fly_gpu.cu:139)
@@ -350,12 +353,23 @@ extern "C" bfs_status bfs_chunk_detect(bfs_chunk* c, const void* d_volt, double 
     return chunk_detect(c, static_cast<const float2*>(d_volt), dm, d_plane, as_stream(stream));
 }
 
-extern "C" bfs_status bfs_chunk_process(bfs_chunk* c, void* d_cplx, const double* dms, int ndm,
-                                        float* d_out, void* stream) {
-    BFS_ARG(c && d_cplx && d_out && (ndm == 0 || dms), "null argument");
-    cudaStream_t s = as_stream(stream);
-    bfs_status st = bfs_chunk_forward_fft(c, d_cplx, stream);
+extern "C" bfs_status bfs_chunk_unpack_fft(bfs_chunk* c, const int8_t* d_raw, void* d_spec, void* stream) {
+    BFS_ARG(c && d_raw && d_spec, "null argument");
+    const bfs_chunk_desc& d = c->d;
+    if (fft_fused_supported(d.nbin, d.npol))
+        return fft_forward_guppi(reinterpret_cast<const signed char*>(d_raw), c->volt, static_cast<float2*>(d_spec),
+                                 c->len_chunk, d.noverlap, d.nfft, d.nchan, d.npol, as_stream(stream));
+    bfs_status st = bfs_chunk_unpack(c, d_raw, d_spec, stream);
     if (st != BFS_OK) return st;
+    return bfs_chunk_forward_fft(c, d_spec, stream);
+}
+
+// Per coherent DM: voltages, detection, preprocessing, FDMT of mask and data,
+// fdmt_normalization (the loop of CChunk_gpu::process after its forward FFT).
+static bfs_status chunk_dm_loop(bfs_chunk* c, const void* d_cplx, const double* dms, int ndm, float* d_out,
+                                void* stream) {
+    cudaStream_t s = as_stream(stream);
+    bfs_status st = BFS_OK;
     const size_t plane_out = static_cast<size_t>(c->d.max_dt) * c->msamp;
     for (int i = 0; i < ndm; ++i) {
         st = chunk_voltages(c, d_cplx, dms[i], c->volt, s);
@@ -375,4 +389,26 @@ extern "C" bfs_status bfs_chunk_process(bfs_chunk* c, void* d_cplx, const double
         if (st != BFS_OK) return st;
     }
     return BFS_OK;
+}
+
+extern "C" bfs_status bfs_chunk_process(bfs_chunk* c, void* d_cplx, const double* dms, int ndm,
+                                        float* d_out, void* stream) {
+    BFS_ARG(c && d_cplx && d_out && (ndm == 0 || dms), "null argument");
+    bfs_status st = bfs_chunk_forward_fft(c, d_cplx, stream);
+    if (st != BFS_OK) return st;
+    return chunk_dm_loop(c, d_cplx, dms, ndm, d_out, stream);
+}
+
+extern "C" bfs_status bfs_chunk_process_spectrum(bfs_chunk* c, const void* d_spec, const double* dms, int ndm,
+                                                 float* d_out, void* stream) {
+    BFS_ARG(c && d_spec && d_out && (ndm == 0 || dms), "null argument");
+    return chunk_dm_loop(c, d_spec, dms, ndm, d_out, stream);
+}
+
+extern "C" bfs_status bfs_chunk_process_raw(bfs_chunk* c, const int8_t* d_raw, void* d_spec, const double* dms,
+                                            int ndm, float* d_out, void* stream) {
+    BFS_ARG(c && d_raw && d_spec && d_out && (ndm == 0 || dms), "null argument");
+    bfs_status st = bfs_chunk_unpack_fft(c, d_raw, d_spec, stream);
+    if (st != BFS_OK) return st;
+    return chunk_dm_loop(c, d_spec, dms, ndm, d_out, stream);
 }

@@ -444,6 +444,23 @@ bfs_status bfs_chunk_detect(bfs_chunk* chunk, const void* d_volt, double dm, flo
  * d_out[i] (max_dt x msamp each). */
 bfs_status bfs_chunk_process(bfs_chunk* chunk, void* d_cplx, const double* dms, int ndm,
                              float* d_out, void* stream);
+/* unpack_chunk_guppi_gpu (Session_guppi_gpu.cu:117-141) followed by the
+ * forward FFT of CChunk_gpu::process (Chunk_gpu.cu:267), as one step: d_spec
+ * (complex values per buffer, bfs_chunk_info[6]) receives the spectra of every
+ * segment.  For nbin = 2^20 a four-step transform whose first pass reads the
+ * int8 samples directly (no complex copy of the chunk); it agrees with
+ * bfs_chunk_unpack + bfs_chunk_forward_fft to FP32 rounding.  Other sizes run
+ * those two.  Uses the chunk's voltage buffer as scratch. */
+bfs_status bfs_chunk_unpack_fft(bfs_chunk* chunk, const int8_t* d_raw, void* d_spec, void* stream);
+/* The per-DM part of CChunkB::process (Chunk_gpu.cu:284-359) on spectra from
+ * bfs_chunk_unpack_fft or bfs_chunk_forward_fft: d_spec is not modified. */
+bfs_status bfs_chunk_process_spectrum(bfs_chunk* chunk, const void* d_spec, const double* dms, int ndm,
+                                      float* d_out, void* stream);
+/* CSession_guppi_gpu::unpack_chunk + CChunkB::process from the raw chunk:
+ * bfs_chunk_unpack_fft into d_spec, then per DM what bfs_chunk_process does
+ * after its forward FFT. */
+bfs_status bfs_chunk_process_raw(bfs_chunk* chunk, const int8_t* d_raw, void* d_spec, const double* dms,
+                                 int ndm, float* d_out, void* stream);
 
 /* ---- self-tests (no reference counterpart) ---- */
 
