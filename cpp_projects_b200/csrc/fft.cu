@@ -34,7 +34,7 @@ constexpr long long kFftN = static_cast<long long>(kF) * kF;
 constexpr int kTile = 33;         // padded row of a warp's 32 x 32 exchange tile
 constexpr int kRegion = 32 * kTile + 4;  // float2 per warp region (the +4 staggers regions' banks)
 constexpr int kColCols = 4;       // columns per CTA in the column pass
-constexpr int kRowRows = 8;       // rows per CTA in the row pass
+constexpr int kRowRows = 4;       // rows per CTA in the row pass (32-byte output runs)
 
 // cos(pi k / 16), k = 0..8, each rounded once to float (sin(pi k/16) = cos16(8-k)).
 __host__ __device__ constexpr float cos16(int k) {
@@ -100,7 +100,7 @@ __device__ __forceinline__ void fft1024_warp(float2 (&r)[32], float2* __restrict
 // Column pass.  grid (kF / kColCols, nfft, nchan); NP2 polarisations.  Warp w
 // transforms column c0 + (w % kColCols) of polarisation w / kColCols.
 template <int NP2>
-__global__ void __launch_bounds__(32 * NP2 * kColCols, 6 / NP2)
+__global__ void __launch_bounds__(32 * NP2 * kColCols)
 k_fft_cols_guppi(const signed char* __restrict__ raw, float2* __restrict__ y, const float2* __restrict__ tw_g,
                  const float2* __restrict__ twa, const float2* __restrict__ twb, long long nsamp, int noverlap,
                  int nfft, int nchan) {
@@ -166,7 +166,7 @@ k_fft_cols_guppi(const signed char* __restrict__ raw, float2* __restrict__ y, co
 
 // Row pass.  grid (kF / kRowRows, segments); warp w transforms row
 // r0 + w (contiguous over n2) and the CTA writes X[k2 N1 + r0 .. + kRowRows).
-__global__ void __launch_bounds__(32 * kRowRows, 3)
+__global__ void __launch_bounds__(32 * kRowRows)
 k_fft_rows(const float2* __restrict__ y, float2* __restrict__ x, const float2* __restrict__ tw_g) {
     extern __shared__ float2 sm_rows[];
     float2* tw = sm_rows;
