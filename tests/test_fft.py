@@ -1,11 +1,14 @@
-"""The fused GUPPI unpack + forward FFT of 2^20-sample segments.
+"""The fused GUPPI unpack + forward FFT of 2^20-sample segments, and the
+coherent stage at the reference's FFT sizes.
 
 CPU: an emulation of the kernels' index arithmetic (32-point decimation-in-
 frequency transforms, bit reversal, the 32 x 33 exchange tile, the four-step
-twiddles) against numpy's FFT.  GPU: bfs_chunk_unpack_fft against the FP64
-FFT of the oracle's unpack and against unpack + cuFFT, and bfs_chunk_process_raw
-against unpack + bfs_chunk_process (tolerance: 1e-5 of the largest magnitude,
-the north-star bound for voltages; the FFT itself is held to 2e-6)."""
+twiddles) against numpy's FFT.  GPU:
+bfs_chunk_unpack_fft against the FP64 FFT of the oracle's unpack and against
+unpack + cuFFT, the voltages against the FP64 oracle, and
+bfs_chunk_process_raw against unpack + bfs_chunk_process (tolerance: 1e-5 of
+the largest magnitude, the north-star bound for voltages; the forward FFT
+itself is held to 2e-6)."""
 import numpy as np
 import pytest
 import torch
@@ -100,6 +103,25 @@ def test_unpack_fft_matches_fp64_and_cufft(cuda, npol):
     # a second call on the same buffers gives the same bits
     ch.unpack_fft(d_raw, spec)
     assert np.array_equal(spec.cpu().numpy().view(np.complex64).reshape(got.shape), got)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dm", [0.0, 56.8])
+def test_voltages_of_2e15_subbands_within_1e5_of_fp64(cuda, dm):
+    """The reference's sizes (nbin 2^20, 32 sub-bands of 2^15 samples): chirp
+    + inverse FFTs against the FP64 oracle applied to the same spectra."""
+    ch, g = _chunk(GEO), co.Geometry(**GEO)
+    spec = ch.complex_buffer(cuda)
+    ch.unpack_fft(torch.from_numpy(_raw(g, 14)).to(cuda), spec)
+    volt = ch.complex_buffer(cuda)
+    ch.voltages(spec, dm, volt)
+    shape = (g.npol // 2, g.nfft, g.nchan, g.nbin)
+    got = volt.cpu().numpy().view(np.complex64).reshape(shape)
+    want = co.voltages(g, spec.cpu().numpy().view(np.complex64).reshape(shape).astype(np.complex128), dm)
+    err = np.abs(got - want).max() / np.abs(want).max()
+    assert err < 1e-5, err
+    ch.voltages(spec, dm, volt)                   # the same bits again
+    assert np.array_equal(volt.cpu().numpy().view(np.complex64).reshape(shape), got)
 
 
 @pytest.mark.gpu
