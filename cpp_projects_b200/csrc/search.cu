@@ -149,7 +149,7 @@ k_boxcar(const float* __restrict__ plane, int rows, int cols, const float* __res
 // warp ORs the lanes' masks of such windows and visits only the start offsets
 // some lane has set.  Interior
 // tiles (every window inside the row) take a copy with no bounds tests.
-constexpr int kRegStarts = 16;
+constexpr int kRegStarts = 8;
 constexpr int kRegThreads = 128;
 constexpr int kRegTile = kRegThreads * kRegStarts;
 
