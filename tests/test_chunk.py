@@ -5,7 +5,7 @@ CChunkB::process chain, against the FP64 oracle (oracle/chunk_oracle.py).
 Tolerances: unpack and the detect gather are exact (the gather is checked on
 the GPU's own voltages with the reference's float rounding of each
 polarisation's power); cuFFT + chirp against FP64 numpy within 1e-5 of the
-largest magnitude (north star: voltages within 1e-5 relative)."""
+largest magnitude (the required bound: voltages within 1e-5 relative)."""
 import numpy as np
 import pytest
 import torch

@@ -7,7 +7,7 @@ twiddles) against numpy's FFT.  GPU:
 bfs_chunk_unpack_fft against the FP64 FFT of the oracle's unpack and against
 unpack + cuFFT, the voltages against the FP64 oracle, and
 bfs_chunk_process_raw against unpack + bfs_chunk_process (tolerance: 1e-5 of
-the largest magnitude, the north-star bound for voltages; the forward FFT
+the largest magnitude, the required bound for voltages; the forward FFT
 itself is held to 2e-6)."""
 import numpy as np
 import pytest

@@ -52,8 +52,9 @@ def test_product_plan_tables_match_oracle(case):
         _capi.lib().bfs_fdmt_plan_destroy(plan)
 
 
-def test_config0_row_counts_match_survey():
-    # level totals of the 512-channel 1200-1600 MHz plan, maxDT 512
+def test_512_channel_plan_row_counts():
+    # level totals of the 512-channel 1200-1600 MHz plan, maxDT 512 (the
+    # figures the algorithmic-byte count of this shape is built from)
     rows = pyoracle.fdmt_rows(1200.0, 1600.0, 512, 512)
     assert list(rows) == [1536, 887, 700, 608, 557, 537, 524, 517, 514, 512]
 
