@@ -2,7 +2,8 @@
 """Throughput of the FDMT + normalise + boxcar + cluster search path on B200.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
-                    [--workload config2|config0]
+                    [--workload config2|config0|config1|config3|config4|config4fwd]
+                    [--form both|batched] [--no-e2e] [--no-cpu-baseline] [--no-ref-gpu]
 
 Workload (default ``config2``): the batched multi-beam search — 48 beams of
 uneven shapes (nchan from {256, 512, 1024, 4096}, 2^14..2^17 samples, max
@@ -16,7 +17,12 @@ then one sort and one clustering for all beams); the plain per-beam form
 (the same kernels with host round trips per beam) is timed beside it and
 must return identical results.  ``config0`` is the single
 512 x 32768 beam of the reference's CPU-runnable case; ``config4fwd`` one
-1024 x 65536 beam (used for profiling: its input exceeds L2).
+1024 x 65536 beam (used for profiling: its input exceeds L2).  The other
+workloads print their own line with the same metric: ``config1`` one raw
+32-channel GUPPI chunk through the coherent stage (fused unpack + FFT, chirp,
+inverse FFTs, detection) into the FDMT and search; ``config3`` a 4096 x 2^17
+plane with FP32 / FP16 / BF16 FDMT planes (error against FP64, recall against
+FP32); ``config4`` forward against adjoint FDMT with the gradient checks.
 
 Metric: channel*samples per second over the whole job (all ranks).
 ``value`` is device-timed with inputs already in HBM (the working set of
