@@ -243,8 +243,12 @@ def run_reference(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded N(0,1) + injected pulses, generated on the host)",
             "impl": "reference",
-            "config": {"workload": f"{args.workload} (bounded CPU sample per step)",
-                       "search": "widths 1..32 pow2, thr 7, clusters +-16 samples/+-8 rows"},
+            "config": {"workload": args.workload, "beams": len(beams),
+                       "chan_samples_per_rank": int(sum(b.nchan * b.nsamp for b in beams)),
+                       "nchan_set": sorted({b.nchan for b in beams}),
+                       "search": "pow2 widths 1..32, S/N > 7, clusters +-16 samples/+-8 rows/any width",
+                       "timed": "a bounded sample of the workload's beams per step (cpu_baseline.sample), "
+                                "rate in channel-samples per second"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
                              "sample": texts},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
