@@ -246,11 +246,17 @@ static int bits_for(unsigned long long v) {
     return b;
 }
 
+// One pass of the split: sort by (group, field), flag the positions where the
+// group changes or the field jumps by more than the metric, and renumber the
+// groups.  With sort_only the pass cannot split (the metric is at least the
+// field's whole range): the sort alone fixes the member order, the groups and
+// their boundaries stay those of the previous pass.
 template <typename K>
 static bfs_status cluster_pass(const bfs_cand* d_cands, unsigned n, int field, int fmin, int fbits,
                                int end_bit, long long metric, unsigned* gid, bool first, void* kin,
                                void* kout, unsigned* v_in, unsigned* v_out, unsigned* flags,
-                               unsigned* scan, void* tmp, size_t tmp_bytes, cudaStream_t s) {
+                               unsigned* scan, void* tmp, size_t tmp_bytes, cudaStream_t s,
+                               bool sort_only = false) {
     const int th = 256;
     const int bl = static_cast<int>((n + th - 1) / th);
     K* k_in = static_cast<K*>(kin);
@@ -260,6 +266,7 @@ static bfs_status cluster_pass(const bfs_cand* d_cands, unsigned n, int field, i
     size_t b = tmp_bytes;
     BFS_CUDA(cub::DeviceRadixSort::SortPairs(tmp, b, k_in, k_out, v_in, v_out, static_cast<int>(n),
                                              0, end_bit > 0 ? end_bit : 1, s));
+    if (sort_only) return BFS_OK;
     k_pass_flags<K><<<bl, th, 0, s>>>(d_cands, k_out, v_out, n, field, fbits, metric, flags);
     BFS_LAUNCH_CHECK("k_pass_flags");
     b = tmp_bytes;
@@ -331,19 +338,24 @@ extern "C" bfs_status bfs_cluster_grouped(const bfs_cand* d_cands, uint32_t n, c
             static_cast<long long>(fmax) - static_cast<long long>(fmin)));
         const int gbits = bits_for(static_cast<unsigned long long>(groups - 1));
         const int end_bit = fbits + gbits;
+        // after a pass that numbered the groups, a metric at least the field's
+        // whole range (fmax - fmin < 2^fbits) cannot split: sort only
+        const bool sort_only = field > 0 && fbits < 62 &&
+                               static_cast<long long>(metrics[field]) >= (1LL << fbits);
         bfs_status st;
         if (end_bit <= 32)
             st = cluster_pass<unsigned>(d_cands, n, field, fmin, fbits, end_bit,
                                         static_cast<long long>(metrics[field]), gid,
                                         field == 0 && d_group0 == nullptr,
-                                        k_in, k_out, v_in, v_out, flags, scan, tmp, tmp_bytes, s);
+                                        k_in, k_out, v_in, v_out, flags, scan, tmp, tmp_bytes, s, sort_only);
         else
             st = cluster_pass<unsigned long long>(d_cands, n, field, fmin, fbits, end_bit,
                                                   static_cast<long long>(metrics[field]), gid,
                                                   field == 0 && d_group0 == nullptr, k_in, k_out,
                                                   v_in, v_out, flags, scan,
-                                                  tmp, tmp_bytes, s);
+                                                  tmp, tmp_bytes, s, sort_only);
         if (st != BFS_OK) return st;
+        if (sort_only) continue;   // same groups, same boundaries (groups stay in gid order)
         BFS_CUDA(cudaMemcpyAsync(&groups, scan + (n - 1), sizeof(unsigned), cudaMemcpyDeviceToHost, s));
         BFS_CUDA(cudaStreamSynchronize(s));
     }
