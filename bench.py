@@ -110,6 +110,11 @@ class ClockSampler:
         self.proc = subprocess.Popen(
             ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
              "-i", str(self.gpu), "-lms", "200"], stdout=self.tmp, stderr=subprocess.DEVNULL)
+        # let the sampler start up (and print its first line) before the
+        # caller times anything: its start-up competes for the host
+        t0 = time.time()
+        while time.time() - t0 < 3.0 and os.path.getsize(self.tmp.name) == 0:
+            time.sleep(0.05)
         return self
 
     def stop(self) -> dict:
@@ -744,10 +749,10 @@ def run_config1(args):
         ev[3].record()
         return n, cl
 
+    clocks = ClockSampler(0).start()   # started (and settled) before the warm-up
     for _ in range(args.warmup):
         step(raw)
     torch.cuda.synchronize()
-    clocks = ClockSampler(0).start()
     t = {"unpack+fft": 0.0, "coherent+fdmt": 0.0, "search": 0.0}
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()

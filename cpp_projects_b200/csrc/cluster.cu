@@ -51,19 +51,24 @@ __global__ void k_pass_keys(const bfs_cand* __restrict__ c, const unsigned* __re
     vals[i] = i;
 }
 
+// Group starts in the sorted order: the group changes, or the field grows by
+// more than the metric.  A key's low fbits bits are its field minus the
+// smallest field (exact: fbits covers the range), so the sorted keys alone
+// give both tests.
 template <typename K>
-__global__ void k_pass_flags(const bfs_cand* __restrict__ c, const K* __restrict__ keys,
-                             const unsigned* __restrict__ vals, unsigned n, int field, int fbits,
-                             long long metric, unsigned* __restrict__ flags) {
+__global__ void k_pass_flags(const K* __restrict__ keys, unsigned n, int fbits, long long metric,
+                             unsigned* __restrict__ flags) {
     const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     unsigned f = 1u;
     if (i > 0) {
-        const K g0 = fbits >= static_cast<int>(8 * sizeof(K)) ? K(0) : (keys[i - 1] >> fbits);
-        const K g1 = fbits >= static_cast<int>(8 * sizeof(K)) ? K(0) : (keys[i] >> fbits);
+        const bool whole = fbits >= static_cast<int>(8 * sizeof(K));
+        const K k0 = keys[i - 1], k1 = keys[i];
+        const K g0 = whole ? K(0) : (k0 >> fbits);
+        const K g1 = whole ? K(0) : (k1 >> fbits);
         if (g0 == g1) {
-            const long long d = static_cast<long long>(field_of(c[vals[i]], field)) -
-                                static_cast<long long>(field_of(c[vals[i - 1]], field));
+            const K mask = whole ? ~K(0) : ((K(1) << fbits) - K(1));
+            const long long d = static_cast<long long>(k1 & mask) - static_cast<long long>(k0 & mask);
             f = (d > metric) ? 1u : 0u;
         }
     }
@@ -267,7 +272,7 @@ static bfs_status cluster_pass(const bfs_cand* d_cands, unsigned n, int field, i
     BFS_CUDA(cub::DeviceRadixSort::SortPairs(tmp, b, k_in, k_out, v_in, v_out, static_cast<int>(n),
                                              0, end_bit > 0 ? end_bit : 1, s));
     if (sort_only) return BFS_OK;
-    k_pass_flags<K><<<bl, th, 0, s>>>(d_cands, k_out, v_out, n, field, fbits, metric, flags);
+    k_pass_flags<K><<<bl, th, 0, s>>>(k_out, n, fbits, metric, flags);
     BFS_LAUNCH_CHECK("k_pass_flags");
     b = tmp_bytes;
     BFS_CUDA(cub::DeviceScan::InclusiveSum(tmp, b, flags, scan, static_cast<int>(n), s));
