@@ -356,7 +356,11 @@ extern "C" bfs_status bfs_chunk_detect(bfs_chunk* c, const void* d_volt, double 
 extern "C" bfs_status bfs_chunk_unpack_fft(bfs_chunk* c, const int8_t* d_raw, void* d_spec, void* stream) {
     BFS_ARG(c && d_raw && d_spec, "null argument");
     const bfs_chunk_desc& d = c->d;
-    if (fft_fused_supported(d.nbin, d.npol))
+    // the fused transform reads whole samples (npol bytes) as one word and
+    // writes float2s: it needs the raw chunk npol-aligned and d_spec 8-aligned
+    const bool aligned = (reinterpret_cast<uintptr_t>(d_raw) % d.npol) == 0 &&
+                         (reinterpret_cast<uintptr_t>(d_spec) % sizeof(float2)) == 0;
+    if (aligned && fft_fused_supported(d.nbin, d.npol))
         return fft_forward_guppi(reinterpret_cast<const signed char*>(d_raw), c->volt, static_cast<float2*>(d_spec),
                                  c->len_chunk, d.noverlap, d.nfft, d.nchan, d.npol, as_stream(stream));
     bfs_status st = bfs_chunk_unpack(c, d_raw, d_spec, stream);

@@ -449,8 +449,11 @@ bfs_status bfs_chunk_process(bfs_chunk* chunk, void* d_cplx, const double* dms, 
  * (complex values per buffer, bfs_chunk_info[6]) receives the spectra of every
  * segment.  For nbin = 2^20 a four-step transform whose first pass reads the
  * int8 samples directly (no complex copy of the chunk); it agrees with
- * bfs_chunk_unpack + bfs_chunk_forward_fft to FP32 rounding.  Other sizes run
- * those two.  Uses the chunk's voltage buffer as scratch. */
+ * bfs_chunk_unpack + bfs_chunk_forward_fft to FP32 rounding.  Other sizes (or a
+ * d_raw not aligned to npol bytes, a d_spec not aligned to 8) run those two.
+ * Uses the chunk's voltage buffer as scratch.  The first call on a device
+ * builds the transform's twiddle tables (allocates, synchronous; kept until
+ * exit): make it before any stream capture. */
 bfs_status bfs_chunk_unpack_fft(bfs_chunk* chunk, const int8_t* d_raw, void* d_spec, void* stream);
 /* The per-DM part of CChunkB::process (Chunk_gpu.cu:284-359) on spectra from
  * bfs_chunk_unpack_fft or bfs_chunk_forward_fft: d_spec is not modified. */

@@ -148,3 +148,20 @@ def test_unpack_fft_other_sizes_use_unpack_and_cufft(cuda):
     ch.unpack(d_raw, b)
     ch.forward_fft(b)
     assert torch.equal(a, b)
+
+
+@pytest.mark.gpu
+def test_unpack_fft_misaligned_raw_takes_the_unpack_path(cuda):
+    """A raw chunk that does not start on a sample (npol-byte) boundary cannot
+    be read as whole words: the call falls back to unpack + cuFFT."""
+    ch, g = _chunk(GEO), co.Geometry(**GEO)
+    raw = _raw(g, 15)
+    buf = torch.zeros(raw.size + 8, dtype=torch.int8, device=cuda)
+    d_raw = buf[1:1 + raw.size].view(raw.shape)
+    d_raw.copy_(torch.from_numpy(raw).to(cuda))
+    assert d_raw.data_ptr() % g.npol != 0
+    a, b = ch.complex_buffer(cuda), ch.complex_buffer(cuda)
+    ch.unpack_fft(d_raw, a)
+    ch.unpack(d_raw, b)
+    ch.forward_fft(b)
+    assert torch.equal(a, b)
