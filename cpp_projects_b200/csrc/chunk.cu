@@ -124,7 +124,7 @@ constexpr int kDetectCols = 4;
 __global__ void __launch_bounds__(kDetectThreads)
 k_detect(const float2* __restrict__ volt, float* __restrict__ plane, int nchan, int len_sft, int mbin,
          int nbin, int nfft, int npol2, int nov_pc, int mbin_adj, int msamp, const int* __restrict__ shift,
-         double inv_nbin2) {
+         double inv_nbin2, int vec_store) {
     const int r = blockIdx.y;
     const int c = (blockIdx.x * kDetectThreads + threadIdx.x) * kDetectCols;
     if (c >= msamp) return;
@@ -171,7 +171,7 @@ k_detect(const float2* __restrict__ volt, float* __restrict__ plane, int nchan, 
         }
     }
     float* o = plane + static_cast<size_t>(r) * msamp + c;
-    if ((msamp & 3) == 0) {   // c is a multiple of 4: the row offset keeps 16-byte alignment
+    if (vec_store) {   // 16-byte aligned plane, msamp % 4 == 0: every row offset keeps the alignment
         *reinterpret_cast<float4*>(o) = make_float4(acc[0], acc[1], acc[2], acc[3]);
     } else {
 #pragma unroll
@@ -179,6 +179,9 @@ k_detect(const float2* __restrict__ volt, float* __restrict__ plane, int nchan, 
             if (c + j < msamp) o[j] = acc[j];
     }
 }
+
+// Complex buffers are read and written as float2: 8-byte alignment.
+bool cplx_aligned(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 7) == 0; }
 
 bfs_status cufft_check(cufftResult r, const char* what) {
     if (r == CUFFT_SUCCESS) return BFS_OK;
@@ -266,6 +269,7 @@ extern "C" bfs_status bfs_chunk_info(const bfs_chunk* c, int64_t* info, int cap)
 
 extern "C" bfs_status bfs_chunk_unpack(bfs_chunk* c, const int8_t* d_raw, void* d_cplx, void* stream) {
     BFS_ARG(c && d_raw && d_cplx, "null argument");
+    BFS_ARG(cplx_aligned(d_cplx), "d_cplx must be 8-byte aligned");
     const bfs_chunk_desc& d = c->d;
     dim3 grid((d.nbin + 255) / 256, d.nfft, d.nchan);
     BFS_ARG(grid.y <= 65535 && grid.z <= 65535, "too many segments or channels");
@@ -278,6 +282,7 @@ extern "C" bfs_status bfs_chunk_unpack(bfs_chunk* c, const int8_t* d_raw, void* 
 
 extern "C" bfs_status bfs_chunk_forward_fft(bfs_chunk* c, void* d_cplx, void* stream) {
     BFS_ARG(c && d_cplx, "null argument");
+    BFS_ARG(cplx_aligned(d_cplx), "d_cplx must be 8-byte aligned");
     bfs_status st = cufft_check(cufftSetStream(c->fwd, as_stream(stream)), "cufftSetStream");
     if (st != BFS_OK) return st;
     return cufft_check(cufftExecC2C(c->fwd, static_cast<cufftComplex*>(d_cplx),
@@ -308,6 +313,7 @@ static bfs_status chunk_voltages(bfs_chunk* c, const void* d_spec, double dm, fl
 extern "C" bfs_status bfs_chunk_voltages(bfs_chunk* c, const void* d_spec, double dm, void* d_volt,
                                          void* stream) {
     BFS_ARG(c && d_spec && d_volt, "null argument");
+    BFS_ARG(cplx_aligned(d_spec) && cplx_aligned(d_volt), "d_spec and d_volt must be 8-byte aligned");
     return chunk_voltages(c, d_spec, dm, static_cast<float2*>(d_volt), as_stream(stream));
 }
 
@@ -339,8 +345,10 @@ static bfs_status chunk_detect(bfs_chunk* c, const float2* d_volt, double dm, fl
     BFS_ARG(d.npol / 2 <= 2, "at most two polarisations");
     const bool pow2 = (d.nbin & (d.nbin - 1)) == 0;
     const double inv_nbin2 = pow2 ? 1.0 / (static_cast<double>(d.nbin) * d.nbin) : 0.0;  // exact for 2^k
+    const int vec_store = (c->msamp % 4 == 0) && (reinterpret_cast<uintptr_t>(d_plane) & 15) == 0;
     k_detect<<<grid, kDetectThreads, 0, s>>>(d_volt, d_plane, d.nchan, d.len_sft, c->mbin, d.nbin, d.nfft,
-                                  d.npol / 2, c->nov_pc, c->mbin_adj, c->msamp, c->d_shift, inv_nbin2);
+                                  d.npol / 2, c->nov_pc, c->mbin_adj, c->msamp, c->d_shift, inv_nbin2,
+                                  vec_store);
     BFS_LAUNCH_CHECK("k_detect");
     // the host vector must outlive the (pageable, staged) copy: wait for it
     BFS_CUDA(cudaStreamSynchronize(s));
@@ -350,11 +358,13 @@ static bfs_status chunk_detect(bfs_chunk* c, const float2* d_volt, double dm, fl
 extern "C" bfs_status bfs_chunk_detect(bfs_chunk* c, const void* d_volt, double dm, float* d_plane,
                                        void* stream) {
     BFS_ARG(c && d_volt && d_plane, "null argument");
+    BFS_ARG(cplx_aligned(d_volt), "d_volt must be 8-byte aligned");
     return chunk_detect(c, static_cast<const float2*>(d_volt), dm, d_plane, as_stream(stream));
 }
 
 extern "C" bfs_status bfs_chunk_unpack_fft(bfs_chunk* c, const int8_t* d_raw, void* d_spec, void* stream) {
     BFS_ARG(c && d_raw && d_spec, "null argument");
+    BFS_ARG(cplx_aligned(d_spec), "d_spec must be 8-byte aligned");
     const bfs_chunk_desc& d = c->d;
     // the fused transform reads whole samples (npol bytes) as one word and
     // writes float2s: it needs the raw chunk npol-aligned and d_spec 8-aligned
@@ -398,6 +408,7 @@ static bfs_status chunk_dm_loop(bfs_chunk* c, const void* d_cplx, const double* 
 extern "C" bfs_status bfs_chunk_process(bfs_chunk* c, void* d_cplx, const double* dms, int ndm,
                                         float* d_out, void* stream) {
     BFS_ARG(c && d_cplx && d_out && (ndm == 0 || dms), "null argument");
+    BFS_ARG(cplx_aligned(d_cplx), "d_cplx must be 8-byte aligned");
     bfs_status st = bfs_chunk_forward_fft(c, d_cplx, stream);
     if (st != BFS_OK) return st;
     return chunk_dm_loop(c, d_cplx, dms, ndm, d_out, stream);
@@ -406,12 +417,14 @@ extern "C" bfs_status bfs_chunk_process(bfs_chunk* c, void* d_cplx, const double
 extern "C" bfs_status bfs_chunk_process_spectrum(bfs_chunk* c, const void* d_spec, const double* dms, int ndm,
                                                  float* d_out, void* stream) {
     BFS_ARG(c && d_spec && d_out && (ndm == 0 || dms), "null argument");
+    BFS_ARG(cplx_aligned(d_spec), "d_spec must be 8-byte aligned");
     return chunk_dm_loop(c, d_spec, dms, ndm, d_out, stream);
 }
 
 extern "C" bfs_status bfs_chunk_process_raw(bfs_chunk* c, const int8_t* d_raw, void* d_spec, const double* dms,
                                             int ndm, float* d_out, void* stream) {
     BFS_ARG(c && d_raw && d_spec && d_out && (ndm == 0 || dms), "null argument");
+    BFS_ARG(cplx_aligned(d_spec), "d_spec must be 8-byte aligned");
     bfs_status st = bfs_chunk_unpack_fft(c, d_raw, d_spec, stream);
     if (st != BFS_OK) return st;
     return chunk_dm_loop(c, d_spec, dms, ndm, d_out, stream);
