@@ -36,6 +36,57 @@ def _raw(seed=3):
                                                 dtype=np.int8)
 
 
+@pytest.mark.parametrize("nbin,len_sft,noverlap,nfft,nchan", [
+    (64, 8, 8, 3, 2),      # mbin 8, mbin_adj 6, msamp 18 (not a multiple of 4)
+    (32, 8, 8, 5, 3),      # mbin_adj 2: several (ifft, ibin) carries per thread
+    (4096, 8, 64, 2, 2),   # the GPU tests' geometry
+    (16, 4, 4, 7, 1),      # mbin_adj 2, msamp 14
+])
+def test_detect_gather_column_stepping_matches_direct_indexing(nbin, len_sft, noverlap, nfft, nchan):
+    """k_detect gives each thread 4 consecutive output columns and steps the
+    source column with single carries (idx wraps at msamp, ibin at mbin_adj,
+    q at nbin); emulated here against the direct formula for every column,
+    with shifts of both signs, and every source index checked in bounds."""
+    cols_per_thread = 4
+    mbin = nbin // len_sft
+    nov_pc = noverlap // len_sft
+    mbin_adj = mbin - 2 * nov_pc
+    msamp = nfft * mbin_adj
+    rows = nchan * len_sft
+    npol2 = 2
+    volt_len = npol2 * nfft * nchan * nbin
+    pol_stride = nfft * nchan * nbin
+    rng = np.random.default_rng(nbin + nfft)
+    shifts = rng.integers(-3 * msamp, 3 * msamp, size=rows)
+    for r in range(rows):
+        isub, ifine = r // len_sft, len_sft - 1 - (r % len_sft)
+        coarse = nchan - 1 - isub
+        q0 = ifine * mbin + nov_pc + nbin // 2
+        q0 = q0 - nbin if q0 >= nbin else q0
+        for c in range(0, msamp, cols_per_thread):
+            idx = int(np.fmod(c - shifts[r], msamp))   # C remainder, sign of the dividend
+            if idx < 0:
+                idx += msamp
+            ifft, ibin = idx // mbin_adj, idx % mbin_adj
+            for j in range(cols_per_thread):
+                q = q0 + ibin
+                q = q - nbin if q >= nbin else q
+                if c + j < msamp:
+                    d = (c + j - shifts[r]) % msamp
+                    want = (d // mbin_adj * nchan + coarse) * nbin + \
+                        (ifine * mbin + d % mbin_adj + nov_pc + nbin // 2) % nbin
+                    base = (ifft * nchan + coarse) * nbin + q
+                    assert base == want
+                    assert 0 <= base and base + (npol2 - 1) * pol_stride < volt_len
+                idx += 1
+                if idx == msamp:
+                    idx, ifft, ibin = 0, 0, 0
+                else:
+                    ibin += 1
+                    if ibin == mbin_adj:
+                        ibin, ifft = 0, ifft + 1
+
+
 def test_coherent_dm_grid_matches_reference_rule():
     # CChunkB: step = d_max / ncoherent, count = (int)((d_max - d_min) / step)
     assert list(coherent_dms(0.0, 100.0, 4)) == [0.0, 25.0, 50.0, 75.0]
