@@ -1,9 +1,12 @@
 """CPU: the search oracle reproduces the reference's golden candidate lists
-(clusterization_forpravir/Candidates{1,2}.csv) and its clustering rules."""
+(clusterization_forpravir/Candidates{1,2}.csv) and its clustering rules; the
+boxcar kernel's register-window schedule is checked for every width set."""
 import json
+import re
 from pathlib import Path
 
 import numpy as np
+import pytest
 
 from oracle import pyoracle
 
@@ -76,3 +79,28 @@ def test_oracle_boxcar_truncated_windows_and_edges():
     # w=4 only fits from t=0,1; w=8 never
     assert (0, 2) in widths and (1, 2) in widths and (2, 2) not in widths
     assert not any(w == 3 for _, w in widths)
+
+
+@pytest.mark.parametrize("wmax", [1, 2, 3, 4, 5, 6, 7, 8, 16, 32, 64, 128])
+def test_boxcar_sliding_window_schedule(wmax):
+    """k_boxcar_reg's register window: with S starts per thread, step w reads
+    window values w-1 .. w+S-2; the first S/4 float4s are loaded up front and
+    the vector starting at value w+S-2 at step w.  Every value must be loaded
+    before the step that first reads it, and every float4 read of the thread
+    with the highest start must stay inside the tile of kRegTile + 4 ceil((W-1)/4)
+    values."""
+    src = (Path(__file__).resolve().parent.parent / "cpp_projects_b200" / "csrc" / "search.cu").read_text()
+    S = int(re.search(r"constexpr int kRegStarts = (\d+);", src).group(1))
+    threads = int(re.search(r"constexpr int kRegThreads = (\d+);", src).group(1))
+    vec = (S + wmax - 1 + 3) // 4
+    span = threads * S + 4 * ((wmax - 1 + 3) // 4)
+    loaded = set(range(S))
+    for w in range(1, wmax + 1):
+        b = w + S - 2
+        if b % 4 == 0 and b // 4 >= S // 4 and b // 4 < vec:
+            loaded |= set(range(b, b + 4))
+        assert set(range(w - 1, w + S - 1)) <= loaded, (w, sorted(loaded))
+    last_vec = max([S // 4 - 1] + [(w + S - 2) // 4 for w in range(1, wmax + 1)
+                                    if (w + S - 2) % 4 == 0 and (w + S - 2) // 4 < vec])
+    top = (threads - 1) * (S // 4) + last_vec       # float4 index of the highest read
+    assert 4 * top + 3 < span
