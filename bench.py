@@ -81,14 +81,23 @@ def measured_peaks():
 
 
 def beams_for(workload: str, rank: int):
+    """The workload's beams for one rank: every rank gets the same shapes
+    (weak scaling: fixed work per GPU) with its own noise (another data seed
+    per rank)."""
+    import dataclasses
+
     from cpp_projects_b200 import synth
     if workload == "config0":
-        return [synth.config0(seed=1 + rank)]
-    if workload == "config4fwd":
-        return [synth.config4(seed=4 + rank)]
-    if workload == "config3":
-        return [synth.config3(seed=3 + rank)]
-    return synth.config2(seed=2 + 1000 * rank)
+        beams = [synth.config0(seed=1)]
+    elif workload == "config4fwd":
+        beams = [synth.config4(seed=4)]
+    elif workload == "config3":
+        beams = [synth.config3(seed=3)]
+    else:
+        beams = synth.config2(seed=2)
+    if rank:
+        beams = [dataclasses.replace(b, seed=b.seed + 1_000_003 * rank) for b in beams]
+    return beams
 
 
 # ---------------------------------------------------------------------------
@@ -264,7 +273,6 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 def run_ours(args):
     import torch
-    import torch.distributed as dist
 
     from cpp_projects_b200.pipeline import BatchedSearch, BeamShape, SearchPipeline, device_filterbank
 
@@ -276,10 +284,8 @@ def run_ours(args):
         return 1
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=dev)
+    from cpp_projects_b200.ranks import Ranks
+    ranks = Ranks("nccl", dev)
     if args.warmup < 3:
         args.warmup = 3  # the timing rules require >= 3 warm-up steps
 
@@ -298,16 +304,8 @@ def run_ours(args):
               for b in beams]
     torch.cuda.synchronize()
 
-    def barrier():
-        if world > 1:
-            dist.barrier(device_ids=[local])
-
-    def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = ranks.barrier
+    max_over_ranks = ranks.max
 
     # ---- device-resident timing: plain per-beam form -------------------------
     plain = args.form == "both"
@@ -447,8 +445,7 @@ def run_ours(args):
             "candidates": ncand, "delegates": ndel,
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 
