@@ -67,7 +67,13 @@ def complete_clusterization(cands: torch.Tensor, metrics, stream=None) -> Cluste
 
 
 def select_delegates(cands, perm, offsets, stream=None) -> torch.Tensor:
+    """Per-group argmax of msnr; perm and offsets as ``clusterization_main``
+    returns them (one perm entry per candidate, ngroups + 1 offsets)."""
     ng = int(offsets.shape[0]) - 1
+    if ng < 0:
+        raise ValueError("offsets needs at least one entry")
+    if perm.shape[0] != cands.shape[0]:
+        raise ValueError(f"perm has {perm.shape[0]} entries for {cands.shape[0]} candidates")
     out = torch.empty(max(ng, 1), dtype=torch.int32, device=cands.device)
     _capi.call("bfs_select_delegates", dev_ptr(cands, torch.int32), dev_ptr(perm, torch.int32),
                ctypes.c_uint32(int(cands.shape[0])), dev_ptr(offsets, torch.int32),

@@ -218,7 +218,7 @@ __global__ void k_snr_cells(const float* __restrict__ plane, int rows, int cols,
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const int d = cells[3 * k], t = cells[3 * k + 1], w = cells[3 * k + 2];
-    if (d < 0 || d >= rows || t < 0 || w < 1 || t + w > cols) { snr[k] = __int_as_float(0x7fc00000); return; }
+    if (d < 0 || d >= rows || t < 0 || w < 1 || w > cols - t) { snr[k] = __int_as_float(0x7fc00000); return; }
     const float m = stats[d], sd = stats[rows + d];
     const float* x = plane + static_cast<size_t>(d) * cols + t;
     float sum = 0.0f;

@@ -159,6 +159,7 @@ extern "C" bfs_status bfs_batch_create(const bfs_batch_desc* desc, bfs_batch** o
     b->thr = desc->thr;
     for (int i = 0; i < 3; ++i) b->metrics[i] = desc->metrics[i];
     b->capacity = desc->capacity ? desc->capacity : (1u << 26);
+    BFS_ARG(b->capacity < 0x7fffffffu, "capacity %u too large", b->capacity);
     b->use_graph = desc->use_graph != 0;
     size_t plane = 0;
     for (const bfs_fdmt_desc& d0 : b->beams) {

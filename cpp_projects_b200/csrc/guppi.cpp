@@ -233,6 +233,7 @@ extern "C" bfs_status bfs_guppi_read_chunk(const bfs_guppi_file* g, int block, i
                                            size_t dst_bytes) {
     BFS_ARG(g != nullptr && dst != nullptr, "null argument");
     BFS_ARG(block >= 0 && block < static_cast<int>(g->blocks.size()), "block %d out of range", block);
+    BFS_ARG(len_chunk > 2 * noverlap && noverlap >= 0, "need len_chunk > 2 * noverlap >= 0");
     const bfs_guppi_header& h = g->blocks[block];
     BFS_ARG(dst_bytes >= static_cast<size_t>(h.nchan) * len_chunk * h.npol,
             "dst holds %zu bytes, the chunk needs %lld", dst_bytes,

@@ -574,6 +574,7 @@ extern "C" bfs_status bfs_row_stats(const float* d_in, int rows, int cols, float
 extern "C" bfs_status bfs_norm_rows(const float* d_in, float* d_out, int rows, int cols,
                                     float* d_stats, void* stream) {
     BFS_ARG(d_in && d_out, "null argument");
+    BFS_ARG(rows >= 1 && cols >= 1 && rows <= 65535, "bad shape %dx%d", rows, cols);
     cudaStream_t s = as_stream(stream);
     float* stats = d_stats;
     if (!stats) BFS_TRY_ST(stream_alloc(reinterpret_cast<void**>(&stats), sizeof(float) * 2 * rows, s));

@@ -275,7 +275,11 @@ bfs_status bfs_cluster(const bfs_cand* d_cands, uint32_t n, const int* metrics /
 bfs_status bfs_cluster_grouped(const bfs_cand* d_cands, uint32_t n, const int* d_group0,
                                uint32_t ngroups0, const int* metrics, int* d_perm, int* d_offsets,
                                int* d_delegates, uint32_t* h_ngroups, void* stream);
-/* The reference's per-group argmax on its own (select_delegates_kernel). */
+/* The reference's per-group argmax on its own (select_delegates_kernel).
+ * The device arrays are read as bfs_cluster writes them and are not checked:
+ * d_offsets holds ngroups + 1 non-decreasing entries from 0 to n, and every
+ * d_perm entry is an index into d_cands (0..n-1).  Other contents read
+ * outside the arrays. */
 bfs_status bfs_select_delegates(const bfs_cand* d_cands, const int* d_perm, uint32_t n,
                                 const int* d_offsets, uint32_t ngroups, int* d_delegates,
                                 void* stream);

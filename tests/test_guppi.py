@@ -94,3 +94,17 @@ def test_rejections(tmp_path):
     data = path.read_bytes()
     path.write_bytes(data[:-100])
     assert guppi.GuppiFile(path).nblocks == 1
+
+
+def test_read_chunk_rejects_bad_chunking(tmp_path):
+    path = tmp_path / "d.raw"
+    synth.write_guppi(path, _blocks(4, n=1), 1400.0, 16.0, 2.5e-7)
+    f = guppi.GuppiFile(path)
+    with pytest.raises(BfsError):
+        f.read_chunk(0, 0, 1000, -1)           # negative overlap
+    with pytest.raises(BfsError):
+        f.read_chunk(0, 0, 200, 100)           # len_chunk <= 2 * noverlap
+    with pytest.raises(BfsError):
+        f.read_chunk(0, 10 ** 6, 1000, 100)    # chunk past the block
+    with pytest.raises(BfsError):
+        f.read_chunk(1, 0, 1000, 100)          # block past the file
