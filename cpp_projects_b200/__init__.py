@@ -14,6 +14,9 @@ hot path, calling hand-written sm_100a CUDA through the C ABI in
 * :mod:`.preproc` — ``statistical_preprocessing::calc_fdmt_inputs``,
   ``fdmt_normalization``
 * :mod:`.chunk` — ``CChunk_gpu`` coherent-dedispersion stage
+* :mod:`.guppi` — GUPPI RAW headers, chunk reads, streaming reader
+* :mod:`.session` — ``CSession_guppi_gpu`` (``CSessionB::launch``): a GUPPI
+  file through the chunk stage and the candidate search
 * :mod:`.pipeline` — per-beam and batched (CUDA-graph) search
 * :mod:`.autograd` — differentiable FDMT + boxcar S/N
 """

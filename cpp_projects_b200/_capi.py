@@ -67,6 +67,13 @@ class GuppiHeader(ctypes.Structure):
                 ("reserved", ctypes.c_int * 4)]
 
 
+class GuppiSession(ctypes.Structure):
+    _fields_ = [("len_sft", ctypes.c_int), ("noverlap", ctypes.c_int), ("len_chunk", ctypes.c_int64),
+                ("ncoherent", ctypes.c_int), ("optimal_overlap", ctypes.c_int), ("fmin", ctypes.c_float),
+                ("fmax", ctypes.c_float), ("tsamp", ctypes.c_float), ("d_min", ctypes.c_float),
+                ("d_max", ctypes.c_float), ("reserved", ctypes.c_int * 4)]
+
+
 class Cand(ctypes.Structure):
     _fields_ = [("mt", ctypes.c_int), ("mdt", ctypes.c_int), ("mwidth", ctypes.c_int),
                 ("msnr", ctypes.c_float)]
@@ -128,6 +135,7 @@ _SIGNATURES = {
     "bfs_guppi_reader_next": (_I, [_P, _P, _P, ctypes.POINTER(_P), ctypes.POINTER(_I),
                                    ctypes.POINTER(ctypes.c_int64)]),
     "bfs_guppi_reader_destroy": (_I, [_P]),
+    "bfs_guppi_session_plan": (_I, [_P, ctypes.c_float, ctypes.c_double, ctypes.c_double, _I, _I, _P]),
     "bfs_batch_create": (_I, [ctypes.POINTER(BatchDesc), ctypes.POINTER(_P)]),
     "bfs_batch_destroy": (_I, [_P]),
     "bfs_batch_run": (_I, [_P, _P, _P]),

@@ -67,6 +67,8 @@ class CChunk_gpu:
     def get_noverlap_per_channel(self): return self.noverlap_per_channel
     def get_mbin_adjusted(self): return self.mbin_adjusted
     def get_msamp(self): return self.msamp
+    def set_blockid(self, nC): self.m_Block_id = int(nC)
+    def set_chunkid(self, nC): self.m_Chunk_id = int(nC)
 
     def complex_buffer(self, device) -> torch.Tensor:
         return torch.empty((self.cplx_len, 2), dtype=torch.float32, device=device)

@@ -415,3 +415,73 @@ extern "C" bfs_status bfs_guppi_reader_next(bfs_guppi_reader* r, void* d_dst, vo
     r->last = id;
     return BFS_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Session geometry (CSessionB::launch, MyVSLib_C++/CDMT/SessionB.cpp:144-160
+// and 184-206, with get_optimal_overlap :384-392 and get_coherent_dms
+// :395-401).  The arithmetic keeps the reference's types: float header
+// fields and float products, double dispersion constants, C rounding.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr double kDispersion = 4.148808e3;  // MHz^2 pc^-1 cm^3 s, the session's constant
+
+// Dispersion delay (s) between f_lo and f_hi at dm: the squares are float
+// products, the reciprocals and the rest double, the result stored as float.
+float session_delay(double dm, float f_lo, float f_hi) {
+    const float lo2 = f_lo * f_lo;
+    const float hi2 = f_hi * f_hi;
+    return static_cast<float>(kDispersion * dm * (1.0 / static_cast<double>(lo2) - 1.0 / static_cast<double>(hi2)));
+}
+
+}  // namespace
+
+extern "C" bfs_status bfs_guppi_session_plan(const bfs_guppi_header* h, float pulse_length, double d_min,
+                                             double d_max, int nbin, int nfft, bfs_guppi_session* out) {
+    BFS_ARG(h != nullptr && out != nullptr, "null argument");
+    *out = bfs_guppi_session{};
+    BFS_ARG(std::isfinite(pulse_length) && pulse_length > 0.0f, "pulse length must be positive");
+    BFS_ARG(std::isfinite(h->tbin) && h->tbin > 0.0f, "TBIN must be positive");
+    BFS_ARG(h->nchan >= 1 && h->obsbw > 0.0f && std::isfinite(h->obsbw), "bad band in the header");
+    BFS_ARG(nbin >= 2 && nfft >= 1, "need nbin >= 2 and nfft >= 1");
+    BFS_ARG(std::isfinite(d_max) && d_max > 0.0 && std::isfinite(d_min), "need a positive finite d_max");
+    const float fmin = static_cast<float>(static_cast<double>(h->obsfreq) - std::fabs(h->obsbw) / 2.0);
+    const float fmax = static_cast<float>(static_cast<double>(h->obsfreq) + std::fabs(h->obsbw) / 2.0);
+    BFS_ARG(fmin > 0.0f && fmax > fmin, "band edges %g..%g MHz", fmin, fmax);
+    BFS_ARG(static_cast<float>(d_min) <= static_cast<float>(d_max), "d_min above d_max");
+
+    // fine channels per coarse channel: the pulse length in samples
+    const float np = std::ceil(pulse_length / h->tbin);
+    BFS_ARG(np >= 1.0f && np <= 1048576.0f, "pulse length gives %g fine channels", np);
+    const int len_sft = static_cast<int>(np);
+
+    // overlap: half the delay across the lowest fine channel at d_max,
+    // rounded to a power of two
+    const float bw_chan = std::fabs(h->obsbw) / static_cast<float>(h->nchan * len_sft);
+    const float f_top = fmin + bw_chan;
+    const float delay_samples = std::round(session_delay(d_max, fmin, f_top) / h->tbin);
+    BFS_ARG(std::isfinite(delay_samples) && delay_samples >= 0.0f && delay_samples < 2147483648.0f,
+            "overlap of %g samples", delay_samples);
+    const int optimal = static_cast<int>(delay_samples);
+    const int half = optimal / 2;
+    const int noverlap = half > 0 ? static_cast<int>(std::pow(2.0, std::round(std::log2(static_cast<double>(half)))))
+                                  : 0;
+    BFS_ARG(2LL * noverlap < nbin, "nbin must be greater than %d", 2 * noverlap);
+
+    // coherent DMs: the whole band's delay at d_max in units of t_p^2 / tbin
+    const float t_d = session_delay(d_max, fmin, fmax);
+    const float ncoh = std::ceil(t_d * h->tbin / (pulse_length * pulse_length));
+    BFS_ARG(ncoh >= 1.0f && ncoh <= 1048576.0f, "%g coherent DMs", ncoh);
+
+    out->len_sft = len_sft;
+    out->noverlap = noverlap;
+    out->len_chunk = static_cast<int64_t>(nbin - 2 * noverlap) * nfft;
+    out->ncoherent = static_cast<int>(ncoh);
+    out->optimal_overlap = optimal;
+    out->fmin = fmin;
+    out->fmax = fmax;
+    out->tsamp = h->tbin;
+    out->d_min = static_cast<float>(d_min);
+    out->d_max = static_cast<float>(d_max);
+    return BFS_OK;
+}

@@ -32,6 +32,21 @@ def parse_header(text: bytes) -> dict:
     return _header_dict(h)
 
 
+def session_plan(header: dict, t_p: float, d_min: float, d_max: float, nbin: int, nfft: int) -> dict:
+    """Chunk geometry of a session (CSessionB::launch, SessionB.cpp:144-160,
+    184-206, 384-401) from a block header as ``GuppiFile.header`` or
+    ``parse_header`` return it: len_sft, noverlap, len_chunk, ncoherent,
+    optimal_overlap, fmin, fmax, tsamp, d_min, d_max."""
+    h = _capi.GuppiHeader()
+    for k, _ in h._fields_:
+        if k != "reserved":
+            setattr(h, k, header[k])
+    out = _capi.GuppiSession()
+    _capi.call("bfs_guppi_session_plan", ctypes.byref(h), float(t_p), float(d_min), float(d_max),
+               int(nbin), int(nfft), ctypes.byref(out))
+    return {k: getattr(out, k) for k, _ in out._fields_ if k != "reserved"}
+
+
 class GuppiFile:
     def __init__(self, path: str):
         self.path = str(path)

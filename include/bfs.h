@@ -393,6 +393,33 @@ bfs_status bfs_guppi_reader_next(bfs_guppi_reader* reader, void* d_dst, void* st
                                  const int8_t** h_src, int* block, int64_t* chunk);
 bfs_status bfs_guppi_reader_destroy(bfs_guppi_reader* reader);
 
+/* Chunk geometry of a GUPPI session, as CSessionB::launch derives it from the
+ * first block's header, the pulse length t_p (s), the DM range, nbin and nfft
+ * (L/CDMT/SessionB.cpp:144-160,184-206; get_optimal_overlap :384-392;
+ * get_coherent_dms :395-401), in the reference's float/double arithmetic:
+ *   len_sft   = ceil(t_p / TBIN)
+ *   optimal   = round(delay(d_max, fmin, fmin + OBSBW/(OBSNCHAN len_sft)) / TBIN)
+ *   noverlap  = 2^round(log2(optimal / 2))  (0 when optimal / 2 is 0)
+ *   len_chunk = (nbin - 2 noverlap) nfft
+ *   ncoherent = ceil(delay(d_max, fmin, fmax) TBIN / t_p^2)
+ * with delay(dm, a, b) = 4.148808e3 dm (1/a^2 - 1/b^2) s, a and b in MHz.
+ * d_min / d_max are returned as the chunk receives them (float).  Errors
+ * where the reference would divide by zero or run a chunk of negative length
+ * (d_max <= 0, 2 noverlap >= nbin). */
+typedef struct bfs_guppi_session {
+    int len_sft;          /* fine channels per coarse channel                    */
+    int noverlap;         /* overlap-save samples on each side of a segment      */
+    int64_t len_chunk;    /* samples per channel in one chunk                    */
+    int ncoherent;        /* coherent-DM count handed to the chunk               */
+    int optimal_overlap;  /* get_optimal_overlap(len_sft), samples               */
+    float fmin, fmax;     /* band edges handed to the chunk (MHz)                */
+    float tsamp;          /* TBIN (s)                                            */
+    float d_min, d_max;   /* DM range as the chunk receives it                   */
+    int reserved[4];
+} bfs_guppi_session;
+bfs_status bfs_guppi_session_plan(const bfs_guppi_header* header, float pulse_length, double d_min,
+                                  double d_max, int nbin, int nfft, bfs_guppi_session* out);
+
 /* ------------------------------------------------------------------------
  * Coherent-dedispersion chunk stage.
  * Replaces CSession_guppi_gpu::unpack_chunk (L/CDMT/Session_guppi_gpu.cu:53-60,

@@ -309,3 +309,244 @@ inline bool clusterization_main(const float* d_digitized_fdmt, const int Rows, c
 }
 
 }  // namespace clusterization
+
+// ---------------------------------------------------------------------------
+// Coherent-dedispersion chunk and the GUPPI session driver.
+//
+//   CChunkB              L/CDMT/ChunkB.h:8-114 (geometry, DM grid ChunkB.cpp:171-176)
+//   CChunk_gpu           L/CDMT/Chunk_gpu.cuh:16-72, Chunk_gpu.cu:254-460
+//   CSession_guppi_gpu   L/CDMT/Session_guppi_gpu.cuh:9-39, SessionB.cpp:106-300
+//
+// CChunk_gpu::process takes the unpacked complex chunk (overwritten by the
+// forward FFT), makes one normalised FDMT plane (len_sft x msamp) per
+// coherent DM, runs clusterization_main on all of them (every width 1..4,
+// threshold sigma_bound, splitters {2, 1, 2}, delegate log "candidates.log",
+// delt_bin = tsamp * len_sft) and copies the planes to pvecImg, as the
+// reference does.  The reference's discarded gather_candidates_in_
+// dynamicalArray call and its unused success headers are left out.
+// CSession_guppi_gpu::launch derives the chunk geometry from the first
+// block's header (bfs_guppi_session_plan), streams every chunk of every block
+// through pinned buffers to the device and calls CChunk_gpu::process_raw
+// (unpack and forward FFT fused); it returns 0, or -1 on an error (the value
+// the reference's drivers test for).
+// ---------------------------------------------------------------------------
+class CChunkB {
+public:
+    CChunkB() = default;
+    CChunkB(const float Fmin, const float Fmax, const int npol, const int nchan, const unsigned int len_sft,
+            const int Block_id, const int Chunk_id, const double d_max, const double d_min, const int ncoherent,
+            const float sigma_bound, const int length_sum_wnd, const int nbin, const int nfft,
+            const int noverlap, const float tsamp)
+        : m_Fmin(Fmin), m_Fmax(Fmax), m_npol(npol), m_nchan(nchan), m_len_sft(len_sft), m_tsamp(tsamp),
+          m_Chunk_id(Chunk_id), m_Block_id(Block_id), m_d_max(d_max), m_d_min(d_min), m_ncoherent(ncoherent),
+          m_sigma_bound(sigma_bound), m_length_sum_wnd(length_sum_wnd), m_nbin(nbin), m_nfft(nfft),
+          m_noverlap(noverlap) {
+        const int n = bfs_chunk_coherent_dms(d_min, d_max, ncoherent, nullptr, 0);
+        m_coh_dm_Vector.resize(static_cast<size_t>(n > 0 ? n : 0));
+        if (n > 0) bfs_chunk_coherent_dms(d_min, d_max, ncoherent, m_coh_dm_Vector.data(), n);
+    }
+    virtual ~CChunkB() = default;
+
+    float m_Fmin = 0, m_Fmax = 0;
+    unsigned int m_npol = 0, m_nchan = 0, m_len_sft = 1;
+    float m_tsamp = 0;
+    int m_Chunk_id = 0, m_Block_id = 0;
+    double m_d_max = 0, m_d_min = 0;
+    int m_ncoherent = 0;
+    float m_sigma_bound = 0;
+    int m_length_sum_wnd = 0, m_nbin = 0, m_nfft = 0, m_noverlap = 0;
+    std::vector<double> m_coh_dm_Vector;
+
+    virtual bool process(void* /*pcmparrRawSignalCur*/, std::vector<COutChunkHeader>* /*pvctSuccessHeaders*/,
+                         std::vector<std::vector<float>>* /*pvecImg*/) {
+        return false;
+    }
+    int get_noverlap_per_channel() const { return m_noverlap / static_cast<int>(m_len_sft); }
+    int get_mbin() const { return m_nbin / static_cast<int>(m_len_sft); }
+    int get_mbin_adjusted() const { return get_mbin() - 2 * get_noverlap_per_channel(); }
+    int get_msamp() const { return m_nfft * get_mbin_adjusted(); }
+    void set_chunkid(const int nC) { m_Chunk_id = nC; }
+    void set_blockid(const int nC) { m_Block_id = nC; }
+    static void cutQuadraticFragment(float* parrFragment, float* parrInpImage, int* piRowBegin, int* piColBegin,
+                                     const int QInpImageRows, const int QInpImageCols, const int NUmTargetRow,
+                                     const int NUmTargetCol) {
+        ::cutQuadraticFragment(parrFragment, parrInpImage, piRowBegin, piColBegin, QInpImageRows, QInpImageCols,
+                               NUmTargetRow, NUmTargetCol);
+    }
+};
+
+class CChunk_gpu : public CChunkB {
+public:
+    CChunk_gpu(const float Fmin, const float Fmax, const int npol, const int nchan, const unsigned int len_sft,
+               const int Block_id, const int Chunk_id, const float d_max, const float d_min, const int ncoherent,
+               const float sigma_bound, const int length_sum_wnd, const int nbin, const int nfft,
+               const int noverlap, const float tsamp)
+        : CChunkB(Fmin, Fmax, npol, nchan, len_sft, Block_id, Chunk_id, d_max, d_min, ncoherent, sigma_bound,
+                  length_sum_wnd, nbin, nfft, noverlap, tsamp) {
+        bfs_chunk_desc d{};
+        d.fmin = Fmin; d.fmax = Fmax; d.npol = npol; d.nchan = nchan; d.len_sft = static_cast<int>(len_sft);
+        d.nbin = nbin; d.nfft = nfft; d.noverlap = noverlap; d.tsamp = tsamp; d.max_dt = 0;
+        m_status = bfs_dropin_detail::report(bfs_chunk_create(&d, &m_chunk), "CChunk_gpu");
+        if (!m_chunk) return;
+        int64_t info[8] = {0};
+        bfs_chunk_info(m_chunk, info, 8);
+        m_len_chunk = info[5];
+        m_complex_values = info[6];
+        m_max_dt = static_cast<int>(info[7]);
+        // the threshold and the splitters live in device memory, as in the reference
+        const int splitters[3] = {2, 1, 2};
+        if (cudaMalloc(reinterpret_cast<void**>(&m_pd_thresh), sizeof(float)) != cudaSuccess ||
+            cudaMalloc(reinterpret_cast<void**>(&m_pd_splitters), sizeof(splitters)) != cudaSuccess ||
+            cudaMemcpy(m_pd_thresh, &m_sigma_bound, sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(m_pd_splitters, splitters, sizeof(splitters), cudaMemcpyHostToDevice) != cudaSuccess) {
+            std::fprintf(stderr, "CChunk_gpu: device allocation failed\n");
+            m_status = BFS_ERR_CUDA;
+        }
+    }
+    CChunk_gpu(const CChunk_gpu&) = delete;
+    CChunk_gpu& operator=(const CChunk_gpu&) = delete;
+    ~CChunk_gpu() override {
+        if (m_chunk) bfs_chunk_destroy(m_chunk);
+        cudaFree(m_pdoutImg);
+        cudaFree(m_pd_thresh);
+        cudaFree(m_pd_splitters);
+    }
+
+    // pcmparrRawSignalCur: the unpacked chunk, complex [npol/2][nfft][nchan][nbin] on the device.
+    bool process(void* pcmparrRawSignalCur, std::vector<COutChunkHeader>* pvctSuccessHeaders,
+                 std::vector<std::vector<float>>* pvecImg) override {
+        (void)pvctSuccessHeaders;
+        if (!ready()) return false;
+        const bfs_status st = bfs_chunk_process(m_chunk, pcmparrRawSignalCur, m_coh_dm_Vector.data(),
+                                                static_cast<int>(m_coh_dm_Vector.size()), m_pdoutImg, nullptr);
+        if (bfs_dropin_detail::report(st, "CChunk_gpu::process") != BFS_OK) return false;
+        return search_and_copy(pvecImg);
+    }
+    // process from the int8 GUPPI chunk [nchan][len_chunk][npol] (no reference
+    // counterpart: unpack and forward FFT in one step); d_spec (complex_values()
+    // complex numbers) receives the spectra.
+    bool process_raw(const int8_t* d_raw, void* d_spec, std::vector<COutChunkHeader>* pvctSuccessHeaders,
+                     std::vector<std::vector<float>>* pvecImg) {
+        (void)pvctSuccessHeaders;
+        if (!ready()) return false;
+        const bfs_status st = bfs_chunk_process_raw(m_chunk, d_raw, d_spec, m_coh_dm_Vector.data(),
+                                                    static_cast<int>(m_coh_dm_Vector.size()), m_pdoutImg, nullptr);
+        if (bfs_dropin_detail::report(st, "CChunk_gpu::process_raw") != BFS_OK) return false;
+        return search_and_copy(pvecImg);
+    }
+    // unpack_chunk_guppi_gpu (Session_guppi_gpu.cu:53-60,117-141) into d_cplx.
+    bool unpack(const int8_t* d_raw, void* d_cplx) {
+        return m_chunk && bfs_dropin_detail::report(bfs_chunk_unpack(m_chunk, d_raw, d_cplx, nullptr),
+                                                    "CChunk_gpu::unpack") == BFS_OK;
+    }
+    int64_t len_chunk() const { return m_len_chunk; }
+    int64_t complex_values() const { return m_complex_values; }
+    int max_dt() const { return m_max_dt; }
+    bfs_status last_status() const { return m_status; }
+
+    std::string m_logfile = "candidates.log";  // the reference's fixed log name
+    float* m_pdoutImg = nullptr;               // planes of every coherent DM, max_dt x msamp each
+
+private:
+    bool ready() {
+        if (!m_chunk || m_status != BFS_OK) { std::fprintf(stderr, "CChunk_gpu: not created\n"); return false; }
+        if (m_coh_dm_Vector.empty()) { std::fprintf(stderr, "CChunk_gpu: no coherent DM\n"); return false; }
+        if (!m_pdoutImg) {
+            const size_t n = m_coh_dm_Vector.size() * static_cast<size_t>(m_max_dt) * get_msamp();
+            if (cudaMalloc(reinterpret_cast<void**>(&m_pdoutImg), n * sizeof(float)) != cudaSuccess) {
+                std::fprintf(stderr, "CChunk_gpu: cudaMalloc of the output planes failed\n");
+                m_pdoutImg = nullptr;
+                return false;
+            }
+        }
+        return true;
+    }
+    bool search_and_copy(std::vector<std::vector<float>>* pvecImg) {
+        const int ndm = static_cast<int>(m_coh_dm_Vector.size());
+        const int msamp = get_msamp();
+        clusterization::clusterization_main(m_pdoutImg, m_max_dt * ndm, msamp, *m_pd_thresh, 4, m_pd_splitters,
+                                            m_logfile, m_tsamp * static_cast<float>(m_len_sft), 0.0f);
+        if (pvecImg) {
+            const size_t plane = static_cast<size_t>(m_max_dt) * msamp;
+            pvecImg->resize(static_cast<size_t>(ndm));
+            for (int i = 0; i < ndm; ++i) {
+                (*pvecImg)[i].resize(plane);
+                if (cudaMemcpy((*pvecImg)[i].data(), m_pdoutImg + static_cast<size_t>(i) * plane,
+                               plane * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+                    return false;
+            }
+        }
+        return true;
+    }
+
+    bfs_chunk* m_chunk = nullptr;
+    bfs_status m_status = BFS_OK;
+    int64_t m_len_chunk = 0, m_complex_values = 0;
+    int m_max_dt = 0;
+    float* m_pd_thresh = nullptr;
+    int* m_pd_splitters = nullptr;
+};
+
+class CSession_guppi_gpu {
+public:
+    CSession_guppi_gpu(const char* strGuppiPath, const char* strOutPutPath, const float t_p, const double d_min,
+                       const double d_max, const float sigma_bound, const int length_sum_wnd, const int nbin,
+                       const int nfft)
+        : m_strInpPath(strGuppiPath), m_strOutPutPath(strOutPutPath), m_pulse_length(t_p), m_d_max(d_max),
+          m_d_min(d_min), m_sigma_bound(sigma_bound), m_length_sum_wnd(length_sum_wnd), m_nbin(nbin),
+          m_nfft(nfft) {}
+
+    std::string m_strInpPath, m_strOutPutPath;
+    float m_pulse_length;
+    double m_d_max, m_d_min;
+    float m_sigma_bound;
+    int m_length_sum_wnd, m_nbin, m_nfft;
+    std::vector<COutChunkHeader> m_vctSuccessHeaders;   // unused, as in the reference
+    bfs_guppi_session m_plan{};                         // geometry of the last launch
+
+    int launch(std::vector<std::vector<float>>* pvecImg, int* pmsamp) {
+        using bfs_dropin_detail::report;
+        bfs_guppi_file* f = nullptr;
+        if (report(bfs_guppi_open(m_strInpPath.c_str(), &f), "CSession_guppi_gpu::launch") != BFS_OK) return -1;
+        bfs_guppi_header h{};
+        bfs_guppi_block_header(f, 0, &h);
+        if (report(bfs_guppi_session_plan(&h, m_pulse_length, m_d_min, m_d_max, m_nbin, m_nfft, &m_plan),
+                   "CSession_guppi_gpu::launch") != BFS_OK) {
+            bfs_guppi_close(f);
+            return -1;
+        }
+        int rc = -1;
+        int8_t* d_raw = nullptr;
+        void* d_spec = nullptr;
+        bfs_guppi_reader* reader = nullptr;
+        {
+            CChunk_gpu chunk(m_plan.fmin, m_plan.fmax, h.npol, h.nchan, static_cast<unsigned>(m_plan.len_sft), 0, 0,
+                             m_plan.d_max, m_plan.d_min, m_plan.ncoherent, m_sigma_bound, m_length_sum_wnd,
+                             m_nbin, m_nfft, m_plan.noverlap, m_plan.tsamp);
+            const size_t raw_bytes = static_cast<size_t>(h.nchan) * m_plan.len_chunk * h.npol;
+            if (chunk.last_status() == BFS_OK &&
+                cudaMalloc(reinterpret_cast<void**>(&d_raw), raw_bytes) == cudaSuccess &&
+                cudaMalloc(&d_spec, static_cast<size_t>(chunk.complex_values()) * 2 * sizeof(float)) == cudaSuccess &&
+                report(bfs_guppi_reader_create(f, m_plan.len_chunk, m_plan.noverlap, 2, 1, &reader),
+                       "CSession_guppi_gpu::launch") == BFS_OK) {
+                rc = 0;
+                for (;;) {
+                    int block = -1;
+                    int64_t j = -1;
+                    if (report(bfs_guppi_reader_next(reader, d_raw, nullptr, nullptr, &block, &j),
+                               "CSession_guppi_gpu::launch") != BFS_OK) { rc = -1; break; }
+                    if (block < 0) break;
+                    chunk.set_blockid(block);
+                    chunk.set_chunkid(static_cast<int>(j));
+                    if (!chunk.process_raw(d_raw, d_spec, &m_vctSuccessHeaders, pvecImg)) { rc = -1; break; }
+                    if (pmsamp) *pmsamp = chunk.get_msamp();
+                }
+            }
+            if (reader) bfs_guppi_reader_destroy(reader);
+        }
+        cudaFree(d_raw);
+        cudaFree(d_spec);
+        bfs_guppi_close(f);
+        return rc;
+    }
+};

@@ -476,3 +476,49 @@ def fdmt_normalize(fdmt: np.ndarray, norm: np.ndarray) -> np.ndarray:
     (L/CDMT/Chunk_gpu.cu:842-852)."""
     den = np.sqrt((norm.astype(np.float64) + 1e-8).astype(np.float32))
     return (fdmt.astype(np.float32) / den).astype(np.float32)
+
+
+# --- GUPPI session geometry ---------------------------------------------------
+# A restatement of CSessionB::launch's derivation (MyVSLib_C++/CDMT/
+# SessionB.cpp:144-160 len_sft / overlap / chunk length, :384-392
+# get_optimal_overlap, :395-401 get_coherent_dms, ChunkB.cpp:171-176 the DM
+# grid).  SessionB.cpp includes <fftw3.h>, which is absent here, so the
+# reference's own functions cannot be compiled: this restatement is pinned by
+# hand-worked cases only.  Types follow the reference: float header fields and
+# float products (np.float32), double constants, C round (half away from zero).
+
+def _c_round(x: float) -> float:
+    return float(np.copysign(np.floor(abs(x) + 0.5), x))
+
+
+def _session_delay(dm: float, f_lo: np.float32, f_hi: np.float32) -> np.float32:
+    lo2 = float(np.float32(f_lo * f_lo))
+    hi2 = float(np.float32(f_hi * f_hi))
+    return np.float32(4.148808e3 * dm * (1.0 / lo2 - 1.0 / hi2))
+
+
+def session_plan(obsfreq: float, obsbw: float, nchan: int, tbin: float, t_p: float, d_min: float,
+                 d_max: float, nbin: int, nfft: int) -> dict:
+    f32 = np.float32
+    obsfreq, obsbw, tbin, t_p = f32(obsfreq), abs(f32(obsbw)), f32(tbin), f32(t_p)
+    fmin = f32(float(obsfreq) - float(obsbw) / 2.0)
+    fmax = f32(float(obsfreq) + float(obsbw) / 2.0)
+    len_sft = int(np.ceil(f32(t_p / tbin)))
+    bw_chan = f32(obsbw / f32(nchan * len_sft))
+    f_top = f32(fmin + bw_chan)
+    optimal = int(_c_round(float(f32(_session_delay(d_max, fmin, f_top) / tbin))))
+    half = optimal // 2
+    noverlap = int(2.0 ** _c_round(np.log2(half))) if half > 0 else 0
+    t_d = _session_delay(d_max, fmin, fmax)
+    ncoherent = int(np.ceil(f32(f32(t_d * tbin) / f32(t_p * t_p))))
+    return {"len_sft": len_sft, "noverlap": noverlap, "len_chunk": (nbin - 2 * noverlap) * nfft,
+            "ncoherent": ncoherent, "optimal_overlap": optimal, "fmin": float(fmin), "fmax": float(fmax),
+            "tsamp": float(tbin), "d_min": float(f32(d_min)), "d_max": float(f32(d_max))}
+
+
+def coherent_dms(d_min: float, d_max: float, ncoherent: int) -> np.ndarray:
+    """CChunkB's DM grid (ChunkB.cpp:171-176): step = d_max / ncoherent,
+    (d_max - d_min) / step values d_min + i step (double)."""
+    step = d_max / ncoherent
+    n = int((d_max - d_min) / step)
+    return np.array([d_min + i * step for i in range(max(n, 0))], np.float64)
