@@ -31,6 +31,12 @@ needed); ``e2e`` is the same metric through the public API with each beam's
 input copied from pinned host memory every step and the delegates read back.
 Under torchrun each rank processes its own 48-beam set (weak scaling, no
 collective on the data path); the step time is the max over ranks.
+
+CPU figures (rank 0, one GPU): ``cpu_baseline`` is the reference's own
+CFdmtCpu (built from its sources into oracle/_ref) plus the oracle's
+row-normalise / boxcar / cluster on a bounded sample of the beams;
+``cpu_baseline_variant`` the same with the reference's other CPU FDMT
+(FDMTCPU, Pravir plan), labelled as a different FDMT variant.
 """
 from __future__ import annotations
 
@@ -187,6 +193,42 @@ def cpu_reference_leg(beams, max_seconds: float = 15.0, min_steps: int = 1):
     return done / secs, secs, sample, kind, threads
 
 
+def cpu_pravir_leg(beams, max_seconds: float = 6.0):
+    """A second CPU figure, labelled as a different FDMT variant: the
+    reference's other CPU FDMT (FDMTCPU, Pravir plan, oracle/_ref, all host
+    threads; its output rows are its own delay grid) followed by the same
+    row-normalise / boxcar / cluster restatement, on the given beams (cycled)
+    until max_seconds of work.  None when oracle/_ref holds no FDMTCPU."""
+    from cpp_projects_b200 import synth
+    from oracle import pyoracle
+    if pyoracle.ref_pravir_lib() is None:
+        return None
+    threads = os.cpu_count() or 1
+    done, secs, k = 0, 0.0, 0
+    names = []
+    while (secs < max_seconds and k < 64) or k < 1:
+        b = beams[k % len(beams)]
+        x = synth.filterbank(b)
+        t0 = time.perf_counter()
+        dm = pyoracle.ref_pravir_cpu(b.fmin, b.fmax, x, b.nchan, b.nsamp, b.max_dt, threads=threads)
+        if dm is None:
+            return None
+        z, _, _ = pyoracle.norm_rows(dm)
+        c = pyoracle.boxcar_mt(z, SEARCH["thr"], SEARCH["widths_mode"], SEARCH["param"])
+        if len(c):
+            pyoracle.cluster(c, SEARCH["metrics"])
+        secs += time.perf_counter() - t0
+        done += b.nchan * b.nsamp
+        names.append(f"{b.nchan}x{b.nsamp}")
+        k += 1
+    return {"value": done / secs, "unit": UNIT, "cores": threads, "kind": "reference",
+            "label": "different FDMT variant (the reference's FDMTCPU, Pravir plan)",
+            "sample": (f"{k} beam(s) [{', '.join(names[:6])}{', ...' if k > 6 else ''}]: reference FDMTCPU "
+                       f"({threads} threads) + oracle row-normalise/boxcar ({threads} threads)/cluster "
+                       f"(1 thread)"),
+            "seconds": secs}
+
+
 def reference_gpu_leg(beams, inputs, pipe, dev, stride: int = 4):
     """The reference's own GPU path — CFdmtGpu::process_image, then (the
     reference has no per-row normalisation: this build's bfs_norm_rows) the
@@ -252,6 +294,7 @@ def run_reference(args):
         done += r * secs
         secs_total += secs
     value = done / secs_total
+    pravir = cpu_pravir_leg(sample, max_seconds=5.0)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs_total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -265,7 +308,8 @@ def run_reference(args):
                                 "rate in channel-samples per second"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
                              "sample": texts},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "cpu_baseline_variant": pravir}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -404,12 +448,13 @@ def run_ours(args):
         ref_gpu = reference_gpu_leg(beams, inputs, pipe, dev)
 
     # ---- CPU baseline (rank 0, N=1 only) -------------------------------------
-    cpu = None
+    cpu = cpu_variant = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         small = sorted(beams, key=lambda b: b.nchan * b.nsamp)
         rate, secs, sample, kind, threads = cpu_reference_leg(small, max_seconds=12.0)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample,
                "seconds": secs}
+        cpu_variant = cpu_pravir_leg(small, max_seconds=5.0)
 
     ndel = sum(len(r.delegates) for r in results)
     if rank == 0:
@@ -440,8 +485,8 @@ def run_ours(args):
             "pipeline_balg": {"bytes_per_step": pipe_bytes,
                               "gbs": pipe_bytes / (step_ms / 1e3) / 1e9,
                               "frac_of_peak": pipe_bytes / (step_ms / 1e3) / 1e9 / peak},
-            "e2e": e2e, "cpu_baseline": cpu, "reference_gpu": ref_gpu, "clocks": clk,
-            "gpu_launches": launches,
+            "e2e": e2e, "cpu_baseline": cpu, "cpu_baseline_variant": cpu_variant,
+            "reference_gpu": ref_gpu, "clocks": clk, "gpu_launches": launches,
             "candidates": ncand, "delegates": ndel,
         }
         print(json.dumps(line), flush=True)
