@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 import torch
 
-from cpp_projects_b200 import CFdmtGpu, cluster, search, synth
+from cpp_projects_b200 import CFdmtGpu, cluster, search
 from oracle import pyoracle
 
 pytestmark = pytest.mark.gpu
