@@ -73,7 +73,7 @@ __global__ void k_clean_normalize(float* __restrict__ x, float* __restrict__ mas
     const float mf = g[0], sf = g[1], dmf = g[2], dsf = g[3];
     const bool zap = static_cast<double>(fabsf(buff[rows + row] - dmf)) > 4.0 * static_cast<double>(dsf);
     const size_t base = static_cast<size_t>(row) * cols;
-    if (VEC) {
+    if constexpr (VEC) {
         float4* xr = reinterpret_cast<float4*>(x + base);
         float4* mr = reinterpret_cast<float4*>(mask + base);
         const int n4 = cols >> 2;
@@ -89,15 +89,15 @@ __global__ void k_clean_normalize(float* __restrict__ x, float* __restrict__ mas
                 mr[q] = one;
             }
         }
-        return;
-    }
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cols; t += gridDim.x * blockDim.x) {
-        if (zap) {
-            x[base + t] = 0.0f;
-            mask[base + t] = 0.0f;
-        } else {
-            x[base + t] = clean_sample(x[base + t], mf, sf);
-            mask[base + t] = 1.0f;
+    } else {
+        for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cols; t += gridDim.x * blockDim.x) {
+            if (zap) {
+                x[base + t] = 0.0f;
+                mask[base + t] = 0.0f;
+            } else {
+                x[base + t] = clean_sample(x[base + t], mf, sf);
+                mask[base + t] = 1.0f;
+            }
         }
     }
 }
@@ -114,7 +114,7 @@ __global__ void k_fdmt_normalize(const float* __restrict__ f, const float* __res
                                  float* __restrict__ out) {
     const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
     const long long i0 = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-    if (VEC) {
+    if constexpr (VEC) {
         const float4* f4 = reinterpret_cast<const float4*>(f);
         const float4* n4p = reinterpret_cast<const float4*>(nrm);
         float4* o4 = reinterpret_cast<float4*>(out);
@@ -133,9 +133,9 @@ __global__ void k_fdmt_normalize(const float* __restrict__ f, const float* __res
             o4[i] = make_float4(fdmt_norm_sample(a.x, ma.x), fdmt_norm_sample(a.y, ma.y),
                                 fdmt_norm_sample(a.z, ma.z), fdmt_norm_sample(a.w, ma.w));
         }
-        return;
+    } else {
+        for (long long i = i0; i < n; i += stride) out[i] = fdmt_norm_sample(f[i], nrm[i]);
     }
-    for (long long i = i0; i < n; i += stride) out[i] = fdmt_norm_sample(f[i], nrm[i]);
 }
 
 }  // namespace
