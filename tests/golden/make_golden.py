@@ -12,6 +12,14 @@
   (built from its sources by oracle/Makefile, one thread) on small seeded
   inputs, so the GPU tests can compare against the reference itself on a box
   where the reference checkout does not exist.
+* ``file512.npz`` — the reference's own FDMT test input
+  (``fdmt_class_v0/file512.bin``: a 512 x 512 float32 filterbank of small
+  integers, stored here as int8, which holds it exactly) with the SHA-256 and
+  four rows of the reference's outputs on it: CFdmtCpu (1200-1600 MHz, max
+  delay 512; the file's own band and delay were in test folders that are
+  absent) and a fresh FDMTCPU (Pravir plan; tsamp 1, dt_max 511, dt_step 1,
+  dt_min 0, as fdmt_pr_restr/kernel.cu:357-361 builds it from a 512-row
+  maximum delay).
 """
 from __future__ import annotations
 
@@ -74,5 +82,37 @@ def main(ref_root: str = "/root/reference") -> None:
                                             np.float64))
 
 
+FILE512 = dict(fmin=1200.0, fmax=1600.0, nchan=512, ncols=512, max_dt=512, pravir_dt_max=511)
+FILE512_ROWS = [0, 1, 255, 511]
+
+
+def make_file512(ref_root: str = "/root/reference") -> None:
+    import hashlib
+
+    from oracle import pyoracle
+    x = np.fromfile(Path(ref_root) / "fdmt_class_v0" / "file512.bin", np.float32)
+    q = x.astype(np.int8)
+    if not np.array_equal(q.astype(np.float32), x):
+        raise SystemExit("file512.bin is not int8-valued")
+    c = FILE512
+    x = x.reshape(c["nchan"], c["ncols"])
+    keith = pyoracle.ref_fdmt_cpu(c["fmin"], c["fmax"], x, c["nchan"], c["ncols"], c["max_dt"], threads=1)
+    pravir = pyoracle.ref_pravir_cpu(c["fmin"], c["fmax"], x, c["nchan"], c["ncols"], c["pravir_dt_max"],
+                                     1, 0, tsamp=1.0, threads=1)
+    if keith is None or pravir is None:
+        raise SystemExit("reference FDMTs not built: run make -C oracle")
+    np.savez_compressed(
+        HERE / "file512.npz", input_i8=q.reshape(c["nchan"], c["ncols"]),
+        params=np.array([c["fmin"], c["fmax"], c["nchan"], c["ncols"], c["max_dt"], c["pravir_dt_max"]],
+                        np.float64),
+        rows=np.array(FILE512_ROWS, np.int32),
+        keith_sha256=np.array(hashlib.sha256(keith.tobytes()).hexdigest()),
+        keith_rows=keith[FILE512_ROWS],
+        pravir_sha256=np.array(hashlib.sha256(pravir.tobytes()).hexdigest()),
+        pravir_shape=np.array(pravir.shape, np.int64),
+        pravir_rows=pravir[FILE512_ROWS])
+
+
 if __name__ == "__main__":
     main(*sys.argv[1:])
+    make_file512(*sys.argv[1:])

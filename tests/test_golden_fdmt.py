@@ -37,3 +37,49 @@ def test_gpu_reproduces_reference_output(cuda, path):
     out = torch.empty((max_dt, ncols), device=cuda)
     f.process_image(None if ones else torch.from_numpy(x).to(cuda), out, ones)
     assert np.array_equal(out.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+
+
+# --- the reference's own FDMT test input (fdmt_class_v0/file512.bin) ----------
+FILE512 = Path(__file__).parent / "golden" / "file512.npz"
+REF_FILE512 = Path("/root/reference/fdmt_class_v0/file512.bin")
+
+
+def load512():
+    import hashlib
+    z = np.load(FILE512)
+    fmin, fmax, nchan, ncols, max_dt, pravir_dt_max = z["params"]
+    x = z["input_i8"].astype(np.float32)
+    sha = lambda a: hashlib.sha256(np.ascontiguousarray(a, np.float32).tobytes()).hexdigest()  # noqa: E731
+    return (float(fmin), float(fmax), int(nchan), int(ncols), int(max_dt), int(pravir_dt_max), x, z, sha)
+
+
+def test_file512_fixture_is_the_reference_input():
+    if not REF_FILE512.exists():
+        pytest.skip("reference checkout absent")
+    _, _, nchan, ncols, _, _, x, _, _ = load512()
+    assert np.array_equal(x, np.fromfile(REF_FILE512, np.float32).reshape(nchan, ncols))
+
+
+def test_oracle_reproduces_reference_on_file512():
+    fmin, fmax, nchan, ncols, max_dt, pdt, x, z, sha = load512()
+    keith = pyoracle.fdmt_f32(fmin, fmax, x, nchan, ncols, max_dt)
+    assert sha(keith) == str(z["keith_sha256"])
+    assert np.array_equal(keith[z["rows"]].view(np.uint32), z["keith_rows"].view(np.uint32))
+    pravir = pyoracle.pravir_fdmt(fmin, fmax, x, nchan, ncols, pdt, 1, 0)
+    assert pravir.shape == tuple(z["pravir_shape"]) and sha(pravir) == str(z["pravir_sha256"])
+    assert np.array_equal(pravir[z["rows"]].view(np.uint32), z["pravir_rows"].view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_gpu_reproduces_reference_on_file512(cuda):
+    from cpp_projects_b200 import FDMTGPU, CFdmtGpu
+    fmin, fmax, nchan, ncols, max_dt, pdt, x, z, sha = load512()
+    d_in = torch.from_numpy(x).to(cuda)
+    f = CFdmtGpu(fmin, fmax, nchan, ncols, max_dt)
+    out = torch.empty((max_dt, ncols), device=cuda)
+    f.process_image(d_in, out, False)
+    assert sha(out.cpu().numpy()) == str(z["keith_sha256"])
+    p = FDMTGPU(fmin, fmax, nchan, ncols, 1.0, pdt, 1, 0)
+    pout = torch.empty((p.out_rows, ncols), device=cuda)
+    p.execute(d_in, d_in.numel(), pout, pout.numel())
+    assert sha(pout.cpu().numpy()) == str(z["pravir_sha256"])
