@@ -84,3 +84,48 @@ class CSession_guppi_gpu:
             if pvecImg is not None and planes is not None:
                 pvecImg[:] = list(planes.cpu().numpy())
         return ch.get_msamp()
+
+
+def main(argv=None) -> int:
+    """Command line in the manner of the reference's driver (the GUPPI GPU
+    branch of my_hcdmt_inwork/main.cpp): a GUPPI file through the session,
+    the delegate log and the last chunk's images (``images.npy``, one
+    max_dt x msamp plane per coherent DM) written to the output folder.
+    ``--plan-only`` prints the chunk geometry and exits (no GPU needed)."""
+    import argparse
+    import json
+    from pathlib import Path
+
+    import numpy as np
+
+    ap = argparse.ArgumentParser(prog="python -m cpp_projects_b200.session")
+    ap.add_argument("guppi")
+    ap.add_argument("outdir")
+    ap.add_argument("--t-p", type=float, required=True, help="pulse length, s")
+    ap.add_argument("--d-min", type=float, default=0.0)
+    ap.add_argument("--d-max", type=float, required=True)
+    ap.add_argument("--sigma", type=float, default=6.0, help="detection threshold (S/N)")
+    ap.add_argument("--length-sum-wnd", type=int, default=1)
+    ap.add_argument("--nbin", type=int, default=1 << 20)
+    ap.add_argument("--nfft", type=int, default=1)
+    ap.add_argument("--plan-only", action="store_true")
+    a = ap.parse_args(argv)
+    s = CSession_guppi_gpu(a.guppi, a.outdir, a.t_p, a.d_min, a.d_max, a.sigma, a.length_sum_wnd,
+                           a.nbin, a.nfft)
+    p = s.plan()
+    if a.plan_only:
+        print(json.dumps(p))
+        return 0
+    out = Path(a.outdir)
+    out.mkdir(parents=True, exist_ok=True)
+    imgs: list = []
+    msamp = s.launch(imgs, logfile=str(out / "candidates.log"))
+    if imgs:
+        np.save(out / "images.npy", np.stack(imgs))
+    ndel = sum(cl.ngroups for _, _, cl in s.results if cl is not None)
+    print(json.dumps({**p, "msamp": msamp, "chunks": len(s.results), "delegates": ndel}))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -163,3 +163,16 @@ def build_session_demo(tmp: Path) -> Path:
 
 def test_cpp_session_driver_compiles(tmp_path):
     assert build_session_demo(tmp_path).exists()
+
+
+def test_session_command_line_plan(tmp_path):
+    import json
+    import sys
+    path = tmp_path / "s.raw"
+    synth.write_guppi(path, [np.zeros((8, 9000, 4), np.int8)], 1216.0, 32.0, 0.25e-6)
+    r = subprocess.run([sys.executable, "-m", "cpp_projects_b200.session", str(path), str(tmp_path / "out"),
+                        "--t-p", "1.9e-6", "--d-max", "2", "--nbin", "4096", "--nfft", "2", "--plan-only"],
+                       capture_output=True, text=True, cwd=ROOT, timeout=300)
+    assert r.returncode == 0, r.stderr
+    p = json.loads(r.stdout)
+    assert (p["len_sft"], p["noverlap"], p["len_chunk"], p["ncoherent"]) == (8, 8, 8160, 21)
