@@ -8,6 +8,12 @@ Prints one JSON line: the plan's fused depth, milliseconds per call, the
 level-by-level algorithmic bytes of one call and the resulting GB/s.  Used
 for the autotuner's choices, for the reduced-precision and adjoint timings,
 and as the command under ncu for the per-kernel captures.
+
+For 512, 1024 and 2048 channels the line also carries the figure the
+reference's FDMT drivers print, "GFLP/sec": a constant operation count per
+test size (MyVSLib_C++/Constants.h:6-9; 1024 channels use the 512 x 1024
+count, as fdmt_class_v0/kernel.cu:24,176-199 selects it) divided by the time
+per call.
 """
 from __future__ import annotations
 
@@ -19,6 +25,8 @@ import torch
 from .fdmt import CFdmtGpu
 
 PRECISIONS = {"f32": 0, "f16": 1, "bf16": 2}
+# giga-operations per call of the reference's FDMT test sizes (Constants.h:6-9)
+REFERENCE_GFLOP = {512: 0.00320386, 1024: 0.006518622, 2048: 0.0586616}
 
 
 def main(argv=None) -> int:
@@ -60,7 +68,9 @@ def main(argv=None) -> int:
     ms = e0.elapsed_time(e1) / a.reps
     print(json.dumps({"nchan": a.nchan, "ncols": a.ncols, "max_dt": max_dt, "precision": a.precision,
                       "adjoint": a.adjoint, "fuse_depth": f.info.fuse_depth, "ms": ms,
-                      "alg_bytes": f.alg_bytes, "alg_gbs": f.alg_bytes / (ms / 1e3) / 1e9}))
+                      "alg_bytes": f.alg_bytes, "alg_gbs": f.alg_bytes / (ms / 1e3) / 1e9,
+                      "reference_gflop_per_s": (REFERENCE_GFLOP[a.nchan] / (ms / 1e3)
+                                                if a.nchan in REFERENCE_GFLOP else None)}))
     return 0
 
 
