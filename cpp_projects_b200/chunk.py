@@ -23,11 +23,13 @@ from ._tensors import dev_ptr, stream_handle
 
 def coherent_dms(d_min: float, d_max: float, ncoherent: int) -> np.ndarray:
     """The coherent-DM grid of CChunkB's constructor (ChunkB.cpp:171-176)."""
-    buf = np.zeros(4096, np.float64)
-    n = _capi.lib().bfs_chunk_coherent_dms(ctypes.c_double(d_min), ctypes.c_double(d_max),
-                                           int(ncoherent), buf.ctypes.data_as(ctypes.c_void_p),
-                                           buf.size)
-    return buf[: min(n, buf.size)].copy()
+    fn = _capi.lib().bfs_chunk_coherent_dms
+    n = fn(ctypes.c_double(d_min), ctypes.c_double(d_max), int(ncoherent), None, 0)
+    buf = np.zeros(max(n, 0), np.float64)
+    if n > 0:
+        fn(ctypes.c_double(d_min), ctypes.c_double(d_max), int(ncoherent), buf.ctypes.data_as(ctypes.c_void_p),
+           buf.size)
+    return buf
 
 
 class CChunk_gpu:

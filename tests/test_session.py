@@ -176,3 +176,11 @@ def test_session_command_line_plan(tmp_path):
     assert r.returncode == 0, r.stderr
     p = json.loads(r.stdout)
     assert (p["len_sft"], p["noverlap"], p["len_chunk"], p["ncoherent"]) == (8, 8, 8160, 21)
+
+
+@pytest.mark.parametrize("args", [(0.0, 100.0, 212), (0.0, 1000.0, 4846), (5.0, 100.0, 7), (0.0, 2.0, 21)])
+def test_coherent_dm_grid_matches_oracle_at_any_count(args):
+    from cpp_projects_b200.chunk import coherent_dms
+    got = coherent_dms(*args)
+    want = pyoracle.coherent_dms(*args)
+    assert len(got) == len(want) and np.array_equal(got, want)
