@@ -14,15 +14,20 @@ SessionB.cpp:255-267) and ``CChunk_gpu.search`` writes the delegate log.
 As in the reference, every chunk writes the same log file (the chunk's
 ``candidates.log``; the output path is stored but not used), the images
 handed back are those of the last chunk, and the return value is msamp.
-Unlike the reference, the clusters of every chunk are kept in
-``results`` as ``(block, chunk, Clusters | None)``.
+Unlike the reference, every chunk's delegates are kept on the host in
+``results`` as ``(block, chunk, delegates, group_sizes)``: the delegate Cand
+records sorted by mt and the sizes of their groups in the log's pairing
+(empty arrays when no candidate passed); the device buffers of a chunk are
+released before the next one.
 """
 from __future__ import annotations
 
+import numpy as np
 import torch
 
 from . import guppi
 from .chunk import CChunk_gpu
+from .search import CAND_DTYPE
 
 
 class CSession_guppi_gpu:
@@ -78,7 +83,11 @@ class CSession_guppi_gpu:
                     ch.set_blockid(block)
                     ch.set_chunkid(chunk)
                     planes = ch.process_raw(d_raw, spec, stream=stream)
-                    self.results.append((block, chunk, ch.search(planes, logfile, 0.0)))
+                    cl = ch.search(planes, logfile, 0.0)
+                    if cl is None:
+                        self.results.append((block, chunk, np.zeros(0, CAND_DTYPE), np.zeros(0, np.int64)))
+                    else:
+                        self.results.append((block, chunk, cl.delegate_records(), cl.group_sizes()))
             finally:
                 reader.close()
             if pvecImg is not None and planes is not None:
@@ -95,8 +104,6 @@ def main(argv=None) -> int:
     import argparse
     import json
     from pathlib import Path
-
-    import numpy as np
 
     ap = argparse.ArgumentParser(prog="python -m cpp_projects_b200.session")
     ap.add_argument("guppi")
@@ -122,7 +129,7 @@ def main(argv=None) -> int:
     msamp = s.launch(imgs, logfile=str(out / "candidates.log"))
     if imgs:
         np.save(out / "images.npy", np.stack(imgs))
-    ndel = sum(cl.ngroups for _, _, cl in s.results if cl is not None)
+    ndel = sum(len(d) for _, _, d, _ in s.results)
     print(json.dumps({**p, "msamp": msamp, "chunks": len(s.results), "delegates": ndel}))
     return 0
 

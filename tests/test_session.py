@@ -87,6 +87,7 @@ class _StandInChunk:
         self.p, self.calls = p, calls
         self.m_coh_dm_Vector = pyoracle.coherent_dms(p["d_min"], p["d_max"], p["ncoherent"])
         self.block = self.chunk = -1
+        self.searched = []
 
     def complex_buffer(self, device):
         return torch.zeros(4, 2)
@@ -105,7 +106,24 @@ class _StandInChunk:
         return torch.full((len(self.m_coh_dm_Vector), 2, 3), float(len(self.calls)))
 
     def search(self, planes, logfile, t0):
-        return ("searched", float(planes[0, 0, 0]), logfile, t0)
+        self.searched.append((float(planes[0, 0, 0]), logfile, t0))
+        k = int(planes[0, 0, 0])
+        if k % 2 == 0:
+            return None                                   # no candidate passed
+        return _StandInClusters(k)
+
+
+class _StandInClusters:
+    def __init__(self, k):
+        self.k = k
+
+    def delegate_records(self):
+        c = np.zeros(self.k, pyoracle.CAND_DTYPE)
+        c["mt"] = np.arange(self.k)
+        return c
+
+    def group_sizes(self):
+        return np.full(self.k, 2, np.int64)
 
 
 class _CpuSession(CSession_guppi_gpu):
@@ -114,7 +132,8 @@ class _CpuSession(CSession_guppi_gpu):
         self.calls = []
 
     def createChunk(self, p, hdr):
-        return _StandInChunk(p, hdr, self.calls)
+        self.chunk = _StandInChunk(p, hdr, self.calls)
+        return self.chunk
 
     def open_reader(self, f, p, device, stream):
         return guppi.GuppiReader(f, p["len_chunk"], p["noverlap"], nbuffers=2)   # host buffers
@@ -135,9 +154,12 @@ def test_session_loop_hands_every_chunk_in_order(tmp_path):
     assert [(b, j) for b, j, _ in s.calls] == want
     for b, j, data in s.calls:
         assert np.array_equal(data, f.read_chunk(b, j, p["len_chunk"], p["noverlap"]))
-    assert [(b, j) for b, j, _ in s.results] == want
-    assert [r[2] for r in s.results] == [("searched", float(k + 1), str(tmp_path / "c.log"), 0.0)
-                                         for k in range(len(want))]
+    assert [(b, j) for b, j, _, _ in s.results] == want
+    assert s.chunk.searched == [(float(k + 1), str(tmp_path / "c.log"), 0.0) for k in range(len(want))]
+    for k, (_, _, dl, sizes) in enumerate(s.results):
+        n = (k + 1) if (k + 1) % 2 else 0        # odd chunks found k + 1 delegates, even ones none
+        assert dl.dtype == pyoracle.CAND_DTYPE and list(dl["mt"]) == list(range(n))
+        assert list(sizes) == [2] * n
     ndm = len(pyoracle.coherent_dms(p["d_min"], p["d_max"], p["ncoherent"]))
     assert len(imgs) == ndm and all(np.all(x == len(want)) for x in imgs)   # the last chunk's images
 

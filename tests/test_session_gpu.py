@@ -44,14 +44,15 @@ def test_session_matches_the_chunk_stage_run_directly(cuda, tmp_path):
     assert msamp == ch.get_msamp() == NFFT * (NBIN // 8 - 2)
     spec = ch.complex_buffer(cuda)
     chunks = [(b, j) for b in range(f.nblocks) for j in range(f.chunk_count(b, p["len_chunk"], p["noverlap"]))]
-    assert [(b, j) for b, j, _ in s.results] == chunks
+    assert [(b, j) for b, j, _, _ in s.results] == chunks
     planes = None
-    for b, j, cl in s.results:
+    for b, j, delegates, sizes in s.results:
         raw = torch.from_numpy(f.read_chunk(b, j, p["len_chunk"], p["noverlap"])).to(cuda)
         planes = ch.process_raw(raw, spec)
         want = ch.search(planes, None, 0.0)
-        assert want is not None and cl is not None and cl.ngroups == want.ngroups > 0
-        assert np.array_equal(cl.delegate_records(), want.delegate_records())
+        assert want is not None and len(delegates) == want.ngroups > 0
+        assert np.array_equal(delegates, want.delegate_records())
+        assert np.array_equal(sizes, want.group_sizes())
     ndm = len(ch.m_coh_dm_Vector)
     assert len(imgs) == ndm and imgs[0].shape == (8, msamp)
     assert np.array_equal(np.stack(imgs).view(np.uint32), planes.cpu().numpy().view(np.uint32))
