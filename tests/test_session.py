@@ -206,3 +206,54 @@ def test_coherent_dm_grid_matches_oracle_at_any_count(args):
     got = coherent_dms(*args)
     want = pyoracle.coherent_dms(*args)
     assert len(got) == len(want) and np.array_equal(got, want)
+
+
+def test_cpp_session_driver_control_flow_with_a_stand_in_gpu(tmp_path):
+    """session_demo linked with tests/cpp/session_mock.cpp (CUDA runtime and
+    GPU entries replaced by host stand-ins; file index and geometry from the
+    real library): the C++ CSession_guppi_gpu reads every chunk, hands the
+    last chunk's planes back per DM and writes that chunk's delegate log."""
+    exe = tmp_path / "session_demo_mock"
+    cmd = ["g++", "-std=c++17", "-O1", "-Wall", "-Werror", str(ROOT / "tests/cpp/session_demo.cpp"),
+           str(ROOT / "tests/cpp/session_mock.cpp"), "-I", str(ROOT / "include"), "-I", str(CUDA / "include"),
+           "-L", str(_capi.LIB_PATH.parent), "-lbfs_b200", f"-Wl,-rpath,{_capi.LIB_PATH.parent}",
+           "-o", str(exe)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    rng = np.random.default_rng(11)
+    blocks = [rng.integers(-8, 8, (8, n, 4)).astype(np.int8) for n in (9000, 12000)]
+    path = tmp_path / "s.raw"
+    synth.write_guppi(path, blocks, 1216.0, 32.0, 0.25e-6, directio=1)
+    run = tmp_path / "run"
+    run.mkdir()
+    t_p = float(np.float32(1.9e-6)).hex()
+    r = subprocess.run([str(exe), str(path), str(run / "img.bin"), t_p, "0.0", "2.0", "3.0", "4096", "2"],
+                       cwd=run, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    msamp, ndm, len_sft, noverlap, ncoherent, len_chunk = (int(v) for v in r.stdout.split())
+    f = guppi.GuppiFile(path)
+    p = guppi.session_plan(f.header(0), 1.9e-6, 0.0, 2.0, 4096, 2)
+    assert (len_sft, noverlap, ncoherent, len_chunk) == (p["len_sft"], p["noverlap"], p["ncoherent"],
+                                                         p["len_chunk"])
+    assert ndm == len(pyoracle.coherent_dms(p["d_min"], p["d_max"], p["ncoherent"]))
+    assert msamp == 2 * (4096 // len_sft - 2 * (noverlap // len_sft))
+    # the stand-in planes of the last chunk
+    last = (f.nblocks - 1, f.chunk_count(f.nblocks - 1, len_chunk, noverlap) - 1)
+    s = int(f.read_chunk(*last, len_chunk, noverlap).astype(np.int64).sum())
+    i, rr, t = np.meshgrid(np.arange(ndm), np.arange(len_sft), np.arange(msamp), indexing="ij")
+    want = ((s + 7 * i + 3 * rr + t) % 97).astype(np.float32)
+    got = np.fromfile(run / "img.bin", np.float32).reshape(ndm, len_sft, msamp)
+    assert np.array_equal(got, want)
+    # one candidate per plane row at its first maximum, each its own group, sorted by mt
+    flat = want.reshape(ndm * len_sft, msamp)
+    mt = flat.argmax(axis=1)
+    order = np.argsort(mt, kind="stable")
+    rows = [ln.split() for ln in (run / "candidates.log").read_text().splitlines()]
+    assert rows[0] == ["N", "t,", "bin", "t,", "sec", "dedisp", "width", "SNR", "num"]
+    assert len(rows) == 1 + len(order)
+    delt_bin = np.float32(np.float32(p["tsamp"]) * np.float32(len_sft))
+    for k, row in enumerate(order):
+        n_, t_bin, t_sec, dedisp, width, snr, num = rows[1 + k]
+        assert (int(n_), int(t_bin), int(dedisp), int(width), float(snr), int(num)) == \
+            (k + 1, int(mt[row]), int(row), 1, 96.0, 1)
+        assert abs(float(t_sec) - float(np.float32(mt[row]) * delt_bin)) <= 1e-6 * max(1.0, float(t_sec))
