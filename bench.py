@@ -3,7 +3,7 @@
 
     python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
                     [--workload config2|config0|config1|config3|config4|config4fwd]
-                    [--form both|batched] [--no-e2e] [--no-cpu-baseline] [--no-ref-gpu]
+                    [--form both|batched] [--no-e2e] [--no-cpu-baseline]
 
 Workload (default ``config2``): the batched multi-beam search — 48 beams of
 uneven shapes (nchan from {256, 512, 1024, 4096}, 2^14..2^17 samples, max
@@ -71,7 +71,6 @@ def parse_args(argv=None):
                                            "config1"], default="config2")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--form", choices=["both", "batched"], default="both",
                     help="batched: time only the batched form (profiling runs; no plain-form "
                          "numbers, no FDMT roofline)")
@@ -227,55 +226,6 @@ def cpu_pravir_leg(beams, max_seconds: float = 6.0):
                        f"({threads} threads) + oracle row-normalise/boxcar ({threads} threads)/cluster "
                        f"(1 thread)"),
             "seconds": secs}
-
-
-def reference_gpu_leg(beams, inputs, pipe, dev, stride: int = 4):
-    """The reference's own GPU path — CFdmtGpu::process_image, then (the
-    reference has no per-row normalisation: this build's bfs_norm_rows) the
-    reference's gather_candidates_in_dynamicalArray + complete_clusterization
-    with its log — compiled from the reference's sources (oracle/_ref), on every
-    `stride`-th beam, timed beside this build's pipeline on the same beams."""
-    import tempfile
-
-    import torch
-
-    from cpp_projects_b200 import search
-    from oracle import pyoracle
-    if pyoracle.ref_gpu_lib() is None:
-        return None
-    l = pyoracle.ref_gpu_lib()
-    idx = list(range(0, len(beams), stride))
-    thr = torch.tensor([SEARCH["thr"]], device=dev)
-    metrics = torch.tensor(SEARCH["metrics"], dtype=torch.int32, device=dev)
-    log = tempfile.NamedTemporaryFile(suffix=".log", delete=False).name
-    t_ref = 0.0
-    units = 0
-    for i in idx:
-        b = beams[i]
-        f = pyoracle.RefFdmtGpu(b.fmin, b.fmax, b.nchan, b.nsamp, b.max_dt)
-        out = torch.empty((b.max_dt, b.nsamp), device=dev)
-        z = torch.empty_like(out)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        f.process_image(inputs[i].data_ptr(), out.data_ptr())
-        search.norm_rows(out, out=z)
-        l.ref_search_dynamic(z.data_ptr(), b.max_dt, b.nsamp, thr.data_ptr(), SEARCH["param"],
-                             metrics.data_ptr(), log.encode(), 1e-3, 0.0)
-        torch.cuda.synchronize()
-        t_ref += time.perf_counter() - t0
-        units += b.nchan * b.nsamp
-        del f, out, z
-    os.unlink(log)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for i in idx:
-        pipe.run_beam(i, inputs[i])
-    torch.cuda.synchronize()
-    t_ours = time.perf_counter() - t0
-    return {"value": units / t_ref, "unit": UNIT, "beams": f"{len(idx)} of {len(beams)} (every {stride}th)",
-            "ours_same_beams": units / t_ours, "speedup": t_ref / t_ours,
-            "path": "reference CFdmtGpu + gather_candidates_in_dynamicalArray + complete_clusterization, "
-                    "sm_100a build of its own sources; wall clock, synchronised"}
 
 
 def run_reference(args):
@@ -442,11 +392,6 @@ def run_ours(args):
                "wall_ms_per_step": 1e3 * wall / args.steps}
         del host
 
-    # ---- the reference's own GPU path on a subset (rank 0, N=1) ---------------
-    ref_gpu = None
-    if rank == 0 and world == 1 and not args.no_ref_gpu:
-        ref_gpu = reference_gpu_leg(beams, inputs, pipe, dev)
-
     # ---- CPU baseline (rank 0, N=1 only) -------------------------------------
     cpu = cpu_variant = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -486,7 +431,7 @@ def run_ours(args):
                               "gbs": pipe_bytes / (step_ms / 1e3) / 1e9,
                               "frac_of_peak": pipe_bytes / (step_ms / 1e3) / 1e9 / peak},
             "e2e": e2e, "cpu_baseline": cpu, "cpu_baseline_variant": cpu_variant,
-            "reference_gpu": ref_gpu, "clocks": clk, "gpu_launches": launches,
+            "clocks": clk, "gpu_launches": launches,
             "candidates": ncand, "delegates": ndel,
         }
         print(json.dumps(line), flush=True)
@@ -505,15 +450,14 @@ def run_config3(args):
     """Reduced-precision FDMT: one 4096 x 2^17 beam (1100-1500 MHz, bandpass
     gain, 20 pulses) through FDMT + row statistics + boxcar (widths 1..64,
     S/N > 7) + clustering with FP32, FP16 and BF16 planes between FDMT levels.
-    Reports each form's device time, the FDMT error against the FP64 oracle
-    (on the first 8192 samples: the FDMT is causal, so they equal the
-    transform of the first 8192 input samples), and candidate / delegate /
-    injected-pulse recall of the 16-bit forms against FP32."""
+    Reports each form's device time, the 16-bit forms' FDMT difference from
+    the FP32 form (on the first 8192 samples; the error against FP64 is
+    asserted by the GPU tests), and candidate / delegate / injected-pulse
+    recall of the 16-bit forms against FP32."""
     import torch
 
     from cpp_projects_b200 import search
     from cpp_projects_b200.pipeline import BeamShape, SearchPipeline, device_filterbank
-    from oracle import pyoracle
 
     if not torch.cuda.is_available():
         print(json.dumps({"metric": METRIC, "error": "no CUDA device"}))
@@ -527,8 +471,7 @@ def run_config3(args):
     search_cfg = dict(widths_mode=0, param=6, thr=7.0, metrics=(16, 8, 1 << 30))
     peak, peak_kind = measured_peaks()
     tw = 8192
-    x_head = x[:, :tw].contiguous().cpu().numpy()
-    y64 = pyoracle.fdmt_f64(b.fmin, b.fmax, x_head, b.nchan, tw, b.max_dt)
+    y32 = None                     # the FP32 form's first tw samples (the loop starts with it)
     forms = {}
     keys = {}
     clocks = ClockSampler(0).start()
@@ -550,7 +493,9 @@ def run_config3(args):
         alg = pipe.fdmt_alg_bytes()
         plane = pipe.plane[: b.max_dt * b.nsamp].view(b.max_dt, b.nsamp)
         y = plane[:, :tw].double().cpu().numpy()
-        err = y - y64
+        if y32 is None:
+            y32 = y
+        err = y - y32
         # the candidates of the last run are still in the pipeline's buffer
         keys[name] = _cand_keys(pipe.cands, res.n_candidates, b.nsamp)
         # an injected pulse is found when a candidate lies at its delay row
@@ -566,8 +511,8 @@ def run_config3(args):
             "value": b.nchan * b.nsamp / (ms / 1e3), "ms_per_step": ms, "fdmt_ms": fdmt_ms,
             "fdmt_alg_bytes": alg, "fdmt_gbs": alg / (fdmt_ms / 1e3) / 1e9,
             "fdmt_frac": alg / (fdmt_ms / 1e3) / 1e9 / peak, "fuse_depth": pipe.plans[0].info.fuse_depth,
-            "err_vs_fp64": {"max_rel_to_maxabs": float(np.abs(err).max() / np.abs(y64).max()),
-                            "rms_rel": float(np.sqrt((err ** 2).mean() / (y64 ** 2).mean()))},
+            "diff_vs_f32": {"max_rel_to_maxabs": float(np.abs(err).max() / np.abs(y32).max()),
+                            "rms_rel": float(np.sqrt((err ** 2).mean() / (y32 ** 2).mean()))},
             "candidates": res.n_candidates, "delegates": len(res.delegates),
             "injected_found": f"{found}/{len(b.pulses)}",
             "_delegates": res.delegates,
@@ -626,16 +571,15 @@ def run_config4(args):
     with RFI sinusoids of amplitude 5), per-channel weights w (initially 1),
     loss = -sum of boxcar S/N at the 8 pulse cells.  Times the forward FDMT,
     the adjoint FDMT and the whole forward + backward step (device events);
-    checks the weight gradient against the FP64 reference gradient (oracle
-    FP64 FDMT and adjoint on the host) and against central finite differences
-    (eps 1e-3) of the FP64 loss on 4 channels; runs 30 steps of projected
-    gradient ascent on w in [0, 1] to show the S/N gain."""
+    checks the weight gradient against central finite differences (eps 0.05)
+    of the loss on 4 channels (the FP64 gradient check is a GPU test); runs
+    30 steps of projected gradient ascent on w in [0, 1] to show the S/N
+    gain."""
     import torch
 
     from cpp_projects_b200 import CFdmtGpu, search, synth
     from cpp_projects_b200.autograd import boxcar_snr, fdmt
     from cpp_projects_b200.pipeline import device_filterbank
-    from oracle import pyoracle
 
     if not torch.cuda.is_available():
         print(json.dumps({"metric": METRIC, "error": "no CUDA device"}))
@@ -680,25 +624,20 @@ def run_config4(args):
     loss = step()
     g_gpu = w.grad.double().cpu().numpy()
 
-    # FP64 reference gradient at full size
-    xh = x.double().cpu().numpy()
-    y64 = pyoracle.fdmt_f64(b.fmin, b.fmax, xh, b.nchan, b.nsamp, b.max_dt)
-    snr64, grads = pyoracle.snr_cells_f64(y64, cells)
-    gy64 = np.zeros_like(y64)
-    for k, (d, t, wd) in enumerate(cells):
-        gy64[d] -= grads[k]
-    g64 = (pyoracle.fdmt_adjoint_f64(b.fmin, b.fmax, gy64, b.nchan, b.nsamp, b.max_dt) * xh).sum(1)
-    # central differences of the FP64 loss: y(w +- eps e_c) = y64 +- eps F(x_c e_c)
+    # central differences of the loss on 4 channels, through this build's own
+    # forward path (FP32; eps 0.05 keeps the difference well above FP32
+    # rounding of a loss of ~1e3); the FP64 gradient check is a GPU test
+    eps = 0.05
     rng = np.random.default_rng(0)
     fd = []
-    for c in rng.choice(b.nchan, 4, replace=False):
-        xc = np.zeros_like(xh)
-        xc[c] = xh[c]
-        dy = pyoracle.fdmt_f64(b.fmin, b.fmax, xc, b.nchan, b.nsamp, b.max_dt)
-        lp = -pyoracle.snr_cells_f64(y64 + 1e-3 * dy, cells)[0].sum()
-        lm = -pyoracle.snr_cells_f64(y64 - 1e-3 * dy, cells)[0].sum()
-        fd.append({"channel": int(c), "fd": (lp - lm) / 2e-3, "gpu": float(g_gpu[c]), "fp64": float(g64[c])})
-    gscale = np.abs(g64).max()
+    with torch.no_grad():
+        for c in rng.choice(b.nchan, 4, replace=False):
+            e = torch.zeros(b.nchan, device=dev)
+            e[int(c)] = eps
+            lp = -boxcar_snr(fdmt((1.0 + e)[:, None] * x, plan), cells).sum().item()
+            lm = -boxcar_snr(fdmt((1.0 - e)[:, None] * x, plan), cells).sum().item()
+            fd.append({"channel": int(c), "fd": (lp - lm) / (2 * eps), "gpu": float(g_gpu[c])})
+    gscale = float(np.abs(g_gpu).max())
 
     # projected gradient ascent on the weights
     snr0 = float(-loss.item())
@@ -732,9 +671,8 @@ def run_config4(args):
                      "frac": alg / (adj_ms / 1e3) / 1e9 / peak, "peak_source": peak_kind, "traffic": None},
         "adjoint": {"forward_fdmt_ms": fwd_ms, "adjoint_fdmt_ms": adj_ms, "ratio": adj_ms / fwd_ms,
                     "forward_fuse_depth": plan.info.fuse_depth},
-        "gradient_check": {"loss_gpu": float(loss.item()), "loss_fp64": float(-snr64.sum()),
-                           "max_abs_err_rel_to_max_grad": float(np.abs(g_gpu - g64).max() / gscale),
-                           "finite_differences_eps_1e-3": fd},
+        "gradient_check": {"loss_gpu": float(loss.item()), "max_abs_grad": gscale,
+                           "finite_differences_eps_0.05": fd},
         "weight_optimisation": {"snr_sum_before": snr0, "snr_sum_after_30_adam_steps": snr1,
                                 "mean_w_rfi_channels": float(wf[rfi_ch].mean()),
                                 "mean_w_clean_channels": float(wf[clean].mean())},

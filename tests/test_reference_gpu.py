@@ -84,3 +84,51 @@ def test_fdmt_versus_reference_gpu_class(ref, cuda):
     close = int((rel < 1e-5).sum())
     print(f"rows within 1e-5 of the reference GPU class: {close}/{mdt}")
     assert close >= 0.9 * mdt
+
+
+def test_reference_gpu_search_path_timed_beside_ours(ref, cuda, tmp_path):
+    """The reference's own GPU search path (CFdmtGpu::process_image, then its
+    gather_candidates_in_dynamicalArray + complete_clusterization with its
+    log; per-row normalisation from this build, which the reference lacks)
+    timed beside this build's per-beam pipeline on the same four beams of the
+    48-beam workload (the smallest ones; wall clock, synchronised).  Prints
+    both rates; this build must be the faster."""
+    import time
+
+    from cpp_projects_b200 import synth
+    from cpp_projects_b200.pipeline import BeamShape, SearchPipeline, device_filterbank
+    beams = sorted(synth.config2(seed=2), key=lambda b: b.nchan * b.nsamp)[:4]
+    shapes = [BeamShape(b.nchan, b.nsamp, b.fmin, b.fmax, b.max_dt) for b in beams]
+    pipe = SearchPipeline(shapes, widths_mode=0, param=5, thr=7.0, metrics=(16, 8, 1 << 30),
+                          capacity=1 << 24, device=cuda)
+    inputs = [device_filterbank(b.nchan, b.nsamp, b.fmin, b.fmax, b.seed, b.pulses, cuda) for b in beams]
+    thr = torch.tensor([7.0], device=cuda)
+    metrics = torch.tensor([16, 8, 1 << 30], dtype=torch.int32, device=cuda)
+    log = str(tmp_path / "ref.log").encode()
+    for i in range(len(beams)):                      # warm-up of both paths
+        pipe.run_beam(i, inputs[i])
+    torch.cuda.synchronize()
+    t_ref, units = 0.0, 0
+    for i, b in enumerate(beams):
+        f = pyoracle.RefFdmtGpu(b.fmin, b.fmax, b.nchan, b.nsamp, b.max_dt)
+        out = torch.empty((b.max_dt, b.nsamp), device=cuda)
+        z = torch.empty_like(out)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        assert f.process_image(inputs[i].data_ptr(), out.data_ptr()) == 0
+        search.norm_rows(out, out=z)
+        ref.ref_search_dynamic(z.data_ptr(), b.max_dt, b.nsamp, thr.data_ptr(), 5, metrics.data_ptr(), log,
+                               1e-3, 0.0)
+        torch.cuda.synchronize()
+        t_ref += time.perf_counter() - t0
+        units += b.nchan * b.nsamp
+        del f, out, z
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(len(beams)):
+        pipe.run_beam(i, inputs[i])
+    torch.cuda.synchronize()
+    t_ours = time.perf_counter() - t0
+    print(f"reference GPU path {units / t_ref:.3e} ch*s/s, this build {units / t_ours:.3e} ch*s/s "
+          f"({t_ref / t_ours:.1f}x)")
+    assert t_ours < t_ref
