@@ -71,6 +71,9 @@ def parse_args(argv=None):
                                            "config1"], default="config2")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="no effect: the reference GPU path is timed by the tests now; accepted so "
+                         "the commands recorded with the profiles run unchanged (they skipped it)")
     ap.add_argument("--form", choices=["both", "batched"], default="both",
                     help="batched: time only the batched form (profiling runs; no plain-form "
                          "numbers, no FDMT roofline)")
