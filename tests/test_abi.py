@@ -50,3 +50,20 @@ def test_bad_arguments_return_status_not_crash():
     assert b"fmin" in lib.bfs_last_error()
     desc = _capi.FdmtDesc(fmin=1200.0, fmax=1600.0, nchan=1, ncols=128, max_dt=64)
     assert lib.bfs_fdmt_plan_create_host(ctypes.byref(desc), ctypes.byref(plan)) == _capi.BFS_ERR_ARG
+
+
+def test_header_is_plain_c(tmp_path):
+    """include/bfs.h is a C header: it compiles as pedantic C99 and links
+    against the library from a C program (no C++ types in the interface)."""
+    src = tmp_path / "use.c"
+    src.write_text('#include "bfs.h"\n#include <stdio.h>\n'
+                   'int main(void) { bfs_guppi_session s; bfs_cand c; (void)s; (void)c;\n'
+                   '  printf("%s\\n", bfs_version()); return 0; }\n')
+    exe = tmp_path / "use"
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", str(src),
+                        "-I", str(ROOT / "include"), "-L", str(_capi.LIB_PATH.parent), "-lbfs_b200",
+                        f"-Wl,-rpath,{_capi.LIB_PATH.parent}", "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0 and out.stdout.startswith("bfs-b200")
