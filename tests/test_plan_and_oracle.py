@@ -9,7 +9,7 @@ import pytest
 from cpp_projects_b200 import _capi, synth
 from oracle import pyoracle
 
-# (fmin, fmax, nchan, ncols, max_dt): BASELINE-shaped cases plus odd counts
+# (fmin, fmax, nchan, ncols, max_dt): the workloads' band and channel counts plus odd counts
 CASES = [
     (1200.0, 1600.0, 64, 1024, 64),
     (1200.0, 1600.0, 512, 4096, 512),
