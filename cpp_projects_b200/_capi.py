@@ -34,14 +34,16 @@ class FdmtDesc(ctypes.Structure):
                 ("ncols", ctypes.c_int), ("max_dt", ctypes.c_int), ("plan_kind", ctypes.c_int),
                 ("precision", ctypes.c_int), ("fuse_depth", ctypes.c_int),
                 ("flags", ctypes.c_int), ("head_tile", ctypes.c_int), ("dt_min", ctypes.c_int),
-                ("dt_step", ctypes.c_int), ("tsamp", ctypes.c_float), ("reserved", ctypes.c_int * 3)]
+                ("dt_step", ctypes.c_int), ("tsamp", ctypes.c_float), ("seg_levels", ctypes.c_int),
+                ("seg_rows", ctypes.c_int), ("reserved", ctypes.c_int * 1)]
 
 
 class FdmtInfo(ctypes.Structure):
     _fields_ = [("niter", ctypes.c_int), ("rows_level0", ctypes.c_int),
                 ("fuse_depth", ctypes.c_int), ("rows_total", ctypes.c_int64),
                 ("workspace_bytes", ctypes.c_size_t), ("alg_bytes", ctypes.c_double),
-                ("out_rows", ctypes.c_int)]
+                ("out_rows", ctypes.c_int), ("hbm_passes", ctypes.c_int), ("seg_levels", ctypes.c_int),
+                ("sched_bytes", ctypes.c_double)]
 
 
 class ChunkDesc(ctypes.Structure):
@@ -94,6 +96,9 @@ _SIGNATURES = {
     "bfs_fdmt_plan_create_host": (_I, [ctypes.POINTER(FdmtDesc), ctypes.POINTER(_P)]),
     "bfs_fdmt_autotune": (_I, [ctypes.POINTER(FdmtDesc), ctypes.POINTER(_I), ctypes.POINTER(_I),
                                ctypes.POINTER(_F)]),
+    "bfs_fdmt_autotune_desc": (_I, [ctypes.POINTER(FdmtDesc), ctypes.POINTER(FdmtDesc), ctypes.POINTER(_F)]),
+    "bfs_fdmt_plan_passes": (_I, [_P, ctypes.POINTER(_I), _P, _I]),
+    "bfs_fdmt_plan_segment": (_I, [_P, _I, _P, _I, _P, _I]),
     "bfs_fdmt_plan_destroy": (_I, [_P]),
     "bfs_fdmt_plan_info": (_I, [_P, ctypes.POINTER(FdmtInfo)]),
     "bfs_fdmt_plan_rows": (_I, [_P, _P, _I]),

@@ -694,6 +694,230 @@ cudaError_t launch_level16(const S* src, D* dst, const int4* tab, int rows, int 
     return cudaGetLastError();
 }
 
+constexpr size_t kSegSmemTwoPerSm = 113 * 1024;  // two CTAs of the segment kernel per SM
+
+// Fused merge segment (levels l0+1..l1 over tiles of `rows` level-l1 rows x
+// kSegTile samples; the layout and entries are described with SegPlan).
+// Persistent: CTA b runs tiles b, b + gridDim.x, ... (tile w = row tile
+// w % nrt at time tile w / nrt, so neighbouring CTAs share the rows at tile
+// edges through L2).  A tile's entries and level-l0 rows are copied into
+// shared memory with 16-byte asynchronous copies (each input row's window
+// starts on a 16-byte boundary; pieces outside [0, ncols) are zero-filled
+// and only reach columns no written sample depends on), issued for the NEXT
+// tile before the current one is merged, so HBM loads overlap the merges.
+// Each level merges the rows of the buffer below into the other buffer and
+// level l1 goes straight to HBM:
+//   out[u] = A[u + da] + (t >= shift ? B[u + db] : -)
+// with one round-to-nearest add, so every written sample equals the
+// level-by-level result bit for bit.  A warp merges whole rows, lanes on
+// consecutive columns, so every shared access is one conflict-free
+// wavefront whatever the offsets.
+// Rows without a head row (odd sub-band counts) add the row of -0.0.
+// grid: min(tiles, resident CTAs), block: THREADS
+// 16-byte asynchronous copy to shared-window byte address s (src_bytes < 16:
+// the rest is zero-filled; 0: nothing is read)
+__device__ __forceinline__ void cp_async16(unsigned s, const void* gmem, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// One work item: K consecutive 32-column chunks of one row of a level, from
+// chunk c0, all shared loads issued before the stores.  rd / wr = the float
+// offsets of the buffers of the level below and of this level (32-bit shared
+// offsets, so every access is one LDS / STS with an immediate per chunk).
+// FAST: every sample of the tile is at or past the row's head shift.
+template <int K, bool FAST>
+__device__ __forceinline__ void seg_chunks(float* __restrict__ sm, int rd, int wr, int4 q, int c0,
+                                           int lane, int thr) {
+    const int col = c0 * 32 + lane;
+    const int pa = rd + q.x + col, pb = rd + q.y + col, pw = wr + q.w + col;
+    float va[K], vb[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        va[k] = sm[pa + 32 * k];
+        vb[k] = sm[pb + 32 * k];
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        sm[pw + 32 * k] = (FAST || col + 32 * k >= thr) ? __fadd_rn(va[k], vb[k]) : va[k];
+}
+
+struct SegArgs {
+    const float* in;
+    float* out;
+    const SegTile* tiles;
+    const int4* ent;
+    int ncols, in_pitch, out_pitch, nlev, zx, zy, max_thr, y0, x1, ent_base, max_ent, nrt, total;
+};
+
+template <int NC, int THREADS>
+__global__ void __launch_bounds__(THREADS, THREADS <= 256 ? 2 : 1) k_fdmt_seg(const SegArgs a) {
+    constexpr int kOutCPH = kSegTile / 32;  // chunks of an output row
+    constexpr int kWarps = THREADS / 32;
+    constexpr int kPieces = NC * 8;  // 16-byte pieces per shared row
+    extern __shared__ __align__(16) float sm[];
+    const unsigned sbase = static_cast<unsigned>(__cvta_generic_to_shared(sm));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = threadIdx.x; i < NC * 32; i += THREADS) {
+        sm[a.zx + i] = -0.0f;
+        sm[a.y0 + a.zy + i] = -0.0f;
+        sm[a.x1 + a.zx + i] = -0.0f;
+    }
+
+    // copies tile w's entries and input rows into buffer `buf` (0: X0, 1: X1);
+    // each warp reads the entries of four of its rows at once, then issues
+    // their pieces (a piece starts on a multiple of 4 samples, so it lies
+    // wholly before sample 0 or wholly after it)
+    auto issue = [&](int w, int buf) {
+        const SegTile* tp = a.tiles + w % a.nrt;
+        const int t0 = (w / a.nrt) * kSegTile;
+        const int nin = __ldg(&tp->n[0]);
+        int nent = 0;
+        for (int i = 0; i <= a.nlev; ++i) nent += __ldg(&tp->n[i]);
+        const int4* ge = a.ent + __ldg(&tp->ent);
+        const unsigned se = sbase + 4u * (a.ent_base + 4 * buf * a.max_ent);
+        const unsigned x = sbase + 4u * (buf ? a.x1 : 0);
+        for (int i = threadIdx.x; i < nent; i += THREADS) cp_async16(se + 16u * i, ge + i, 16);
+        for (int r0 = warp; r0 < nin; r0 += 4 * kWarps) {
+            int4 q[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int r = r0 + j * kWarps;
+                q[j] = r < nin ? __ldg(ge + r) : make_int4(0, 0, 0, 0);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (r0 + j * kWarps >= nin) break;
+                const int ts = t0 - q[j].y;  // the row's first sample
+                const float* src = a.in + static_cast<size_t>(q[j].x) * a.in_pitch;
+                const unsigned dst = x + 4u * q[j].w;
+                if (ts >= 0 && ts + 4 * kPieces <= a.ncols) {  // the whole window lies in [0, ncols)
+#pragma unroll
+                    for (int pc = lane; pc < kPieces; pc += 32) cp_async16(dst + 16u * pc, src + ts + 4 * pc, 16);
+                } else {
+                    for (int pc = lane; pc < kPieces; pc += 32) {
+                        const int t = ts + 4 * pc;
+                        const int bytes = t < 0 ? 0 : 4 * max(0, min(4, a.ncols - t));
+                        cp_async16(dst + 16u * pc, bytes > 0 ? src + t : src, bytes);
+                    }
+                }
+            }
+        }
+    };
+
+    int w = blockIdx.x;
+    if (w < a.total) issue(w, 0);
+    for (int j = 0; w < a.total; ++j, w += gridDim.x) {
+        const int buf = j & 1;
+        cp_async_wait_all();
+        __syncthreads();  // this tile's rows are in; every warp is done with the previous tile
+        if (w + static_cast<int>(gridDim.x) < a.total) issue(w + gridDim.x, buf ^ 1);
+
+        const SegTile* tp = a.tiles + w % a.nrt;
+        const int t0 = (w / a.nrt) * kSegTile;
+        const int xo = buf ? a.x1 : 0;  // this tile's X buffer
+        const int4* e = reinterpret_cast<const int4*>(sm + a.ent_base) + buf * a.max_ent + __ldg(&tp->n[0]);
+        const bool fast = t0 >= a.max_thr;  // no sample of this tile precedes its head row's shift
+        for (int lev = 1; lev < a.nlev; ++lev) {
+            const int nl = __ldg(&tp->n[lev]);
+            const int rd = (lev & 1) ? xo : a.y0;
+            const int wr = (lev & 1) ? a.y0 : xo;
+            if (fast) {
+                for (int r = warp; r < nl; r += kWarps) seg_chunks<NC, true>(sm, rd, wr, e[r], 0, lane, 0);
+            } else {
+                for (int r = warp; r < nl; r += kWarps) {
+                    const int4 q = e[r];
+                    seg_chunks<NC, false>(sm, rd, wr, q, 0, lane, q.z - t0);
+                }
+            }
+            e += nl;
+            __syncthreads();
+        }
+        // level l1: kSegTile samples per row, straight to HBM (q.w is the plane row)
+        const int nl = __ldg(&tp->n[a.nlev]);
+        const int rd = (a.nlev & 1) ? xo : a.y0;
+        for (int r = warp; r < nl; r += kWarps) {
+            const int4 q = e[r];
+            const int col = lane;
+            const int pa = rd + q.x + col, pb = rd + q.y + col;
+            float va[kOutCPH], vb[kOutCPH];
+#pragma unroll
+            for (int k = 0; k < kOutCPH; ++k) {
+                va[k] = sm[pa + 32 * k];
+                vb[k] = sm[pb + 32 * k];
+            }
+            float* dst = a.out + static_cast<size_t>(q.w) * a.out_pitch + t0 + col;
+            const int thr = q.z - t0;
+            const int lim = a.ncols - t0 - col;  // samples of this row left from this lane's first
+#pragma unroll
+            for (int k = 0; k < kOutCPH; ++k)
+                if (32 * k < lim) dst[32 * k] = (fast || col + 32 * k >= thr) ? __fadd_rn(va[k], vb[k]) : va[k];
+        }
+    }
+}
+
+template <int NC, int THREADS>
+cudaError_t launch_seg_nc(const SegPlan& sp, const SegArgs& args, cudaStream_t s) {
+    auto kern = k_fdmt_seg<NC, THREADS>;
+    // The shared-memory opt-in is one value per kernel and device: it only
+    // ever grows (a smaller setting would refuse a later, larger launch).
+    // Resident CTAs per SM are cached per (device, size).  Both happen on the
+    // first launch of a size, which therefore comes before any stream capture.
+    static std::mutex mu;
+    static std::map<int, size_t> optin;
+    static std::map<std::pair<int, size_t>, int> resident;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int per_sm = 0, sms = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        size_t& have = optin[dev];
+        if (have < sp.smem_bytes) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 static_cast<int>(sp.smem_bytes));
+            if (e != cudaSuccess) return e;
+            have = sp.smem_bytes;
+        }
+        auto it = resident.find({dev, sp.smem_bytes});
+        if (it == resident.end()) {
+            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, sp.smem_bytes);
+            if (e != cudaSuccess) return e;
+            if (per_sm < 1) return cudaErrorInvalidConfiguration;
+            it = resident.emplace(std::make_pair(dev, sp.smem_bytes), per_sm).first;
+        }
+        per_sm = it->second;
+    }
+    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    const int grid = std::min(args.total, sms * per_sm);
+    kern<<<grid, THREADS, sp.smem_bytes, s>>>(args);
+    return cudaGetLastError();
+}
+
+// Launches one fused segment (sp.nc is one of the instantiated chunk counts;
+// 256 threads when two CTAs fit an SM, else 512).
+cudaError_t launch_seg(const SegPlan& sp, const float* src, float* dst, const SegTile* tiles,
+                       const int4* ent, int T, int in_pitch, int out_pitch, cudaStream_t s) {
+    SegArgs a;
+    a.in = src; a.out = dst; a.tiles = tiles; a.ent = ent;
+    a.ncols = T; a.in_pitch = in_pitch; a.out_pitch = out_pitch;
+    a.nlev = sp.l1 - sp.l0; a.max_thr = sp.max_thr;
+    a.zx = sp.rows_x * sp.pitch; a.zy = sp.rows_y * sp.pitch;
+    a.y0 = sp.y0; a.x1 = sp.x1; a.ent_base = sp.ent_base; a.max_ent = sp.max_ent;
+    a.nrt = static_cast<int>(sp.tiles.size());
+    const long long total = static_cast<long long>(a.nrt) * ((T + kSegTile - 1) / kSegTile);
+    if (total > (1LL << 30)) return cudaErrorInvalidConfiguration;
+    a.total = static_cast<int>(total);
+    const bool two = sp.smem_bytes <= kSegSmemTwoPerSm;
+    switch (sp.nc) {
+        case 9: return two ? launch_seg_nc<9, 256>(sp, a, s) : launch_seg_nc<9, 512>(sp, a, s);
+        case 10: return two ? launch_seg_nc<10, 256>(sp, a, s) : launch_seg_nc<10, 512>(sp, a, s);
+        case 12: return two ? launch_seg_nc<12, 256>(sp, a, s) : launch_seg_nc<12, 512>(sp, a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 // Row pitch (elements) of the workspace planes: ncols rounded up to 128 bytes.
 inline int plane_pitch(int ncols, int elem_bytes = 4) {
     const int per = 128 / elem_bytes;
@@ -733,6 +957,75 @@ static std::vector<std::vector<int>> row_exponents(const FdmtPlanHost& h) {
     return ex;
 }
 
+constexpr int kSegDefaultLevels = 3;
+
+// The passes after the head (or level 0): levels k+1..niter cut into fused
+// segments of about desc->seg_levels levels (FP32 plans), or one plain merge
+// pass per level; then the ping-pong plane of every level that reaches HBM.
+static bfs_status build_passes(const bfs_fdmt_desc* desc, bfs_fdmt_plan* p) {
+    const FdmtPlanHost& h = p->host;
+    const int k = p->head.depth;
+    const int want = desc->seg_levels == 0 ? kSegDefaultLevels : desc->seg_levels;
+    BFS_ARG(want >= 1 && want <= kSegMaxLevels, "seg_levels %d out of range (0..%d)", desc->seg_levels,
+            kSegMaxLevels);
+    BFS_ARG(desc->seg_rows >= 0, "seg_rows %d is negative", desc->seg_rows);
+    const bool explicit_seg = desc->seg_levels >= 2 || desc->seg_rows > 0;
+    BFS_ARG(!explicit_seg || p->precision == BFS_PREC_F32,
+            "fused merge segments are implemented for FP32 plans");
+    p->passes.clear();
+    auto plain = [&](int l) {
+        SegPlan sp;
+        sp.l0 = l - 1;
+        sp.l1 = l;
+        p->passes.push_back(sp);
+    };
+    const int left = h.niter - k;
+    if (want < 2 || p->precision != BFS_PREC_F32 || left < 2) {
+        for (int l = k + 1; l <= h.niter; ++l) plain(l);
+    } else {
+        const int nseg = (left + want - 1) / want;
+        int l0 = k;
+        for (int i = 0; i < nseg; ++i) {
+            const int l1 = l0 + left / nseg + (i < left % nseg ? 1 : 0);
+            if (l1 == l0 + 1) {
+                plain(l1);
+            } else {
+                // rows per tile: the most that keep two CTAs per SM, else one
+                std::vector<std::pair<int, size_t>> rows_try = {
+                    {64, kHeadSmemTwoPerSm}, {32, kHeadSmemTwoPerSm}, {16, kHeadSmemTwoPerSm},
+                    {32, kHeadSmemMax}, {16, kHeadSmemMax}, {8, kHeadSmemMax}};
+                if (desc->seg_rows > 0) rows_try = {{desc->seg_rows, kHeadSmemMax}};
+                bool ok = false;
+                for (const auto& [G, limit] : rows_try) {
+                    SegPlan sp;
+                    if (build_seg_plan(h, l0, l1, G, kSegTile, limit, &sp)) {
+                        p->passes.push_back(std::move(sp));
+                        ok = true;
+                        break;
+                    }
+                }
+                BFS_ARG(ok || !explicit_seg, "seg_levels %d / seg_rows %d are not usable for this plan",
+                        desc->seg_levels, desc->seg_rows);
+                if (!ok)
+                    for (int l = l0 + 1; l <= l1; ++l) plain(l);
+            }
+            l0 = l1;
+        }
+    }
+    // planes in HBM: level k, then every pass's output, alternating between
+    // the two buffers (the last level goes to the caller's output)
+    p->plane_buf.assign(h.niter + 1, -1);
+    int b = 0;
+    p->plane_buf[k] = b;
+    for (const SegPlan& sp : p->passes) p->plane_buf[sp.l1] = (b ^= 1);
+    p->buf_rows[0] = p->buf_rows[1] = 0;
+    for (int l = k; l < h.niter; ++l)
+        if (p->plane_buf[l] >= 0)
+            p->buf_rows[p->plane_buf[l]] =
+                std::max(p->buf_rows[p->plane_buf[l]], static_cast<size_t>(h.lv[l].total_rows()));
+    return BFS_OK;
+}
+
 static bfs_status plan_host_part(const bfs_fdmt_desc* desc, std::unique_ptr<bfs_fdmt_plan>& p) {
     BFS_ARG(desc != nullptr, "null argument");
     BFS_ARG(desc->plan_kind == BFS_PLAN_KEITH || desc->plan_kind == BFS_PLAN_PRAVIR,
@@ -750,7 +1043,7 @@ static bfs_status plan_host_part(const bfs_fdmt_desc* desc, std::unique_ptr<bfs_
                                           desc->dt_step > 0 ? desc->dt_step : 1, desc->dt_min, &p->host);
         if (st != BFS_OK) return st;
         p->fuse_depth = 0;
-        return BFS_OK;
+        return build_passes(desc, p.get());
     }
     bfs_status st = build_fdmt_plan(desc->fmin, desc->fmax, desc->nchan, desc->ncols,
                                     desc->max_dt, &p->host);
@@ -776,7 +1069,7 @@ static bfs_status plan_host_part(const bfs_fdmt_desc* desc, std::unique_ptr<bfs_
                 "fuse_depth %d is not usable for this plan", desc->fuse_depth);
     }
     p->fuse_depth = p->head.depth;
-    return BFS_OK;
+    return build_passes(desc, p.get());
 }
 
 static inline int bfs_fdmt_plan_depth_of(int d) { return d; }
@@ -794,7 +1087,7 @@ struct TuneKey {
                         o.fmin_bits, o.fmax_bits);
     }
 };
-struct TuneVal { int depth, tile; float ms; };
+struct TuneVal { int depth, tile, seg, rows; float ms; };
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneVal> g_tune;
 
@@ -817,17 +1110,24 @@ static bfs_status tune_fdmt(const bfs_fdmt_desc& base, TuneVal* best) {
         auto it = g_tune.find(tune_key(base));
         if (it != g_tune.end()) { *best = it->second; return BFS_OK; }
     }
-    struct Cand { int depth, tile; };
-    std::vector<Cand> cands = {{0, 0}};
+    struct Cand { int depth, tile, seg, rows; };
+    std::vector<Cand> cands;
+    // one merge pass per level: head depth x head tile
+    cands.push_back({0, 0, 1, 0});
     for (int k : {2, 3, 4, 5})
-        for (int tile : {256, 512}) cands.push_back({k, tile});
+        for (int tile : {256, 512}) cands.push_back({k, tile, 1, 0});
+    // fused merge segments of 2, 3 or 4 levels x 16 or 32 rows per tile (FP32)
+    if (base.precision == BFS_PREC_F32)
+        for (int seg : {2, 3, 4})
+            for (int rows : {16, 32})
+                for (int k : {0, 2, 3, 4}) cands.push_back({k, k ? 256 : 0, seg, rows});
     const size_t in_n = static_cast<size_t>(base.nchan) * base.ncols;
     const size_t out_n = static_cast<size_t>(base.max_dt) * base.ncols;
     float *d_in = nullptr, *d_out = nullptr;
     void* ws = nullptr;
     size_t ws_bytes = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    TuneVal win{0, 0, 1e30f};
+    TuneVal win{0, 0, 1, 0, 1e30f};
     bfs_status st = BFS_OK;
     cudaStream_t s = nullptr;
     if (cudaMalloc(&d_in, in_n * sizeof(float)) != cudaSuccess ||
@@ -841,6 +1141,8 @@ static bfs_status tune_fdmt(const bfs_fdmt_desc& base, TuneVal* best) {
         bfs_fdmt_desc d = base;
         d.fuse_depth = c.depth;
         d.head_tile = c.tile;
+        d.seg_levels = c.seg;
+        d.seg_rows = c.rows;
         d.flags = BFS_FDMT_EXTERNAL_WS;
         bfs_fdmt_plan* p = nullptr;
         if (bfs_fdmt_plan_create(&d, &p) != BFS_OK) continue;  // depth/tile not usable here
@@ -853,8 +1155,12 @@ static bfs_status tune_fdmt(const bfs_fdmt_desc& base, TuneVal* best) {
             ws_bytes = need;
         }
         float ms = 1e30f;
+        // a segment length that fell back to plain levels duplicates seg = 1
+        bool fused = false;
+        for (const SegPlan& sp : p->passes) fused |= !sp.tiles.empty();
+        if (c.seg > 1 && !fused) { bfs_fdmt_plan_destroy(p); continue; }
         bool ok = bfs_fdmt_execute_ws(p, d_in, d_out, 0, ws, ws_bytes, s) == BFS_OK;
-        for (int rep = 0; rep < 3 && ok; ++rep) {
+        for (int rep = 0; rep < 2 && ok; ++rep) {
             cudaEventRecord(e0, s);
             ok = bfs_fdmt_execute_ws(p, d_in, d_out, 0, ws, ws_bytes, s) == BFS_OK;
             cudaEventRecord(e1, s);
@@ -864,7 +1170,7 @@ static bfs_status tune_fdmt(const bfs_fdmt_desc& base, TuneVal* best) {
             ms = std::min(ms, t);
         }
         bfs_fdmt_plan_destroy(p);
-        if (ok && ms < win.ms) win = TuneVal{bfs_fdmt_plan_depth_of(c.depth), c.tile, ms};
+        if (ok && ms < win.ms) win = TuneVal{bfs_fdmt_plan_depth_of(c.depth), c.tile, c.seg, c.rows, ms};
     }
     if (ws) cudaFree(ws);
     if (d_in) cudaFree(d_in);
@@ -879,14 +1185,28 @@ static bfs_status tune_fdmt(const bfs_fdmt_desc& base, TuneVal* best) {
     return BFS_OK;
 }
 
-extern "C" bfs_status bfs_fdmt_autotune(const bfs_fdmt_desc* desc, int* depth, int* tile, float* ms) {
+extern "C" bfs_status bfs_fdmt_autotune_desc(const bfs_fdmt_desc* desc, bfs_fdmt_desc* tuned, float* ms) {
     BFS_ARG(desc != nullptr, "null argument");
     TuneVal v{};
     bfs_status st = tune_fdmt(*desc, &v);
     if (st != BFS_OK) return st;
-    if (depth) *depth = v.depth;
-    if (tile) *tile = v.tile;
+    if (tuned) {
+        *tuned = *desc;
+        tuned->fuse_depth = v.depth;
+        tuned->head_tile = v.tile;
+        tuned->seg_levels = v.seg;
+        tuned->seg_rows = v.rows;
+    }
     if (ms) *ms = v.ms;
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_fdmt_autotune(const bfs_fdmt_desc* desc, int* depth, int* tile, float* ms) {
+    bfs_fdmt_desc t{};
+    bfs_status st = bfs_fdmt_autotune_desc(desc, &t, ms);
+    if (st != BFS_OK) return st;
+    if (depth) *depth = t.fuse_depth;
+    if (tile) *tile = t.head_tile;
     return BFS_OK;
 }
 
@@ -910,6 +1230,8 @@ extern "C" bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc_in, bfs_fdm
         if (ts != BFS_OK) return ts;
         tuned.fuse_depth = v.depth;
         tuned.head_tile = v.tile;
+        tuned.seg_levels = v.seg;
+        tuned.seg_rows = v.rows;
     }
     const bfs_fdmt_desc* desc = &tuned;
     std::unique_ptr<bfs_fdmt_plan> p;
@@ -957,10 +1279,28 @@ extern "C" bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc_in, bfs_fdm
         BFS_CUDA(cudaMemcpy(p->d_tab, tab.data(), tab.size() * sizeof(int4),
                             cudaMemcpyHostToDevice));
     }
-    // ping-pong planes: level l lives in buffer l & 1; the last level goes to the
-    // output; levels inside the fused head never reach HBM
-    for (int l = p->head.depth; l < h.niter; ++l)
-        p->buf_rows[l & 1] = std::max(p->buf_rows[l & 1], static_cast<size_t>(h.lv[l].total_rows()));
+    // fused segments: every pass's tiles and entries, concatenated
+    {
+        std::vector<SegTile> tiles;
+        std::vector<int> ent;
+        p->seg_tile0.assign(p->passes.size(), 0);
+        p->seg_ent0.assign(p->passes.size(), 0);
+        for (size_t i = 0; i < p->passes.size(); ++i) {
+            p->seg_tile0[i] = tiles.size();
+            p->seg_ent0[i] = ent.size();
+            tiles.insert(tiles.end(), p->passes[i].tiles.begin(), p->passes[i].tiles.end());
+            ent.insert(ent.end(), p->passes[i].ent.begin(), p->passes[i].ent.end());
+        }
+        if (!tiles.empty()) {
+            BFS_CUDA(cudaMalloc(&p->d_seg_tiles, tiles.size() * sizeof(SegTile)));
+            BFS_CUDA(cudaMemcpy(p->d_seg_tiles, tiles.data(), tiles.size() * sizeof(SegTile),
+                                cudaMemcpyHostToDevice));
+            BFS_CUDA(cudaMalloc(&p->d_seg_ent, ent.size() * sizeof(int)));
+            BFS_CUDA(cudaMemcpy(p->d_seg_ent, ent.data(), ent.size() * sizeof(int), cudaMemcpyHostToDevice));
+        }
+    }
+    // ping-pong planes (sized by build_passes); levels inside the fused head
+    // or a fused segment never reach HBM
     p->external_ws = (desc->flags & BFS_FDMT_EXTERNAL_WS) != 0;
     const int eb = elem_bytes_of(p->precision);
     for (int b = 0; b < 2 && !p->external_ws; ++b) {
@@ -1003,6 +1343,41 @@ extern "C" bfs_status bfs_fdmt_plan_head(const bfs_fdmt_plan* plan, int* params,
     return BFS_OK;
 }
 
+extern "C" bfs_status bfs_fdmt_plan_passes(const bfs_fdmt_plan* plan, int* npasses, int* params, int cap) {
+    BFS_ARG(plan != nullptr && npasses != nullptr, "null argument");
+    const int n = static_cast<int>(plan->passes.size());
+    *npasses = n;
+    if (params) {
+        BFS_ARG(cap >= 12 * n, "params needs %d ints", 12 * n);
+        for (int i = 0; i < n; ++i) {
+            const SegPlan& sp = plan->passes[i];
+            const int v[12] = {sp.l0, sp.l1, sp.rows, sp.tile, sp.nc, sp.pitch, sp.rows_x, sp.rows_y,
+                               sp.max_ent, sp.max_thr, static_cast<int>(sp.tiles.size()),
+                               static_cast<int>(sp.ent.size() / 4)};
+            std::memcpy(params + 12 * i, v, sizeof(v));
+        }
+    }
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_fdmt_plan_segment(const bfs_fdmt_plan* plan, int pass, int* tiles, int tiles_cap,
+                                            int* ent, int ent_cap) {
+    BFS_ARG(plan != nullptr, "null argument");
+    BFS_ARG(pass >= 0 && pass < static_cast<int>(plan->passes.size()), "pass %d out of range", pass);
+    const SegPlan& sp = plan->passes[pass];
+    constexpr int ti = static_cast<int>(sizeof(SegTile) / sizeof(int));
+    static_assert(ti == 8, "SegTile is 8 ints");
+    if (tiles) {
+        BFS_ARG(tiles_cap >= ti * static_cast<int>(sp.tiles.size()), "tiles needs %zu ints", ti * sp.tiles.size());
+        std::memcpy(tiles, sp.tiles.data(), sp.tiles.size() * sizeof(SegTile));
+    }
+    if (ent) {
+        BFS_ARG(ent_cap >= static_cast<int>(sp.ent.size()), "ent needs %zu ints", sp.ent.size());
+        std::memcpy(ent, sp.ent.data(), sp.ent.size() * sizeof(int));
+    }
+    return BFS_OK;
+}
+
 // Bytes of the level-by-level algorithm: the input read, the level-0 plane
 // written, each level's two input rows read and output row written per
 // output row; intermediate planes of eb bytes per value, the output FP32.
@@ -1026,6 +1401,17 @@ extern "C" bfs_status bfs_fdmt_plan_info(const bfs_fdmt_plan* plan, bfs_fdmt_inf
     info->workspace_bytes = plan->ws_bytes;
     info->alg_bytes = fdmt_alg_bytes(h, plan->precision);
     info->out_rows = h.out_rows();
+    info->hbm_passes = static_cast<int>(plan->passes.size());
+    int seg = 1;
+    for (const SegPlan& sp : plan->passes) seg = std::max(seg, sp.l1 - sp.l0);
+    info->seg_levels = seg;
+    // every plane that reaches HBM written once and read once, the input read,
+    // the output written: the DRAM bytes this schedule cannot avoid
+    const double eb = elem_bytes_of(plan->precision);
+    double rows = 4.0 * h.nchan + 4.0 * h.out_rows();
+    for (int l = 0; l < h.niter; ++l)
+        if (!plan->plane_buf.empty() && plan->plane_buf[l] >= 0) rows += 2.0 * eb * h.lv[l].total_rows();
+    info->sched_bytes = rows * h.ncols;
     return BFS_OK;
 }
 
@@ -1126,21 +1512,22 @@ static bfs_status fdmt_run16(bfs_fdmt_plan* plan, const float* d_in, float* d_ou
         cudaError_t e = (k == h.niter)
             ? launch_head<float>(hp, h, d_in, d_out, T, plan->d_head_groups, plan->d_head_tab,
                                  b_ones ? 1 : 0, s)
-            : launch_head<S>(hp, h, d_in, bufs[k & 1], P, plan->d_head_groups, plan->d_head_tab,
-                             b_ones ? 1 : 0, s);
+            : launch_head<S>(hp, h, d_in, bufs[plan->plane_buf[k]], P, plan->d_head_groups,
+                             plan->d_head_tab, b_ones ? 1 : 0, s);
         if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_head: %s", cudaGetErrorString(e));
     } else {
         BFS_ARG(h.nchan <= 65535, "nchan too large for this build");
-        cudaError_t e = launch_init<S>(d_in, bufs[0], h, P, b_ones ? 1 : 0, s, plan->d_lvl0);
+        cudaError_t e = launch_init<S>(d_in, bufs[plan->plane_buf[0]], h, P, b_ones ? 1 : 0, s, plan->d_lvl0);
         if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_init: %s", cudaGetErrorString(e));
     }
-    for (int l = k + 1; l <= h.niter; ++l) {
-        const S* src = bufs[(l - 1) & 1];
+    for (const SegPlan& sp : plan->passes) {  // 16-bit plans: one plain pass per level
+        const int l = sp.l1;
+        const S* src = bufs[plan->plane_buf[sp.l0]];
         const int4* tab = plan->d_tab + plan->tab_off[l];
         const int rows = h.lv[l].total_rows();
         cudaError_t e = (l == h.niter)
             ? launch_level16<S, float>(src, d_out, tab, rows, T, P, T, s)
-            : launch_level16<S, S>(src, bufs[l & 1], tab, rows, T, P, P, s);
+            : launch_level16<S, S>(src, bufs[plan->plane_buf[l]], tab, rows, T, P, P, s);
         if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_level16: %s", cudaGetErrorString(e));
     }
     return BFS_OK;
@@ -1166,25 +1553,35 @@ static bfs_status fdmt_run(bfs_fdmt_plan* plan, const float* d_in, float* d_out,
     const int T = h.ncols;
     const int P = plane_pitch(T);
     float* bufs[2] = {buf0, buf1};
+    auto plane = [&](int l) { return l == h.niter ? d_out : bufs[plan->plane_buf[l]]; };
+    auto pitch = [&](int l) { return l == h.niter ? T : P; };
     const int k = plan->head.depth;
     if (k > 0) {
         const HeadPlan& hp = plan->head;
         BFS_ARG(h.nchan / hp.group <= 65535, "nchan too large for this build");
-        float* dst = (k == h.niter) ? d_out : bufs[k & 1];
-        cudaError_t e = launch_head<float>(hp, h, d_in, dst, (k == h.niter) ? T : P,
-                                           plan->d_head_groups, plan->d_head_tab, b_ones ? 1 : 0, s);
+        cudaError_t e = launch_head<float>(hp, h, d_in, plane(k), pitch(k), plan->d_head_groups,
+                                           plan->d_head_tab, b_ones ? 1 : 0, s);
         if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_head: %s", cudaGetErrorString(e));
     } else {
         BFS_ARG(h.nchan <= 65535, "nchan too large for this build");
-        cudaError_t e = launch_init<float>(d_in, bufs[0], h, P, b_ones ? 1 : 0, s, plan->d_lvl0);
+        cudaError_t e = launch_init<float>(d_in, plane(0), h, P, b_ones ? 1 : 0, s, plan->d_lvl0);
         if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_init: %s", cudaGetErrorString(e));
     }
-    for (int l = k + 1; l <= h.niter; ++l) {
-        const float* src = bufs[(l - 1) & 1];
-        float* dst = (l == h.niter) ? d_out : bufs[l & 1];
-        cudaError_t e = launch_level(src, dst, plan->d_tab + plan->tab_off[l], h.lv[l].total_rows(),
-                                     T, P, (l == h.niter) ? T : P, s);
-        if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_level: %s", cudaGetErrorString(e));
+    for (size_t i = 0; i < plan->passes.size(); ++i) {
+        const SegPlan& sp = plan->passes[i];
+        const float* src = plane(sp.l0);
+        cudaError_t e;
+        if (sp.tiles.empty()) {
+            e = launch_level(src, plane(sp.l1), plan->d_tab + plan->tab_off[sp.l1],
+                             h.lv[sp.l1].total_rows(), T, P, pitch(sp.l1), s);
+        } else {
+            e = launch_seg(sp, src, plane(sp.l1), plan->d_seg_tiles + plan->seg_tile0[i],
+                           reinterpret_cast<const int4*>(plan->d_seg_ent + plan->seg_ent0[i]), T, P,
+                           pitch(sp.l1), s);
+        }
+        if (e != cudaSuccess)
+            return fail(BFS_ERR_CUDA, "%s (levels %d..%d): %s", sp.tiles.empty() ? "k_fdmt_level" : "k_fdmt_seg",
+                        sp.l0 + 1, sp.l1, cudaGetErrorString(e));
     }
     return BFS_OK;
 }

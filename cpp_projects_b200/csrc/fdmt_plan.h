@@ -22,6 +22,13 @@ struct bfs_fdmt_plan {
     bfs::HeadPlan head;                     // fused levels 0..k (depth 0 = not used)
     bfs::HeadGroup* d_head_groups = nullptr;
     int* d_head_tab = nullptr;
+    // passes after the head (or level 0): a fused segment of levels l0+1..l1
+    // (tiles non-empty) or one plain merge level (l1 = l0 + 1, no tiles)
+    std::vector<bfs::SegPlan> passes;
+    std::vector<int> plane_buf;        // per level: ping-pong plane holding it in HBM (-1: never)
+    bfs::SegTile* d_seg_tiles = nullptr;  // every fused segment's tiles, concatenated
+    int* d_seg_ent = nullptr;          // every fused segment's entries, concatenated
+    std::vector<size_t> seg_tile0, seg_ent0;  // per pass: offsets into the two arrays
     int* d_lvl0 = nullptr;             // Pravir plans: level-0 row cumsum (nchan+1) then delays
     int* d_ones_tau = nullptr;         // FDMT of 0/1 rows: tau [out_row][channel] (first use)
     int ones_max_tau = -1;
@@ -36,6 +43,8 @@ struct bfs_fdmt_plan {
         if (d_head_groups) cudaFree(d_head_groups);
         if (d_head_tab) cudaFree(d_head_tab);
         if (d_lvl0) cudaFree(d_lvl0);
+        if (d_seg_tiles) cudaFree(d_seg_tiles);
+        if (d_seg_ent) cudaFree(d_seg_ent);
         if (d_ones_tau) cudaFree(d_ones_tau);
         for (void* b : d_buf)
             if (b) cudaFree(b);

@@ -131,4 +131,66 @@ struct HeadPlan {
 // (k > trailing zero bits of nchan, k > niter, or too much shared memory).
 bool build_head_plan(const FdmtPlanHost& p, int k, int tile, size_t smem_limit, HeadPlan* out);
 
+// ---------------------------------------------------------------------------
+// Fused merge segment: levels l0+1..l1 in one pass over HBM.  The level-l1
+// plane is cut into tiles of `rows` consecutive rows x `tile` samples.  For
+// one such tile the rows of levels l0..l1-1 it depends on (a row DAG through
+// the merge tables) are held in shared memory, each over its own window of
+// samples: a row reached from the tile's rows through head shifts between
+// lo and hi samples in total needs the samples [t0 - hi, t0 + tile - lo),
+// which is `tile` + (hi - lo) columns wide, and hi - lo stays small (the
+// shifts of neighbouring rows differ by a sample or two), however large the
+// shifts themselves are.  So any adjacent levels fuse, the last ones
+// included, with only the level-l0 rows read from HBM and the level-l1
+// rows written.
+// ---------------------------------------------------------------------------
+constexpr int kSegMaxLevels = 6;
+constexpr int kSegTile = 256;    // output samples per segment tile
+constexpr int kSegMaxChunks = 12;  // 32-column chunks per shared row at most
+
+struct SegTile {                 // device-side, one per row tile of a segment
+    int ent;                     // first entry of the tile in the segment's entries
+    int n[kSegMaxLevels + 1];    // n[0] input rows, n[i] rows of level l0 + i (n[m]: output)
+};
+
+// Shared memory: three buffers X0, Y, X1, each of its rows, then a row of
+// -0.0 (x + -0 == x bit for bit: the head row of rows without one) and a
+// guard row (a chunk of the last row may read up to one pitch past it, in
+// columns no written sample depends on); then the entries of two tiles.
+// Level i of a tile is held in X (i even) or Y (i odd); a CTA runs tiles one
+// after another, loading the next tile's input rows into the other X buffer
+// while it merges the current one.  Entries, 4 ints each, in the tile's
+// order: n[0] input rows {plane row, window lead E (a multiple of 4, so each
+// row's window starts on a 16-byte boundary of the plane), 0, offset in X},
+// then for every level i = 1..m its rows {offset of the tail row's sample and
+// of the head row's sample minus the shift, both in the buffer of level
+// i-1, first sample that adds the head row relative to t0 (shift + lead),
+// destination: offset in the buffer of level i, or the plane row at level
+// m}.  Offsets count floats; local column u of a row with lead E holds
+// sample t0 - E + u.
+struct SegPlan {
+    int l0 = 0, l1 = 0;
+    int rows = 0;                // output rows per tile
+    int tile = 0;                // output samples per tile (multiple of 32)
+    int nc = 0;                  // 32-column chunks per shared row
+    int pitch = 0;               // floats per shared row (32 nc)
+    int rows_x = 0, rows_y = 0;  // rows of buffer X (levels l0, l0+2, ..) and Y (l0+1, ..)
+    int size_x = 0, size_y = 0;  // floats of a buffer: its rows, the -0.0 row, the guard row
+    int max_thr = 0;             // tiles with t0 >= max_thr never need the t >= shift test
+    int max_in_rows = 0;         // most input rows of one tile
+    int64_t in_rows = 0;         // input rows summed over tiles (HBM reads per time tile)
+    int y0 = 0, x1 = 0;          // offsets of buffers Y and X1 (X0 is at 0)
+    int ent_base = 0;            // offset (floats) of the two staged entry buffers
+    int max_ent = 0;             // most entries of one tile
+    size_t smem_bytes = 0;
+    std::vector<SegTile> tiles;
+    std::vector<int> ent;
+};
+
+// Segment plan for levels l0+1..l1 with `rows` output rows and `tile`
+// samples per tile; false when it needs more than kSegMaxLevels levels,
+// kSegMaxChunks chunks per row or smem_limit bytes of shared memory.
+bool build_seg_plan(const FdmtPlanHost& p, int l0, int l1, int rows, int tile, size_t smem_limit,
+                    SegPlan* out);
+
 }  // namespace bfs

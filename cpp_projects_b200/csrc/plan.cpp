@@ -217,6 +217,118 @@ bool build_head_plan(const FdmtPlanHost& p, int k, int tile, size_t smem_limit, 
     return true;
 }
 
+bool build_seg_plan(const FdmtPlanHost& p, int l0, int l1, int G, int TT, size_t smem_limit,
+                    SegPlan* out) {
+    const int m = l1 - l0;
+    if (m < 1 || m > kSegMaxLevels || l0 < 0 || l1 > p.niter || G < 1 || TT != kSegTile) return false;
+    // window of a row: {lo, hi} = least and largest total head shift from the tile's rows
+    struct Win { int row, lo, hi; };
+    const int R = p.lv[l1].total_rows();
+    std::vector<std::vector<std::vector<Win>>> tiles;  // [tile][i = 0..m] rows sorted by row
+    int spread = 0;
+    for (int g0 = 0; g0 < R; g0 += G) {
+        std::vector<std::vector<Win>> need(m + 1);
+        for (int g = g0; g < std::min(R, g0 + G); ++g) need[m].push_back({g, 0, 0});
+        for (int i = m; i >= 1; --i) {
+            const FdmtLevel& L = p.lv[l0 + i];
+            std::vector<Win> below;
+            below.reserve(2 * need[i].size());
+            for (const Win& w : need[i]) {
+                below.push_back({L.a_row[w.row], w.lo, w.hi});
+                if (L.b_row[w.row] >= 0)
+                    below.push_back({L.b_row[w.row], w.lo + L.shift[w.row], w.hi + L.shift[w.row]});
+            }
+            std::sort(below.begin(), below.end(), [](const Win& a, const Win& b) { return a.row < b.row; });
+            for (const Win& w : below) {
+                if (!need[i - 1].empty() && need[i - 1].back().row == w.row) {
+                    Win& v = need[i - 1].back();
+                    v.lo = std::min(v.lo, w.lo);
+                    v.hi = std::max(v.hi, w.hi);
+                } else {
+                    need[i - 1].push_back(w);
+                }
+            }
+            for (const Win& w : need[i - 1]) spread = std::max(spread, w.hi - w.lo);
+        }
+        // input rows start their window on a multiple of 4 samples (16-byte
+        // copies): the lead grows to the next multiple of 4, the window by as much
+        for (Win& w : need[0]) {
+            const int e4 = (w.hi + 3) & ~3;
+            spread = std::max(spread, e4 - w.lo);
+            w.hi = e4;
+        }
+        tiles.push_back(std::move(need));
+    }
+    SegPlan s;
+    s.l0 = l0; s.l1 = l1; s.rows = G; s.tile = TT;
+    // chunks per shared row, rounded up to a count the kernel instantiates
+    // (9, 10 or 12 for the 256-sample tile)
+    const int nc = (TT + spread + 31) / 32;
+    s.nc = nc <= 9 ? 9 : nc <= 10 ? 10 : 12;
+    if (nc > kSegMaxChunks) return false;
+    s.pitch = 32 * s.nc;
+    for (const auto& need : tiles) {
+        for (int i = 0; i < m; ++i) {
+            int& r = (i & 1) ? s.rows_y : s.rows_x;
+            r = std::max(r, static_cast<int>(need[i].size()));
+        }
+        s.max_in_rows = std::max(s.max_in_rows, static_cast<int>(need[0].size()));
+        s.in_rows += static_cast<int64_t>(need[0].size());
+    }
+    s.size_x = (s.rows_x + 2) * s.pitch;
+    s.size_y = (s.rows_y + 2) * s.pitch;
+    s.y0 = s.size_x;
+    s.x1 = s.size_x + s.size_y;
+    s.ent_base = s.x1 + s.size_x;
+    for (const auto& need : tiles) {
+        int ne = 0;
+        for (int i = 0; i <= m; ++i) ne += static_cast<int>(need[i].size());
+        s.max_ent = std::max(s.max_ent, ne);
+    }
+    s.smem_bytes = static_cast<size_t>(s.ent_base) * sizeof(float) + 2 * static_cast<size_t>(s.max_ent) * 16;
+    if (s.smem_bytes > smem_limit) return false;
+    auto zero_of = [&](int i) { return ((i & 1) ? s.rows_y : s.rows_x) * s.pitch; };
+    auto slot_of = [](const std::vector<Win>& v, int row) {
+        auto it = std::lower_bound(v.begin(), v.end(), row, [](const Win& w, int r) { return w.row < r; });
+        return static_cast<int>(it - v.begin());
+    };
+    for (const auto& need : tiles) {
+        SegTile st{};
+        st.ent = static_cast<int>(s.ent.size() / 4);
+        for (int i = 0; i <= m; ++i) st.n[i] = static_cast<int>(need[i].size());
+        for (int j = 0; j < st.n[0]; ++j) {
+            const Win& w = need[0][j];
+            s.ent.insert(s.ent.end(), {w.row, w.hi, 0, j * s.pitch});
+        }
+        for (int i = 1; i <= m; ++i) {
+            const FdmtLevel& L = p.lv[l0 + i];
+            const std::vector<Win>& lower = need[i - 1];
+            for (int j = 0; j < st.n[i]; ++j) {
+                const Win& w = need[i][j];
+                const int eg = i == m ? 0 : w.hi;  // output rows: lead 0 (samples t0 ..)
+                const int ja = slot_of(lower, L.a_row[w.row]);
+                const int offa = ja * s.pitch + (lower[ja].hi - eg);
+                int offb = zero_of(i - 1), thr = 0;
+                if (L.b_row[w.row] >= 0) {
+                    const int jb = slot_of(lower, L.b_row[w.row]);
+                    const int sh = L.shift[w.row];
+                    offb = jb * s.pitch + (lower[jb].hi - eg - sh);
+                    thr = sh + eg;
+                    s.max_thr = std::max(s.max_thr, thr);
+                    // the head row's window covers every sample this row reads
+                    if (lower[jb].hi - eg - sh < 0 || lower[jb].lo > w.lo + sh) return false;
+                    if (lower[jb].hi - eg - sh > s.pitch) return false;
+                }
+                if (lower[ja].hi - eg < 0 || lower[ja].lo > w.lo || lower[ja].hi - eg > s.pitch) return false;
+                const int dst = i == m ? w.row : j * s.pitch;
+                s.ent.insert(s.ent.end(), {offa, offb, thr, dst});
+            }
+        }
+        s.tiles.push_back(st);
+    }
+    *out = std::move(s);
+    return true;
+}
 
 void build_adjoint_tables(const FdmtPlanHost& p, AdjointTables* out) {
     out->off_pos.assign(p.niter + 1, 0);

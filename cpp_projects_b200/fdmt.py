@@ -20,8 +20,9 @@ from ._tensors import dev_ptr, stream_handle
 
 
 def autotune(Fmin: float, Fmax: float, nchan: int, cols: int, imaxDt: int) -> tuple[int, int, float]:
-    """Time the fused-head depths and tile widths for this shape on the
-    current device (cached per shape): returns (fuse_depth, head_tile, ms)."""
+    """Time the fused-head depths, tile widths and merge-segment lengths for
+    this shape on the current device (cached per shape): returns
+    (fuse_depth, head_tile, ms)."""
     desc = _capi.FdmtDesc(fmin=float(Fmin), fmax=float(Fmax), nchan=int(nchan), ncols=int(cols),
                           max_dt=int(imaxDt))
     depth, tile, ms = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_float(0)
@@ -30,10 +31,19 @@ def autotune(Fmin: float, Fmax: float, nchan: int, cols: int, imaxDt: int) -> tu
     return depth.value, tile.value, ms.value
 
 
+def autotune_desc(desc: "_capi.FdmtDesc") -> tuple["_capi.FdmtDesc", float]:
+    """The tuned description (fuse_depth, head_tile, seg_levels, seg_rows
+    filled in) of `desc` on the current device, and its time in ms."""
+    out = _capi.FdmtDesc()
+    ms = ctypes.c_float(0)
+    _capi.call("bfs_fdmt_autotune_desc", ctypes.byref(desc), ctypes.byref(out), ctypes.byref(ms))
+    return out, ms.value
+
+
 class CFdmtGpu:
     def __init__(self, Fmin: float, Fmax: float, nchan: int, cols: int, imaxDt: int,
                  fuse_depth: int = -1, external_ws: bool = False, head_tile: int = 0,
-                 precision: int = 0):
+                 precision: int = 0, seg_levels: int = 0, seg_rows: int = 0):
         self.m_Fmin = float(Fmin)
         self.m_Fmax = float(Fmax)
         self.m_nchan = int(nchan)
@@ -44,7 +54,8 @@ class CFdmtGpu:
                               ncols=self.m_cols, max_dt=self.m_imaxDt, plan_kind=0,
                               precision=int(precision), fuse_depth=int(fuse_depth),
                               flags=_capi.BFS_FDMT_EXTERNAL_WS if external_ws else 0,
-                              head_tile=int(head_tile))
+                              head_tile=int(head_tile), seg_levels=int(seg_levels),
+                              seg_rows=int(seg_rows))
         self._plan = ctypes.c_void_p()
         _capi.call("bfs_fdmt_plan_create", ctypes.byref(desc), ctypes.byref(self._plan))
         info = _capi.FdmtInfo()

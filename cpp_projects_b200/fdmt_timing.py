@@ -2,6 +2,7 @@
 
     python -m cpp_projects_b200.fdmt_timing --nchan 1024 --ncols 65536 \
         [--max-dt 1024] [--fmin 1200 --fmax 1600] [--fuse -2] [--tile 0] \
+        [--seg-levels 0] [--seg-rows 0] \
         [--precision f32|f16|bf16] [--adjoint] [--reps 10] [--warmup 3]
 
 Prints one JSON line: the plan's fused depth, milliseconds per call, the
@@ -38,6 +39,8 @@ def main(argv=None) -> int:
     ap.add_argument("--fmax", type=float, default=1600.0)
     ap.add_argument("--fuse", type=int, default=-2, help="-2 autotune, -1 default head, 0 none, k")
     ap.add_argument("--tile", type=int, default=0)
+    ap.add_argument("--seg-levels", type=int, default=0, help="merge levels per fused pass (1: none)")
+    ap.add_argument("--seg-rows", type=int, default=0, help="output rows per fused tile (0: auto)")
     ap.add_argument("--precision", choices=sorted(PRECISIONS), default="f32")
     ap.add_argument("--adjoint", action="store_true")
     ap.add_argument("--reps", type=int, default=10)
@@ -46,7 +49,7 @@ def main(argv=None) -> int:
     max_dt = a.max_dt or a.nchan
     dev = torch.device("cuda", 0)
     f = CFdmtGpu(a.fmin, a.fmax, a.nchan, a.ncols, max_dt, fuse_depth=a.fuse, head_tile=a.tile,
-                 precision=PRECISIONS[a.precision])
+                 precision=PRECISIONS[a.precision], seg_levels=a.seg_levels, seg_rows=a.seg_rows)
     g = torch.Generator(device=dev).manual_seed(1)
     if a.adjoint:
         src = torch.randn((max_dt, a.ncols), device=dev, generator=g)
@@ -67,7 +70,9 @@ def main(argv=None) -> int:
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / a.reps
     print(json.dumps({"nchan": a.nchan, "ncols": a.ncols, "max_dt": max_dt, "precision": a.precision,
-                      "adjoint": a.adjoint, "fuse_depth": f.info.fuse_depth, "ms": ms,
+                      "adjoint": a.adjoint, "fuse_depth": f.info.fuse_depth,
+                      "hbm_passes": f.info.hbm_passes, "seg_levels": f.info.seg_levels, "ms": ms,
+                      "sched_bytes": f.info.sched_bytes,
                       "alg_bytes": f.alg_bytes, "alg_gbs": f.alg_bytes / (ms / 1e3) / 1e9,
                       "reference_gflop_per_s": (REFERENCE_GFLOP[a.nchan] / (ms / 1e3)
                                                 if a.nchan in REFERENCE_GFLOP else None)}))

@@ -22,10 +22,10 @@ from .fdmt import CFdmtGpu
 
 
 def fdmt_launches(plan: CFdmtGpu) -> int:
-    """Kernels one FDMT launches: init + one per level, or the fused head
-    (init + the first ``depth`` levels) + one per remaining level."""
-    depth = plan.info.fuse_depth
-    return 1 + plan.m_iNumIter - depth
+    """Kernels one FDMT launches: level 0 (or the fused head over the first
+    ``depth`` levels), then one per merge pass (a plain level or a fused
+    segment of several levels)."""
+    return 1 + plan.info.hbm_passes
 
 
 @dataclass
@@ -157,12 +157,12 @@ class BatchedSearch:
             p = ctypes.c_void_p()
             dd = self._capi.FdmtDesc.from_buffer_copy(d)
             if dd.fuse_depth == self._capi.BFS_FUSE_AUTOTUNE:  # the batch's plans: cached choice
-                from .fdmt import autotune
-                dd.fuse_depth, dd.head_tile, _ = autotune(dd.fmin, dd.fmax, dd.nchan, dd.ncols, dd.max_dt)
+                from .fdmt import autotune_desc
+                dd, _ = autotune_desc(dd)
             self._capi.call("bfs_fdmt_plan_create_host", ctypes.byref(dd), ctypes.byref(p))
             self._capi.call("bfs_fdmt_plan_info", p, ctypes.byref(info))
             self._capi.lib().bfs_fdmt_plan_destroy(p)
-            k += 1 + info.niter - info.fuse_depth + 2
+            k += 1 + info.hbm_passes + 2
         return k + ((2 + 12 + 4) if n_candidates else 0)
 
     def run(self, inputs: list[torch.Tensor], stream=None) -> list[BeamResult]:

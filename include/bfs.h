@@ -86,7 +86,11 @@ typedef struct bfs_fdmt_desc {
     int dt_min;        /* BFS_PLAN_PRAVIR: smallest delay of the grid (0)              */
     int dt_step;       /* BFS_PLAN_PRAVIR: grid step (0 is taken as 1)                 */
     float tsamp;       /* BFS_PLAN_PRAVIR: sample time (s), for the DM grid only       */
-    int reserved[3];
+    int seg_levels;    /* merge levels fused per HBM pass after the head (FP32 plans):
+                          0: 3; 1: one pass per level; 2..6                              */
+    int seg_rows;      /* output rows per tile of a fused pass (0: the most that keep
+                          two CTAs per SM, of 64 / 32 / 16)                              */
+    int reserved[1];
 } bfs_fdmt_desc;
 
 typedef struct bfs_fdmt_plan bfs_fdmt_plan;
@@ -99,14 +103,23 @@ typedef struct bfs_fdmt_info {
     size_t workspace_bytes; /* device scratch the plan owns                   */
     double alg_bytes;       /* level-by-level algorithmic bytes of one call   */
     int out_rows;           /* output rows (max_dt; Pravir: the grid length)  */
+    int hbm_passes;         /* merge passes after the head (each reads and writes HBM) */
+    int seg_levels;         /* most merge levels fused into one of those passes */
+    double sched_bytes;     /* DRAM bytes this schedule cannot avoid: the input read,
+                               every plane that reaches HBM written and read once,
+                               the output written                              */
 } bfs_fdmt_info;
 
 bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc, bfs_fdmt_plan** plan);
 /* The autotuner alone (no reference counterpart): times fusion depths
- * {0,2,3,4,5} x head tiles {256,512} on this shape with zero input (the
+ * {0,2,3,4,5} x head tiles {256,512} x merge segments of 1..4 levels on this shape with zero input (the
  * kernels' cost does not depend on the values) and returns the fastest;
  * results are cached per (nchan, max_dt, band, ncols rounded up to 2^k). */
 bfs_status bfs_fdmt_autotune(const bfs_fdmt_desc* desc, int* depth, int* head_tile, float* ms);
+/* The same measurement over fusion depth, head tile and fused merge-segment
+ * length (1..4 levels per HBM pass, FP32): *tuned = *desc with fuse_depth,
+ * head_tile, seg_levels and seg_rows set to the fastest (cached per shape). */
+bfs_status bfs_fdmt_autotune_desc(const bfs_fdmt_desc* desc, bfs_fdmt_desc* tuned, float* ms);
 /* Same plan without device resources (introspection only; execute fails). */
 bfs_status bfs_fdmt_plan_create_host(const bfs_fdmt_desc* desc, bfs_fdmt_plan** plan);
 bfs_status bfs_fdmt_plan_destroy(bfs_fdmt_plan* plan);
@@ -129,6 +142,22 @@ bfs_status bfs_fdmt_plan_tables(const bfs_fdmt_plan* plan, int level, int* a_row
  * (optional) receives 4 ints per row {tail, head, shift, 0} local to a group. */
 bfs_status bfs_fdmt_plan_head(const bfs_fdmt_plan* plan, int* params, int* groups, int group_cap,
                               int* tab, int tab_cap);
+/* Merge passes after the fused head (no reference counterpart; introspection
+ * for tests and tuning): *npasses receives their number; params (optional,
+ * cap ints) 12 ints per pass {first input level l0, output level l1, output
+ * rows per tile, samples per tile, 32-column chunks per shared row, shared
+ * row pitch, shared rows of buffer X, of buffer Y, most entries of a tile,
+ * largest head-row threshold, tiles, entries}.  A pass with 0 tiles is one
+ * plain merge level; the others fuse levels l0+1..l1 in shared memory. */
+bfs_status bfs_fdmt_plan_passes(const bfs_fdmt_plan* plan, int* npasses, int* params, int cap);
+/* One fused pass's tiles (8 ints each: first entry, input rows, then the
+ * rows of levels l0+1.. up to 6 levels) and entries (4 ints each: input rows
+ * {plane row, window lead, 0, offset in buffer X}; level rows {tail offset,
+ * head offset minus the shift (both in the buffer of the level below), shift
+ * + lead, offset in this level's buffer or the output plane row}).  Each
+ * shared buffer holds its rows, a row of -0.0 and a guard row. */
+bfs_status bfs_fdmt_plan_segment(const bfs_fdmt_plan* plan, int pass, int* tiles, int tiles_cap,
+                                 int* ent, int ent_cap);
 /* d_in: nchan*ncols floats (ignored when b_ones != 0: an all-ones image is used,
  * the reference's normalisation mode), d_out: max_dt*ncols floats. */
 bfs_status bfs_fdmt_execute(bfs_fdmt_plan* plan, const float* d_in, float* d_out, int b_ones,

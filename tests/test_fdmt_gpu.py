@@ -90,10 +90,24 @@ def test_fdmt_bit_exact_on_special_values(cuda, shape, fuse):
 
 
 def test_autotune_returns_a_valid_choice(cuda):
-    from cpp_projects_b200.fdmt import autotune
+    from cpp_projects_b200 import _capi
+    from cpp_projects_b200.fdmt import autotune, autotune_desc
     depth, tile, ms = autotune(1200.0, 1600.0, 1024, 65536, 1024)
-    assert depth in (0, 2, 3, 4, 5) and tile in (256, 512) and ms > 0
+    assert depth in (0, 2, 3, 4, 5) and ms > 0
+    assert tile in ((0,) if depth == 0 else (256, 512))
     assert autotune(1200.0, 1600.0, 1024, 65536, 1024)[:2] == (depth, tile)  # cached
+    d = _capi.FdmtDesc(fmin=1200.0, fmax=1600.0, nchan=1024, ncols=65536, max_dt=1024)
+    t, ms2 = autotune_desc(d)
+    assert (t.fuse_depth, t.head_tile) == (depth, tile) and ms2 == ms
+    assert t.seg_levels in (1, 2, 3, 4) and t.seg_rows in ((0,) if t.seg_levels == 1 else (16, 32))
+    # the tuned plan is the one the autotuning plan request builds, and bit-exact
+    x = np.random.default_rng(7).standard_normal((1024, 4096)).astype(np.float32)
+    f = CFdmtGpu(1200.0, 1600.0, 1024, 4096, 1024, fuse_depth=t.fuse_depth, head_tile=t.head_tile,
+                 seg_levels=t.seg_levels, seg_rows=t.seg_rows)
+    d_out = torch.empty((1024, 4096), device=cuda)
+    f.process_image(torch.from_numpy(x).to(cuda), d_out, False)
+    want = pyoracle.fdmt_f32(1200.0, 1600.0, x, 1024, 4096, 1024)
+    assert np.array_equal(_bits(d_out.cpu().numpy()), _bits(want))
 
 
 @pytest.mark.parametrize("fuse", [0, -1])
