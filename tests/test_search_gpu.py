@@ -18,6 +18,17 @@ pytestmark = pytest.mark.gpu
 GOLDEN = json.loads((Path(__file__).parent / "golden" / "cluster_golden.json").read_text())
 
 
+def normalise_with(y, stats):
+    """(x - mean_r) / std_r in float32, one rounding per operation (the
+    oracle's and the product's arithmetic), with given row statistics."""
+    r = y.shape[0]
+    m, sd = stats[:r, None], stats[r:, None]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        z = ((y - m).astype(np.float32) / sd).astype(np.float32)
+    z[np.broadcast_to(sd == 0, z.shape)] = 0.0
+    return z
+
+
 def golden_plane():
     p = GOLDEN["plane"]
     a = np.full((p["rows"], p["cols"]), p["base"], np.float32)
@@ -91,9 +102,16 @@ def test_boxcar_with_fused_row_normalisation(cuda):
     assert np.abs(stg[32:].view(np.int32) - s.view(np.int32)).max() <= 1
     assert np.abs(zg.cpu().numpy().view(np.int32) - z.view(np.int32)).max() <= 1
     got, n = search.boxcar_gather(d, 3.0, 0, 5, stats=st)
-    want = pyoracle.boxcar(z, 3.0, 0, 5)
-    if np.array_equal(stg[:32], m) and np.array_equal(stg[32:], s):
-        assert same_cands(search.cands_to_numpy(got), want)
+    # the boxcar's fused normalisation against the oracle's, both given the
+    # GPU's statistics: identical lists (the statistics themselves are within
+    # 1 ulp of the oracle's, asserted above)
+    want = pyoracle.boxcar(normalise_with(x, stg), 3.0, 0, 5)
+    assert n == len(want) and same_cands(search.cands_to_numpy(got), want)
+    # and given the oracle's own statistics, the oracle's own normalised plane
+    st_o = torch.from_numpy(np.concatenate([m, s])).to(cuda)
+    got_o, n_o = search.boxcar_gather(d, 3.0, 0, 5, stats=st_o)
+    want_o = pyoracle.boxcar(z, 3.0, 0, 5)
+    assert n_o == len(want_o) and same_cands(search.cands_to_numpy(got_o), want_o)
 
 
 def test_boxcar_fast_snr_mode_is_within_two_ulp(cuda):
@@ -192,7 +210,21 @@ def test_config0_search_chain_finds_the_pulse(cuda):
     best = cl.delegate_records()
     top = best[np.argmax(best["msnr"])]
     assert abs(int(top["mdt"]) - 256) <= 8 and 10240 <= int(top["mt"]) <= 10270
-    # parity of the whole chain with the oracle on the same plane
-    z, _, _ = pyoracle.norm_rows(dm.cpu().numpy())
-    want = pyoracle.boxcar(z, 7.0, 0, 5)
-    assert n == len(want)
+    # parity of the whole chain with the oracle on the same plane: the FDMT
+    # bit for bit, the row statistics within 1 ulp, then (given the same
+    # statistics) the full candidate list, the groups and the delegates
+    y = dm.cpu().numpy()
+    want_y = pyoracle.fdmt_f32(beam.fmin, beam.fmax, synth.filterbank(beam), beam.nchan, beam.nsamp,
+                               beam.max_dt)
+    assert np.array_equal(y.view(np.uint32), want_y.view(np.uint32))
+    stg = st.cpu().numpy()
+    _, m, sd = pyoracle.norm_rows(y)
+    assert np.abs(stg[:512].view(np.int32) - m.view(np.int32)).max() <= 1
+    assert np.abs(stg[512:].view(np.int32) - sd.view(np.int32)).max() <= 1
+    want = pyoracle.boxcar(normalise_with(y, stg), 7.0, 0, 5)
+    assert n == len(want) and same_cands(search.cands_to_numpy(cands), want)
+    perm, offs, dl = pyoracle.cluster(want, (16, 8, 1 << 30))
+    assert cl.ngroups == len(offs) - 1
+    np.testing.assert_array_equal(cl.perm.cpu().numpy(), perm)
+    np.testing.assert_array_equal(cl.offsets.cpu().numpy(), offs)
+    np.testing.assert_array_equal(cl.delegates.cpu().numpy(), dl)
