@@ -3,7 +3,11 @@
 
     python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
                     [--workload config2|config0|config1|config3|config4|config4fwd]
-                    [--form both|batched] [--no-e2e] [--no-cpu-baseline]
+                    [--form both|batched] [--no-e2e] [--no-cpu-baseline] [--dry-run]
+
+--gpus N without torchrun relaunches this script as N ranks through
+torch.distributed.run (127.0.0.1); under torchrun the ranks come from the
+environment.
 
 Workload (default ``config2``): the batched multi-beam search — 48 beams of
 uneven shapes (nchan from {256, 512, 1024, 4096}, 2^14..2^17 samples, max
@@ -71,9 +75,9 @@ def parse_args(argv=None):
                                            "config1"], default="config2")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-ref-gpu", action="store_true",
-                    help="no effect: the reference GPU path is timed by the tests now; accepted so "
-                         "the commands recorded with the profiles run unchanged (they skipped it)")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="rank coordination only (launch, barrier, max over ranks, per-rank beam "
+                         "sets) with no GPU work: prints the line's shape with value null")
     ap.add_argument("--form", choices=["both", "batched"], default="both",
                     help="batched: time only the batched form (profiling runs; no plain-form "
                          "numbers, no FDMT roofline)")
@@ -181,7 +185,7 @@ def cpu_reference_leg(beams, max_seconds: float = 15.0, min_steps: int = 1):
         else:
             dm = pyoracle.fdmt_f32(b.fmin, b.fmax, x, b.nchan, b.nsamp, b.max_dt)
         z, _, _ = pyoracle.norm_rows(dm)
-        c = pyoracle.boxcar_mt(z, SEARCH["thr"], SEARCH["widths_mode"], SEARCH["param"])
+        c = pyoracle.boxcar_mt(z, SEARCH["thr"], SEARCH["widths_mode"], SEARCH["param"], cap=1 << 27)
         if len(c):
             pyoracle.cluster(c, SEARCH["metrics"])
         secs += time.perf_counter() - t0
@@ -216,7 +220,7 @@ def cpu_pravir_leg(beams, max_seconds: float = 6.0):
         if dm is None:
             return None
         z, _, _ = pyoracle.norm_rows(dm)
-        c = pyoracle.boxcar_mt(z, SEARCH["thr"], SEARCH["widths_mode"], SEARCH["param"])
+        c = pyoracle.boxcar_mt(z, SEARCH["thr"], SEARCH["widths_mode"], SEARCH["param"], cap=1 << 27)
         if len(c):
             pyoracle.cluster(c, SEARCH["metrics"])
         secs += time.perf_counter() - t0
@@ -231,14 +235,74 @@ def cpu_pravir_leg(beams, max_seconds: float = 6.0):
             "seconds": secs}
 
 
+def stratified(beams):
+    """The workload's beams ordered for bounded samples: the smallest beam of
+    every channel count, then the second smallest of every count, ... (every
+    channel class appears in the first few beams of a sample)."""
+    by = {}
+    for b in sorted(beams, key=lambda b: b.nchan * b.nsamp):
+        by.setdefault(b.nchan, []).append(b)
+    out = []
+    for k in range(max(len(v) for v in by.values())):
+        out += [v[k] for n, v in sorted(by.items()) if k < len(v)]
+    return out
+
+
+def reference_gpu_leg(sample, warmup: int, nbeams: int = 4):
+    """The reference's own GPU search path, built from its sources into
+    oracle/_ref/libref_gpu.so: CFdmtGpu::process_image, then (the reference has
+    no per-row normalisation: this build's, as a stand-in) its
+    gather_candidates_in_dynamicalArray and complete_clusterization with its
+    log, on one beam of each channel count (the first `nbeams` of the
+    stratified sample), wall clock with device synchronisation.  None when the
+    library or a GPU is missing."""
+    try:
+        import torch
+    except ImportError:
+        return None
+    from oracle import pyoracle
+    if not torch.cuda.is_available() or pyoracle.ref_gpu_lib() is None:
+        return None
+    from cpp_projects_b200 import search
+    from cpp_projects_b200.pipeline import device_filterbank
+    lib = pyoracle.ref_gpu_lib()
+    dev = torch.device("cuda", 0)
+    beams = sample[:nbeams]
+    thr = torch.tensor([SEARCH["thr"]], device=dev)
+    metrics = torch.tensor(list(SEARCH["metrics"]), dtype=torch.int32, device=dev)
+    log = str(Path(tempfile.gettempdir()) / "bench_ref_gpu.log").encode()
+    secs, units = 0.0, 0
+    for rep in range(max(1, warmup) + 1):   # the first pass warms up
+        for b in beams:
+            x = device_filterbank(b.nchan, b.nsamp, b.fmin, b.fmax, b.seed, b.pulses, dev)
+            f = pyoracle.RefFdmtGpu(b.fmin, b.fmax, b.nchan, b.nsamp, b.max_dt)
+            out = torch.empty((b.max_dt, b.nsamp), device=dev)
+            z = torch.empty_like(out)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            if f.process_image(x.data_ptr(), out.data_ptr()) != 0:
+                return None
+            search.norm_rows(out, out=z)
+            lib.ref_search_dynamic(z.data_ptr(), b.max_dt, b.nsamp, thr.data_ptr(), SEARCH["param"],
+                                   metrics.data_ptr(), log, 1e-3, 0.0)
+            torch.cuda.synchronize()
+            if rep > 0:
+                secs += time.perf_counter() - t0
+                units += b.nchan * b.nsamp
+            del f, out, z, x
+    return {"value": units / secs, "unit": UNIT,
+            "sample": f"{len(beams)} beam(s) [{', '.join(f'{b.nchan}x{b.nsamp}' for b in beams)}]: the "
+                      "reference's CFdmtGpu + gather_candidates_in_dynamicalArray + complete_clusterization "
+                      "(built from its sources for sm_100a), per-row normalisation by this build",
+            "seconds": secs}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     beams = beams_for(args.workload, 0)
-    # bounded sample: the smallest beams of the workload, about 10-20 s per step
-    order = sorted(range(len(beams)), key=lambda i: beams[i].nchan * beams[i].nsamp)
-    sample = [beams[i] for i in order]
+    sample = stratified(beams)
     for _ in range(args.warmup):
         cpu_reference_leg(sample[:1], max_seconds=0.0)
     done, secs_total, texts, kind, threads = 0.0, 0.0, "", "port", 1
@@ -248,6 +312,7 @@ def run_reference(args):
         secs_total += secs
     value = done / secs_total
     pravir = cpu_pravir_leg(sample, max_seconds=5.0)
+    ref_gpu = reference_gpu_leg(sample, args.warmup)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs_total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -262,7 +327,7 @@ def run_reference(args):
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
                              "sample": texts},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "cpu_baseline_variant": pravir}
+            "cpu_baseline_variant": pravir, "reference_gpu": ref_gpu}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -353,13 +418,20 @@ def run_ours(args):
 
     peak, peak_kind = measured_peaks()
     fdmt_bytes = pipe.fdmt_alg_bytes()
-    achieved = fdmt_bytes / (fdmt_ms / 1e3) / 1e9 if plain else None
+    sched = pipe.fdmt_sched_bytes()
+    sched_bytes = sum(sched)
+    # achieved: the bytes this schedule must move (input, each plane that
+    # reaches HBM written and read once, output) over the FDMT's event time;
+    # traffic: those bytes scaled by the DRAM / schedule-byte ratio measured
+    # with ncu on one FDMT of each channel count (profiles/traffic.json)
+    achieved = sched_bytes / (fdmt_ms / 1e3) / 1e9 if plain else None
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
-        t = json.loads(tf.read_text()).get(args.workload)
-        if t:
-            traffic = t.get("fdmt_dram_bytes_per_step")
+        ratio = json.loads(tf.read_text()).get("fdmt_dram_over_sched", {})
+        if all(str(b.nchan) in ratio for b in beams):
+            traffic = sum(sb * ratio[str(b.nchan)] for sb, b in zip(sched, beams))
+    compulsory = sum(4.0 * b.nsamp * (b.nchan + 3 * b.max_dt) for b in beams)
     pipe_bytes = fdmt_bytes + pipe.search_alg_bytes()
 
     # ---- end to end: pinned host inputs, copied every step ------------------
@@ -398,7 +470,7 @@ def run_ours(args):
     # ---- CPU baseline (rank 0, N=1 only) -------------------------------------
     cpu = cpu_variant = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        small = sorted(beams, key=lambda b: b.nchan * b.nsamp)
+        small = stratified(beams)
         rate, secs, sample, kind, threads = cpu_reference_leg(small, max_seconds=12.0)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample,
                "seconds": secs}
@@ -419,10 +491,19 @@ def run_ours(args):
                        "form": "batched: one CUDA graph for every beam's FDMT + statistics + "
                                "boxcar, one sort and one clustering for all beams",
                        "parallelism": f"{world} independent rank(s), beams sharded, no collective"},
-            "roofline": {"bound": "hbm", "kernel": "FDMT (bfs_fdmt_execute: init + level kernels)",
+            "roofline": {"bound": "hbm",
+                         "kernel": "FDMT (fused head or level 0, then fused merge segments)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if plain else None, "peak_source": peak_kind,
-                         "traffic": traffic, "alg_bytes_per_step": fdmt_bytes,
+                         "traffic": traffic,
+                         "bytes": "achieved = schedule bytes per step / FDMT time; traffic = DRAM bytes "
+                                  "per step (ncu ratio per channel count x schedule bytes)",
+                         "sched_bytes_per_step": sched_bytes,
+                         "level_by_level_bytes_per_step": fdmt_bytes,
+                         "level_by_level_gbs": fdmt_bytes / (fdmt_ms / 1e3) / 1e9 if plain else None,
+                         "compulsory_io_bytes_per_step": compulsory,
+                         "compulsory_io": "input read + FDMT output written + row statistics and "
+                                          "boxcar reads of the output",
                          "fdmt_ms_per_step": fdmt_ms,
                          "timed_in": "plain per-beam form (events around each beam's FDMT; "
                                      "same autotuned plans as the batched form)"},
@@ -825,8 +906,62 @@ def run_config1(args):
     return 0
 
 
+def launch_ranks(args, argv) -> int:
+    """--gpus N without a launcher: start N ranks of this script (one process
+    per GPU) through torch.distributed.run on 127.0.0.1, with a bound on the
+    whole job; they print the line (rank 0)."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(ROOT / "bench.py")] + list(argv)
+    env = dict(os.environ, OMP_NUM_THREADS=os.environ.get("OMP_NUM_THREADS", "1"))
+    try:
+        return subprocess.call(cmd, env=env, timeout=3600)
+    except subprocess.TimeoutExpired:
+        print(json.dumps({"metric": METRIC, "error": f"{args.gpus}-rank job exceeded 3600 s"}), flush=True)
+        return 1
+
+
+def run_dry(args) -> int:
+    """The multi-rank plumbing without GPU work: every rank builds its beam
+    set, meets the others at the barrier and takes the maximum over ranks of
+    a stand-in step time; rank 0 prints the line with each rank's beam seeds."""
+    import torch
+    from cpp_projects_b200.ranks import Ranks
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    gpu = torch.cuda.is_available()
+    ranks = Ranks("nccl" if gpu else "gloo", torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+                  if gpu else None, timeout_s=60)
+    beams = beams_for(args.workload, rank)
+    ranks.barrier()
+    slowest = ranks.max(float(rank + 1))
+    seeds = [b.seed for b in beams]
+    all_seeds = [seeds]
+    if world > 1:
+        import torch.distributed as dist
+        all_seeds = [None] * world
+        dist.all_gather_object(all_seeds, seeds)
+    ranks.barrier()
+    ranks.close()
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": None, "unit": UNIT, "n_gpus": world, "steps": 0,
+                          "warmup": 0, "dry_run": True, "scaling": "weak",
+                          "config": {"workload": args.workload, "beams": len(beams),
+                                     "parallelism": f"{world} independent rank(s), beams sharded, no collective"},
+                          "slowest_rank_stand_in": slowest, "rank_seeds": all_seeds}), flush=True)
+    return 0
+
+
 def main(argv=None):
+    argv = sys.argv[1:] if argv is None else argv
     args = parse_args(argv)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return launch_ranks(args, argv)
+    if args.dry_run:
+        return run_dry(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "config1":

@@ -127,6 +127,20 @@ class CFdmtGpu:
                    ctypes.c_size_t(workspace.numel() * workspace.element_size()), stream_handle(stream))
 
     # --- plan introspection ------------------------------------------------
+    def passes(self) -> list[list[int]]:
+        """[l0, l1] of every merge pass after the head: a plain level (l1 =
+        l0 + 1) or a fused segment of levels l0+1..l1."""
+        n = ctypes.c_int(0)
+        _capi.call("bfs_fdmt_plan_passes", self._plan, ctypes.byref(n), None, 0)
+        p = np.zeros(max(1, n.value) * 12, np.int32)
+        _capi.call("bfs_fdmt_plan_passes", self._plan, ctypes.byref(n), p.ctypes.data_as(ctypes.c_void_p), p.size)
+        return [[int(p[12 * i]), int(p[12 * i + 1])] for i in range(n.value)]
+
+    @property
+    def sched_bytes(self) -> float:
+        """DRAM bytes of one call that this plan's schedule cannot avoid."""
+        return float(self.info.sched_bytes)
+
     def rows_per_level(self) -> np.ndarray:
         rows = np.zeros(self.m_iNumIter + 1, np.int32)
         _capi.call("bfs_fdmt_plan_rows", self._plan, rows.ctypes.data_as(ctypes.c_void_p),

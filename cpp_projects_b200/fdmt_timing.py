@@ -3,10 +3,14 @@
     python -m cpp_projects_b200.fdmt_timing --nchan 1024 --ncols 65536 \
         [--max-dt 1024] [--fmin 1200 --fmax 1600] [--fuse -2] [--tile 0] \
         [--seg-levels 0] [--seg-rows 0] \
-        [--precision f32|f16|bf16] [--adjoint] [--reps 10] [--warmup 3]
+        [--precision f32|f16|bf16] [--adjoint] [--reps 10] [--warmup 3] [--profile-one]
+        [--print-tuned]
 
-Prints one JSON line: the plan's fused depth, milliseconds per call, the
-level-by-level algorithmic bytes of one call and the resulting GB/s.  Used
+Prints one JSON line: the plan's fused depth and merge passes ([first
+level, last level] of each pass after the head), milliseconds per call, the
+level-by-level algorithmic bytes of one call and the resulting GB/s, and the
+bytes this schedule cannot avoid (every plane that reaches HBM written and
+read once).  Used
 for the autotuner's choices, for the reduced-precision and adjoint timings,
 and as the command under ncu for the per-kernel captures.
 
@@ -45,8 +49,21 @@ def main(argv=None) -> int:
     ap.add_argument("--adjoint", action="store_true")
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--profile-one", action="store_true",
+                    help="after the timing, one more call between cudaProfilerStart / Stop (for "
+                         "ncu --profile-from-start off: one FDMT's launches, none of the tuning)")
+    ap.add_argument("--print-tuned", action="store_true",
+                    help="autotune this shape and print the chosen schedule as command-line options "
+                         "(--fuse k --tile t --seg-levels s --seg-rows r), then exit")
     a = ap.parse_args(argv)
     max_dt = a.max_dt or a.nchan
+    if a.print_tuned:
+        from . import _capi
+        from .fdmt import autotune_desc
+        t, _ = autotune_desc(_capi.FdmtDesc(fmin=a.fmin, fmax=a.fmax, nchan=a.nchan, ncols=a.ncols,
+                                            max_dt=max_dt, precision=PRECISIONS[a.precision]))
+        print(f"--fuse {t.fuse_depth} --tile {t.head_tile} --seg-levels {t.seg_levels} --seg-rows {t.seg_rows}")
+        return 0
     dev = torch.device("cuda", 0)
     f = CFdmtGpu(a.fmin, a.fmax, a.nchan, a.ncols, max_dt, fuse_depth=a.fuse, head_tile=a.tile,
                  precision=PRECISIONS[a.precision], seg_levels=a.seg_levels, seg_rows=a.seg_rows)
@@ -69,7 +86,12 @@ def main(argv=None) -> int:
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / a.reps
-    print(json.dumps({"nchan": a.nchan, "ncols": a.ncols, "max_dt": max_dt, "precision": a.precision,
+    if a.profile_one:
+        torch.cuda.profiler.start()
+        run()
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+    print(json.dumps({"passes": f.passes(),"nchan": a.nchan, "ncols": a.ncols, "max_dt": max_dt, "precision": a.precision,
                       "adjoint": a.adjoint, "fuse_depth": f.info.fuse_depth,
                       "hbm_passes": f.info.hbm_passes, "seg_levels": f.info.seg_levels, "ms": ms,
                       "sched_bytes": f.info.sched_bytes,

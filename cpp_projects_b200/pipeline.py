@@ -68,7 +68,13 @@ class SearchPipeline:
         return sum(s.nchan * s.nsamp for s in self.shapes)
 
     def fdmt_alg_bytes(self) -> float:
+        """Level-by-level bytes of the reference's algorithm, summed over beams."""
         return sum(p.alg_bytes for p in self.plans)
+
+    def fdmt_sched_bytes(self) -> list[float]:
+        """Per beam: the DRAM bytes its FDMT schedule cannot avoid (input read,
+        every plane that reaches HBM written and read once, output written)."""
+        return [p.sched_bytes for p in self.plans]
 
     def search_alg_bytes(self) -> float:
         """Row-statistics read + boxcar read of each DM-time plane."""

@@ -9,6 +9,7 @@ and bench.py's CPU-baseline leg may use this module, and only as the checker.
 from __future__ import annotations
 
 import ctypes
+import os
 import subprocess
 from pathlib import Path
 
@@ -23,6 +24,16 @@ CAND_DTYPE = np.dtype([("mt", "<i4"), ("mdt", "<i4"), ("mwidth", "<i4"), ("msnr"
 _lib = None
 _ref = None
 _ref_gpu = None
+
+
+def reference_dir() -> Path:
+    """The reference checkout the oracle's recipe builds from:
+    BFS_REFERENCE_DIR, else oracle/Makefile's default (it may be absent)."""
+    env = os.environ.get("BFS_REFERENCE_DIR")
+    if env:
+        return Path(env)
+    r = subprocess.run(["make", "-s", "-C", str(HERE), "print-ref"], capture_output=True, text=True)
+    return Path(r.stdout.strip()) if r.returncode == 0 and r.stdout.strip() else Path("/nonexistent")
 
 
 def build() -> None:

@@ -54,8 +54,9 @@ def read_csv(path: Path):
     return rows
 
 
-def main(ref_root: str = "/root/reference") -> None:
-    ref = Path(ref_root)
+def main(ref_root: str | None = None) -> None:
+    from oracle import pyoracle
+    ref = Path(ref_root) if ref_root else pyoracle.reference_dir()
     d = ref / "clusterization_forpravir"
     golden = {
         "source": "clusterization_forpravir/Candidates{1,2}.csv",
@@ -86,11 +87,12 @@ FILE512 = dict(fmin=1200.0, fmax=1600.0, nchan=512, ncols=512, max_dt=512, pravi
 FILE512_ROWS = [0, 1, 255, 511]
 
 
-def make_file512(ref_root: str = "/root/reference") -> None:
+def make_file512(ref_root: str | None = None) -> None:
     import hashlib
 
     from oracle import pyoracle
-    x = np.fromfile(Path(ref_root) / "fdmt_class_v0" / "file512.bin", np.float32)
+    ref = Path(ref_root) if ref_root else pyoracle.reference_dir()
+    x = np.fromfile(ref / "fdmt_class_v0" / "file512.bin", np.float32)
     q = x.astype(np.int8)
     if not np.array_equal(q.astype(np.float32), x):
         raise SystemExit("file512.bin is not int8-valued")

@@ -41,7 +41,7 @@ def test_gpu_reproduces_reference_output(cuda, path):
 
 # --- the reference's own FDMT test input (fdmt_class_v0/file512.bin) ----------
 FILE512 = Path(__file__).parent / "golden" / "file512.npz"
-REF_FILE512 = Path("/root/reference/fdmt_class_v0/file512.bin")
+REF_FILE512 = pyoracle.reference_dir() / "fdmt_class_v0" / "file512.bin"
 
 
 def load512():

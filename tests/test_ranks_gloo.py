@@ -63,3 +63,32 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch):
     with contextlib.redirect_stdout(buf):
         rc = bench.run_reference(args)
     assert rc == 0 and buf.getvalue() == ""
+
+
+def test_bench_gpus_2_launches_two_ranks():
+    """bench.py --gpus 2 without a launcher starts two ranks itself
+    (torch.distributed.run on 127.0.0.1; gloo here, no GPU) and prints one
+    line with n_gpus = 2 and one 48-beam set per rank."""
+    import subprocess
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--gpus", "2", "--dry-run"],
+                       capture_output=True, text=True, timeout=300, cwd=str(ROOT))
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["n_gpus"] == 2 and line["dry_run"] and line["slowest_rank_stand_in"] == 2.0
+    s0, s1 = line["rank_seeds"]
+    assert len(s0) == len(s1) == 48 and set(s0).isdisjoint(s1)
+
+
+def test_stratified_sample_covers_every_channel_count_first():
+    sys.path.insert(0, str(ROOT))
+    import bench
+    beams = bench.beams_for("config2", 0)
+    s = bench.stratified(beams)
+    assert sorted(b.seed for b in s) == sorted(b.seed for b in beams)
+    assert [b.nchan for b in s[:4]] == [256, 512, 1024, 4096]
+    # within a channel count, smallest first
+    for n in (256, 512, 1024, 4096):
+        sizes = [b.nsamp for b in s if b.nchan == n]
+        assert sizes == sorted(sizes)
