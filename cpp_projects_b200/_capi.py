@@ -35,7 +35,7 @@ class FdmtDesc(ctypes.Structure):
                 ("precision", ctypes.c_int), ("fuse_depth", ctypes.c_int),
                 ("flags", ctypes.c_int), ("head_tile", ctypes.c_int), ("dt_min", ctypes.c_int),
                 ("dt_step", ctypes.c_int), ("tsamp", ctypes.c_float), ("seg_levels", ctypes.c_int),
-                ("seg_rows", ctypes.c_int), ("reserved", ctypes.c_int * 1)]
+                ("seg_rows", ctypes.c_int), ("seg_threads", ctypes.c_int)]
 
 
 class FdmtInfo(ctypes.Structure):

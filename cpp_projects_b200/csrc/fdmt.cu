@@ -720,6 +720,11 @@ __device__ __forceinline__ void cp_async16(unsigned s, const void* gmem, int src
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes)
                  : "memory");
 }
+// 4-byte form (any 4-byte aligned addresses)
+__device__ __forceinline__ void cp_async4(unsigned s, const void* gmem, int src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes)
+                 : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // One work item: K consecutive 32-column chunks of one row of a level, from
@@ -743,16 +748,87 @@ __device__ __forceinline__ void seg_chunks(float* __restrict__ sm, int rd, int w
         sm[pw + 32 * k] = (FAST || col + 32 * k >= thr) ? __fadd_rn(va[k], vb[k]) : va[k];
 }
 
+// Two rows of a level (fast tiles: every sample at or past every head
+// shift), all 4K shared loads of both rows issued before any store.
+template <int K>
+__device__ __forceinline__ void seg_rows2(float* __restrict__ sm, int rd, int wr, int4 q0, int4 q1, bool two,
+                                          int lane) {
+    const int pa0 = rd + q0.x + lane, pb0 = rd + q0.y + lane, pw0 = wr + q0.w + lane;
+    const int pa1 = rd + q1.x + lane, pb1 = rd + q1.y + lane, pw1 = wr + q1.w + lane;
+    float a0[K], b0[K], a1[K], b1[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        a0[k] = sm[pa0 + 32 * k];
+        b0[k] = sm[pb0 + 32 * k];
+    }
+    if (two) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            a1[k] = sm[pa1 + 32 * k];
+            b1[k] = sm[pb1 + 32 * k];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) sm[pw0 + 32 * k] = __fadd_rn(a0[k], b0[k]);
+    if (two) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) sm[pw1 + 32 * k] = __fadd_rn(a1[k], b1[k]);
+    }
+}
+
+// Level-0 row r of a channel at K chunks: the reference's running mean
+// v_0 = x[t], v_k = (v_{k-1} k + x[t-k]) / (k+1) (k = 1..r), one rounding per
+// operation as in k_fdmt_init4, from the channel's staged samples (pa = the
+// offset of x[t] for this lane's first column); 0 before sample r.
+template <int R, int K, bool FAST>
+__device__ __forceinline__ void seg_level0_chunks(float* __restrict__ sm, int pa, int pw, int col, int thr) {
+    float v[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = sm[pa + 32 * k];
+#pragma unroll
+    for (int r = 1; r <= R; ++r) {
+        float x[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) x[k] = sm[pa + 32 * k - r];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const float m = r == 1 ? v[k] : __fmul_rn(v[k], static_cast<float>(r));
+            v[k] = div_small(__fadd_rn(m, x[k]), r + 1);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) sm[pw + 32 * k] = (FAST || col + 32 * k >= thr) ? v[k] : 0.0f;
+}
+
+// One level-0 row of an input segment (entry {x offset, -, r + lead, dst | r << 20}).
+template <int R0C, int NC, bool FAST>
+__device__ __forceinline__ void seg_level0_row(float* __restrict__ sm, int rd, int wr, int4 q, int lane,
+                                               int t0) {
+    const int r = (q.w >> 20) & 15;
+    const int pa = rd + q.x + lane, pw = wr + (q.w & 0xfffff) + lane;
+    const int thr = q.z - t0;
+    switch (r) {
+        case 0: seg_level0_chunks<0, NC, FAST>(sm, pa, pw, lane, thr); break;
+        case 1: if constexpr (R0C > 1) seg_level0_chunks<1, NC, FAST>(sm, pa, pw, lane, thr); break;
+        case 2: if constexpr (R0C > 2) seg_level0_chunks<2, NC, FAST>(sm, pa, pw, lane, thr); break;
+        case 3: if constexpr (R0C > 3) seg_level0_chunks<3, NC, FAST>(sm, pa, pw, lane, thr); break;
+        default: if constexpr (R0C > 4) seg_level0_chunks<4, NC, FAST>(sm, pa, pw, lane, thr); break;
+    }
+}
+
 struct SegArgs {
     const float* in;
     float* out;
     const SegTile* tiles;
     const int4* ent;
     int ncols, in_pitch, out_pitch, nlev, zx, zy, max_thr, y0, x1, ent_base, max_ent, nrt, total;
+    int vec;   // input rows 16-byte aligned: 16-byte copies, else 4-byte copies
+    int ones;  // the input is all ones (normalisation mode): no loads
 };
 
-template <int NC, int THREADS>
+template <int NC, int THREADS, int R0C>
 __global__ void __launch_bounds__(THREADS, THREADS <= 256 ? 2 : 1) k_fdmt_seg(const SegArgs a) {
+    static_assert(THREADS == 256 || THREADS == 512 || THREADS == 1024, "CTA size");
     constexpr int kOutCPH = kSegTile / 32;  // chunks of an output row
     constexpr int kWarps = THREADS / 32;
     constexpr int kPieces = NC * 8;  // 16-byte pieces per shared row
@@ -769,13 +845,21 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 256 ? 2 : 1) k_fdmt_seg(co
     // each warp reads the entries of four of its rows at once, then issues
     // their pieces (a piece starts on a multiple of 4 samples, so it lies
     // wholly before sample 0 or wholly after it)
-    auto issue = [&](int w, int buf) {
-        const SegTile* tp = a.tiles + w % a.nrt;
-        const int t0 = (w / a.nrt) * kSegTile;
-        const int nin = __ldg(&tp->n[0]);
-        int nent = 0;
-        for (int i = 0; i <= a.nlev; ++i) nent += __ldg(&tp->n[i]);
-        const int4* ge = a.ent + __ldg(&tp->ent);
+    // the tile's record {first entry, row counts}, two 16-byte loads
+    auto tile_rec = [&](int rt, int4& lo, int4& hi) {
+        const int4* t = reinterpret_cast<const int4*>(a.tiles + rt);
+        lo = __ldg(t);
+        hi = __ldg(t + 1);
+    };
+    auto issue = [&](int rt, int tt, int buf) {
+        int4 lo, hi;
+        tile_rec(rt, lo, hi);
+        const int t0 = tt * kSegTile;
+        const int nin = lo.y;
+        // entries: the counts of levels 0..nlev (ent, n0, n1, n2 | n3, n4, n5, n6)
+        const int nent = lo.y + lo.z + lo.w + (a.nlev >= 3 ? hi.x : 0) + (a.nlev >= 4 ? hi.y : 0) +
+                         (a.nlev >= 5 ? hi.z : 0) + (a.nlev >= 6 ? hi.w : 0);
+        const int4* ge = a.ent + lo.x;
         const unsigned se = sbase + 4u * (a.ent_base + 4 * buf * a.max_ent);
         const unsigned x = sbase + 4u * (buf ? a.x1 : 0);
         for (int i = threadIdx.x; i < nent; i += THREADS) cp_async16(se + 16u * i, ge + i, 16);
@@ -792,7 +876,16 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 256 ? 2 : 1) k_fdmt_seg(co
                 const int ts = t0 - q[j].y;  // the row's first sample
                 const float* src = a.in + static_cast<size_t>(q[j].x) * a.in_pitch;
                 const unsigned dst = x + 4u * q[j].w;
-                if (ts >= 0 && ts + 4 * kPieces <= a.ncols) {  // the whole window lies in [0, ncols)
+                if (a.ones) {  // the all-ones image: 1 inside [0, ncols), 0 outside
+                    float* d = sm + (buf ? a.x1 : 0) + q[j].w;
+                    for (int c = lane; c < 32 * NC; c += 32) d[c] = (ts + c >= 0 && ts + c < a.ncols) ? 1.0f : 0.0f;
+                } else if (!a.vec) {  // unaligned rows: 4-byte copies
+                    for (int c = lane; c < 32 * NC; c += 32) {
+                        const int t = ts + c;
+                        const bool in = t >= 0 && t < a.ncols;
+                        cp_async4(dst + 4u * c, in ? src + t : src, in ? 4 : 0);
+                    }
+                } else if (ts >= 0 && ts + 4 * kPieces <= a.ncols) {  // the whole window lies in [0, ncols)
 #pragma unroll
                     for (int pc = lane; pc < kPieces; pc += 32) cp_async16(dst + 16u * pc, src + ts + 4 * pc, 16);
                 } else {
@@ -806,25 +899,51 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 256 ? 2 : 1) k_fdmt_seg(co
         }
     };
 
+    // tile w = (row tile w % nrt, time tile w / nrt), stepped by gridDim.x
+    // without dividing per tile
+    const int gq = static_cast<int>(gridDim.x) / a.nrt, gr = static_cast<int>(gridDim.x) % a.nrt;
+    auto step = [&](int& rt, int& tt) {
+        rt += gr;
+        tt += gq;
+        if (rt >= a.nrt) { rt -= a.nrt; ++tt; }
+    };
     int w = blockIdx.x;
-    if (w < a.total) issue(w, 0);
+    int rt = w % a.nrt, tt = w / a.nrt;  // this CTA's current tile
+    if (w < a.total) issue(rt, tt, 0);
     for (int j = 0; w < a.total; ++j, w += gridDim.x) {
         const int buf = j & 1;
         cp_async_wait_all();
         __syncthreads();  // this tile's rows are in; every warp is done with the previous tile
-        if (w + static_cast<int>(gridDim.x) < a.total) issue(w + gridDim.x, buf ^ 1);
+        int rn = rt, tn = tt;
+        step(rn, tn);
+        if (w + static_cast<int>(gridDim.x) < a.total) issue(rn, tn, buf ^ 1);
 
-        const SegTile* tp = a.tiles + w % a.nrt;
-        const int t0 = (w / a.nrt) * kSegTile;
+        int4 lo, hi;
+        tile_rec(rt, lo, hi);
+        const int nlv[kSegMaxLevels + 1] = {lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+        const int t0 = tt * kSegTile;
+        rt = rn;
+        tt = tn;
         const int xo = buf ? a.x1 : 0;  // this tile's X buffer
-        const int4* e = reinterpret_cast<const int4*>(sm + a.ent_base) + buf * a.max_ent + __ldg(&tp->n[0]);
+        const int4* e = reinterpret_cast<const int4*>(sm + a.ent_base) + buf * a.max_ent + nlv[0];
         const bool fast = t0 >= a.max_thr;  // no sample of this tile precedes its head row's shift
-        for (int lev = 1; lev < a.nlev; ++lev) {
-            const int nl = __ldg(&tp->n[lev]);
+#pragma unroll
+        for (int lev = 1; lev < kSegMaxLevels; ++lev) {
+            if (lev >= a.nlev) break;
+            const int nl = nlv[lev];
             const int rd = (lev & 1) ? xo : a.y0;
             const int wr = (lev & 1) ? a.y0 : xo;
-            if (fast) {
-                for (int r = warp; r < nl; r += kWarps) seg_chunks<NC, true>(sm, rd, wr, e[r], 0, lane, 0);
+            if (R0C > 0 && lev == 1) {  // input segment: level 0 from the staged channels
+                if (fast) {
+                    for (int r = warp; r < nl; r += kWarps) seg_level0_row<R0C, NC, true>(sm, rd, wr, e[r], lane, t0);
+                } else {
+                    for (int r = warp; r < nl; r += kWarps) seg_level0_row<R0C, NC, false>(sm, rd, wr, e[r], lane, t0);
+                }
+            } else if (fast) {
+                for (int r = warp; r < nl; r += 2 * kWarps) {
+                    const int r1 = r + kWarps;
+                    seg_rows2<NC>(sm, rd, wr, e[r], e[r1 < nl ? r1 : r], r1 < nl, lane);
+                }
             } else {
                 for (int r = warp; r < nl; r += kWarps) {
                     const int4 q = e[r];
@@ -835,7 +954,10 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 256 ? 2 : 1) k_fdmt_seg(co
             __syncthreads();
         }
         // level l1: kSegTile samples per row, straight to HBM (q.w is the plane row)
-        const int nl = __ldg(&tp->n[a.nlev]);
+        int nl = nlv[1];
+#pragma unroll
+        for (int i = 2; i <= kSegMaxLevels; ++i)
+            if (i == a.nlev) nl = nlv[i];
         const int rd = (a.nlev & 1) ? xo : a.y0;
         for (int r = warp; r < nl; r += kWarps) {
             const int4 q = e[r];
@@ -857,9 +979,9 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 256 ? 2 : 1) k_fdmt_seg(co
     }
 }
 
-template <int NC, int THREADS>
+template <int NC, int THREADS, int R0C>
 cudaError_t launch_seg_nc(const SegPlan& sp, const SegArgs& args, cudaStream_t s) {
-    auto kern = k_fdmt_seg<NC, THREADS>;
+    auto kern = k_fdmt_seg<NC, THREADS, R0C>;
     // The shared-memory opt-in is one value per kernel and device: it only
     // ever grows (a smaller setting would refuse a later, larger launch).
     // Resident CTAs per SM are cached per (device, size).  Both happen on the
@@ -895,27 +1017,59 @@ cudaError_t launch_seg_nc(const SegPlan& sp, const SegArgs& args, cudaStream_t s
     return cudaGetLastError();
 }
 
+template <int NC, int R0C>
+cudaError_t launch_seg_threads(const SegPlan& sp, const SegArgs& a, cudaStream_t s, int threads) {
+    switch (threads) {
+        case 256: return launch_seg_nc<NC, 256, R0C>(sp, a, s);
+        case 512: return launch_seg_nc<NC, 512, R0C>(sp, a, s);
+        case 1024: return launch_seg_nc<NC, 1024, R0C>(sp, a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int R0C>
+cudaError_t launch_seg_nc_any(const SegPlan& sp, const SegArgs& a, cudaStream_t s, int threads) {
+    switch (sp.nc) {
+        case 9: return launch_seg_threads<9, R0C>(sp, a, s, threads);
+        case 10: return launch_seg_threads<10, R0C>(sp, a, s, threads);
+        case 12: return launch_seg_threads<12, R0C>(sp, a, s, threads);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_seg_r0c(const SegPlan& sp, const SegArgs& a, cudaStream_t s, int threads) {
+    switch (sp.r0c) {
+        case 0: return launch_seg_nc_any<0>(sp, a, s, threads);
+        case 1: return launch_seg_nc_any<1>(sp, a, s, threads);
+        case 2: return launch_seg_nc_any<2>(sp, a, s, threads);
+        case 3: return launch_seg_nc_any<3>(sp, a, s, threads);
+        case 4: return launch_seg_nc_any<4>(sp, a, s, threads);
+        case 5: return launch_seg_nc_any<5>(sp, a, s, threads);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 // Launches one fused segment (sp.nc is one of the instantiated chunk counts;
 // 256 threads when two CTAs fit an SM, else 512).
 cudaError_t launch_seg(const SegPlan& sp, const float* src, float* dst, const SegTile* tiles,
-                       const int4* ent, int T, int in_pitch, int out_pitch, cudaStream_t s) {
+                       const int4* ent, int T, int in_pitch, int out_pitch, cudaStream_t s, int ones = 0) {
     SegArgs a;
     a.in = src; a.out = dst; a.tiles = tiles; a.ent = ent;
+    // 16-byte copies need 16-byte aligned rows (workspace planes always are;
+    // a caller's filterbank when its base is and ncols % 4 == 0)
+    a.vec = (in_pitch % 4 == 0 && (reinterpret_cast<uintptr_t>(src) & 15) == 0) ? 1 : 0;
+    a.ones = ones;
     a.ncols = T; a.in_pitch = in_pitch; a.out_pitch = out_pitch;
-    a.nlev = sp.l1 - sp.l0; a.max_thr = sp.max_thr;
+    a.nlev = sp.l1 - sp.l0 + (sp.r0c > 0 ? 1 : 0); a.max_thr = sp.max_thr;
     a.zx = sp.rows_x * sp.pitch; a.zy = sp.rows_y * sp.pitch;
     a.y0 = sp.y0; a.x1 = sp.x1; a.ent_base = sp.ent_base; a.max_ent = sp.max_ent;
     a.nrt = static_cast<int>(sp.tiles.size());
     const long long total = static_cast<long long>(a.nrt) * ((T + kSegTile - 1) / kSegTile);
     if (total > (1LL << 30)) return cudaErrorInvalidConfiguration;
     a.total = static_cast<int>(total);
-    const bool two = sp.smem_bytes <= kSegSmemTwoPerSm;
-    switch (sp.nc) {
-        case 9: return two ? launch_seg_nc<9, 256>(sp, a, s) : launch_seg_nc<9, 512>(sp, a, s);
-        case 10: return two ? launch_seg_nc<10, 256>(sp, a, s) : launch_seg_nc<10, 512>(sp, a, s);
-        case 12: return two ? launch_seg_nc<12, 256>(sp, a, s) : launch_seg_nc<12, 512>(sp, a, s);
-        default: return cudaErrorInvalidValue;
-    }
+    int threads = sp.threads;
+    if (threads == 0) threads = sp.smem_bytes <= kSegSmemTwoPerSm ? 256 : 512;
+    return launch_seg_r0c(sp, a, s, threads);
 }
 
 // Row pitch (elements) of the workspace planes: ncols rounded up to 128 bytes.
@@ -970,6 +1124,9 @@ static bfs_status build_passes(const bfs_fdmt_desc* desc, bfs_fdmt_plan* p) {
             kSegMaxLevels);
     BFS_ARG(desc->seg_rows >= 0, "seg_rows %d is negative", desc->seg_rows);
     const bool explicit_seg = desc->seg_levels >= 2 || desc->seg_rows > 0;
+    BFS_ARG(desc->seg_threads == 0 || desc->seg_threads == 256 || desc->seg_threads == 512 ||
+                desc->seg_threads == 1024,
+            "seg_threads %d is not 0, 256, 512 or 1024", desc->seg_threads);
     BFS_ARG(!explicit_seg || p->precision == BFS_PREC_F32,
             "fused merge segments are implemented for FP32 plans");
     p->passes.clear();
@@ -987,6 +1144,24 @@ static bfs_status build_passes(const bfs_fdmt_desc* desc, bfs_fdmt_plan* p) {
         int l0 = k;
         for (int i = 0; i < nseg; ++i) {
             const int l1 = l0 + left / nseg + (i < left % nseg ? 1 : 0);
+            // no head: the first segment reads the channels and forms level 0
+            // itself (no level-0 plane), where the plan's level 0 allows it
+            if (i == 0 && k == 0 && h.kind == BFS_PLAN_KEITH && l1 >= 2) {
+                bool ok = false;
+                for (int G : {desc->seg_rows > 0 ? desc->seg_rows : 32, 16}) {
+                    for (size_t limit : {kHeadSmemTwoPerSm, kHeadSmemMax}) {
+                        SegPlan sp;
+                        if (!ok && build_seg_plan(h, 0, l1, G, kSegTile, limit, &sp, true)) {
+                            p->passes.push_back(std::move(sp));
+                            ok = true;
+                        }
+                    }
+                }
+                if (ok) {
+                    l0 = l1;
+                    continue;
+                }
+            }
             if (l1 == l0 + 1) {
                 plain(l1);
             } else {
@@ -1012,11 +1187,15 @@ static bfs_status build_passes(const bfs_fdmt_desc* desc, bfs_fdmt_plan* p) {
             l0 = l1;
         }
     }
-    // planes in HBM: level k, then every pass's output, alternating between
-    // the two buffers (the last level goes to the caller's output)
+    for (SegPlan& sp : p->passes) sp.threads = desc->seg_threads;
+    // planes in HBM: level k (unless an input segment forms it on chip), then
+    // every pass's output, alternating between the two buffers (the last
+    // level goes to the caller's output)
     p->plane_buf.assign(h.niter + 1, -1);
     int b = 0;
-    p->plane_buf[k] = b;
+    const bool in_seg = !p->passes.empty() && p->passes[0].r0c > 0;
+    if (!in_seg) p->plane_buf[k] = b;
+    else b = 1;
     for (const SegPlan& sp : p->passes) p->plane_buf[sp.l1] = (b ^= 1);
     p->buf_rows[0] = p->buf_rows[1] = 0;
     for (int l = k; l < h.niter; ++l)
@@ -1348,13 +1527,13 @@ extern "C" bfs_status bfs_fdmt_plan_passes(const bfs_fdmt_plan* plan, int* npass
     const int n = static_cast<int>(plan->passes.size());
     *npasses = n;
     if (params) {
-        BFS_ARG(cap >= 12 * n, "params needs %d ints", 12 * n);
+        BFS_ARG(cap >= 13 * n, "params needs %d ints", 13 * n);
         for (int i = 0; i < n; ++i) {
             const SegPlan& sp = plan->passes[i];
-            const int v[12] = {sp.l0, sp.l1, sp.rows, sp.tile, sp.nc, sp.pitch, sp.rows_x, sp.rows_y,
+            const int v[13] = {sp.l0, sp.l1, sp.rows, sp.tile, sp.nc, sp.pitch, sp.rows_x, sp.rows_y,
                                sp.max_ent, sp.max_thr, static_cast<int>(sp.tiles.size()),
-                               static_cast<int>(sp.ent.size() / 4)};
-            std::memcpy(params + 12 * i, v, sizeof(v));
+                               static_cast<int>(sp.ent.size() / 4), sp.r0c};
+            std::memcpy(params + 13 * i, v, sizeof(v));
         }
     }
     return BFS_OK;
@@ -1556,12 +1735,15 @@ static bfs_status fdmt_run(bfs_fdmt_plan* plan, const float* d_in, float* d_out,
     auto plane = [&](int l) { return l == h.niter ? d_out : bufs[plan->plane_buf[l]]; };
     auto pitch = [&](int l) { return l == h.niter ? T : P; };
     const int k = plan->head.depth;
+    const bool in_seg = !plan->passes.empty() && plan->passes[0].r0c > 0;
     if (k > 0) {
         const HeadPlan& hp = plan->head;
         BFS_ARG(h.nchan / hp.group <= 65535, "nchan too large for this build");
         cudaError_t e = launch_head<float>(hp, h, d_in, plane(k), pitch(k), plan->d_head_groups,
                                            plan->d_head_tab, b_ones ? 1 : 0, s);
         if (e != cudaSuccess) return fail(BFS_ERR_CUDA, "k_fdmt_head: %s", cudaGetErrorString(e));
+    } else if (in_seg) {
+        // level 0 is formed by the first segment from the channels
     } else {
         BFS_ARG(h.nchan <= 65535, "nchan too large for this build");
         cudaError_t e = launch_init<float>(d_in, plane(0), h, P, b_ones ? 1 : 0, s, plan->d_lvl0);
@@ -1569,11 +1751,15 @@ static bfs_status fdmt_run(bfs_fdmt_plan* plan, const float* d_in, float* d_out,
     }
     for (size_t i = 0; i < plan->passes.size(); ++i) {
         const SegPlan& sp = plan->passes[i];
-        const float* src = plane(sp.l0);
+        const float* src = sp.r0c > 0 ? d_in : plane(sp.l0);
         cudaError_t e;
         if (sp.tiles.empty()) {
             e = launch_level(src, plane(sp.l1), plan->d_tab + plan->tab_off[sp.l1],
                              h.lv[sp.l1].total_rows(), T, P, pitch(sp.l1), s);
+        } else if (sp.r0c > 0) {  // input segment: the caller's filterbank (pitch ncols)
+            e = launch_seg(sp, d_in, plane(sp.l1), plan->d_seg_tiles + plan->seg_tile0[i],
+                           reinterpret_cast<const int4*>(plan->d_seg_ent + plan->seg_ent0[i]), T, T,
+                           pitch(sp.l1), s, b_ones ? 1 : 0);
         } else {
             e = launch_seg(sp, src, plane(sp.l1), plan->d_seg_tiles + plan->seg_tile0[i],
                            reinterpret_cast<const int4*>(plan->d_seg_ent + plan->seg_ent0[i]), T, P,

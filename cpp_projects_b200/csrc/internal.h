@@ -177,6 +177,9 @@ struct SegPlan {
     int rows_x = 0, rows_y = 0;  // rows of buffer X (levels l0, l0+2, ..) and Y (l0+1, ..)
     int size_x = 0, size_y = 0;  // floats of a buffer: its rows, the -0.0 row, the guard row
     int max_thr = 0;             // tiles with t0 >= max_thr never need the t >= shift test
+    int threads = 0;             // CTA size of its kernel (0: 256 when two CTAs fit an SM, else 512)
+    int r0c = 0;                 // input segment (levels 1..l1 straight from the channels):
+                                 // level-0 rows per channel; 0 = the input is a level plane
     int max_in_rows = 0;         // most input rows of one tile
     int64_t in_rows = 0;         // input rows summed over tiles (HBM reads per time tile)
     int y0 = 0, x1 = 0;          // offsets of buffers Y and X1 (X0 is at 0)
@@ -187,10 +190,19 @@ struct SegPlan {
     std::vector<int> ent;
 };
 
+// Input segment (from_input, BFS_PLAN_KEITH, l0 = 0): the tile's input rows
+// are channels of the filterbank, each over the window its level-0 rows need
+// (r more samples on the left for the running mean of row r), and level 1
+// is formed straight from them: a level-1 entry's w packs the destination
+// (low 20 bits), the tail and head rows' level-0 row numbers (4 bits each at
+// 20 and 24) and the shift (4 bits at 28); its x / y point at sample t of the
+// tail channel and t - shift of the head channel.  No level-0 plane exists.
+//
 // Segment plan for levels l0+1..l1 with `rows` output rows and `tile`
 // samples per tile; false when it needs more than kSegMaxLevels levels,
-// kSegMaxChunks chunks per row or smem_limit bytes of shared memory.
+// kSegMaxChunks chunks per row or smem_limit bytes of shared memory (or, for
+// an input segment, a level-0 depth, shift or offset beyond its packing).
 bool build_seg_plan(const FdmtPlanHost& p, int l0, int l1, int rows, int tile, size_t smem_limit,
-                    SegPlan* out);
+                    SegPlan* out, bool from_input = false);
 
 }  // namespace bfs

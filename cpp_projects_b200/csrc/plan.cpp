@@ -218,9 +218,11 @@ bool build_head_plan(const FdmtPlanHost& p, int k, int tile, size_t smem_limit, 
 }
 
 bool build_seg_plan(const FdmtPlanHost& p, int l0, int l1, int G, int TT, size_t smem_limit,
-                    SegPlan* out) {
+                    SegPlan* out, bool from_input) {
     const int m = l1 - l0;
     if (m < 1 || m > kSegMaxLevels || l0 < 0 || l1 > p.niter || G < 1 || TT != kSegTile) return false;
+    const int r0c = p.rows_per_chan0;
+    if (from_input && (p.kind != BFS_PLAN_KEITH || l0 != 0 || m < 2 || r0c < 1 || r0c > 5)) return false;
     // window of a row: {lo, hi} = least and largest total head shift from the tile's rows
     struct Win { int row, lo, hi; };
     const int R = p.lv[l1].total_rows();
@@ -250,6 +252,24 @@ bool build_seg_plan(const FdmtPlanHost& p, int l0, int l1, int G, int TT, size_t
             }
             for (const Win& w : need[i - 1]) spread = std::max(spread, w.hi - w.lo);
         }
+        if (from_input) {
+            // level-0 row (c, r) at sample t is the running mean of channel c
+            // over x[t-r .. t]: the channel's window reaches r samples further
+            // left than the row's.  The tile's channels go in front (its
+            // input rows); the level-0 rows become a level formed in shared
+            // memory.
+            std::vector<Win> ch;
+            for (const Win& w : need[0]) {
+                const int c = w.row / r0c, r = w.row % r0c;
+                if (!ch.empty() && ch.back().row == c) {
+                    ch.back().lo = std::min(ch.back().lo, w.lo);
+                    ch.back().hi = std::max(ch.back().hi, w.hi + r);
+                } else {
+                    ch.push_back({c, w.lo, w.hi + r});
+                }
+            }
+            need.insert(need.begin(), std::move(ch));
+        }
         // input rows start their window on a multiple of 4 samples (16-byte
         // copies): the lead grows to the next multiple of 4, the window by as much
         for (Win& w : need[0]) {
@@ -261,14 +281,17 @@ bool build_seg_plan(const FdmtPlanHost& p, int l0, int l1, int G, int TT, size_t
     }
     SegPlan s;
     s.l0 = l0; s.l1 = l1; s.rows = G; s.tile = TT;
+    s.r0c = from_input ? r0c : 0;
     // chunks per shared row, rounded up to a count the kernel instantiates
     // (9, 10 or 12 for the 256-sample tile)
     const int nc = (TT + spread + 31) / 32;
     s.nc = nc <= 9 ? 9 : nc <= 10 ? 10 : 12;
     if (nc > kSegMaxChunks) return false;
     s.pitch = 32 * s.nc;
+    const int mk = m + (from_input ? 1 : 0);  // levels the kernel forms above its input rows
+    if (mk > kSegMaxLevels) return false;
     for (const auto& need : tiles) {
-        for (int i = 0; i < m; ++i) {
+        for (int i = 0; i < mk; ++i) {
             int& r = (i & 1) ? s.rows_y : s.rows_x;
             r = std::max(r, static_cast<int>(need[i].size()));
         }
@@ -282,7 +305,7 @@ bool build_seg_plan(const FdmtPlanHost& p, int l0, int l1, int G, int TT, size_t
     s.ent_base = s.x1 + s.size_x;
     for (const auto& need : tiles) {
         int ne = 0;
-        for (int i = 0; i <= m; ++i) ne += static_cast<int>(need[i].size());
+        for (int i = 0; i <= mk; ++i) ne += static_cast<int>(need[i].size());
         s.max_ent = std::max(s.max_ent, ne);
     }
     s.smem_bytes = static_cast<size_t>(s.ent_base) * sizeof(float) + 2 * static_cast<size_t>(s.max_ent) * 16;
@@ -295,20 +318,37 @@ bool build_seg_plan(const FdmtPlanHost& p, int l0, int l1, int G, int TT, size_t
     for (const auto& need : tiles) {
         SegTile st{};
         st.ent = static_cast<int>(s.ent.size() / 4);
-        for (int i = 0; i <= m; ++i) st.n[i] = static_cast<int>(need[i].size());
+        for (int i = 0; i <= mk; ++i) st.n[i] = static_cast<int>(need[i].size());
         for (int j = 0; j < st.n[0]; ++j) {
             const Win& w = need[0][j];
             s.ent.insert(s.ent.end(), {w.row, w.hi, 0, j * s.pitch});
         }
+        if (from_input) {
+            // level 0 from the channels: x = the channel's sample t, z = the
+            // first sample that is not 0 (the row number r, plus the lead),
+            // w = destination | r << 20
+            for (int j = 0; j < st.n[1]; ++j) {
+                const Win& w = need[1][j];
+                const int c = w.row / r0c, r = w.row % r0c;
+                const int jc = slot_of(need[0], c);
+                const int off = need[0][jc].hi - w.hi;
+                if (off < r || off > s.pitch || need[0][jc].lo > w.lo) return false;
+                s.max_thr = std::max(s.max_thr, r + w.hi);
+                if (j * s.pitch >= (1 << 20)) return false;
+                s.ent.insert(s.ent.end(), {jc * s.pitch + off, 0, r + w.hi, j * s.pitch | (r << 20)});
+            }
+        }
+        const int k0 = from_input ? 1 : 0;  // need[k0] holds level l0
         for (int i = 1; i <= m; ++i) {
             const FdmtLevel& L = p.lv[l0 + i];
-            const std::vector<Win>& lower = need[i - 1];
-            for (int j = 0; j < st.n[i]; ++j) {
-                const Win& w = need[i][j];
+            const std::vector<Win>& lower = need[k0 + i - 1];
+            const int ki = k0 + i;                 // kernel level: buffer X when even, Y when odd
+            for (int j = 0; j < st.n[ki]; ++j) {
+                const Win& w = need[ki][j];
                 const int eg = i == m ? 0 : w.hi;  // output rows: lead 0 (samples t0 ..)
                 const int ja = slot_of(lower, L.a_row[w.row]);
                 const int offa = ja * s.pitch + (lower[ja].hi - eg);
-                int offb = zero_of(i - 1), thr = 0;
+                int offb = zero_of(ki - 1), thr = 0;
                 if (L.b_row[w.row] >= 0) {
                     const int jb = slot_of(lower, L.b_row[w.row]);
                     const int sh = L.shift[w.row];

@@ -90,7 +90,8 @@ typedef struct bfs_fdmt_desc {
                           0: 3; 1: one pass per level; 2..6                              */
     int seg_rows;      /* output rows per tile of a fused pass (0: the most that keep
                           two CTAs per SM, of 64 / 32 / 16)                              */
-    int reserved[1];
+    int seg_threads;   /* threads per CTA of the fused passes: 256, 512, 1024 (0: 256
+                          when two CTAs fit an SM, else 512)                             */
 } bfs_fdmt_desc;
 
 typedef struct bfs_fdmt_plan bfs_fdmt_plan;
@@ -144,11 +145,13 @@ bfs_status bfs_fdmt_plan_head(const bfs_fdmt_plan* plan, int* params, int* group
                               int* tab, int tab_cap);
 /* Merge passes after the fused head (no reference counterpart; introspection
  * for tests and tuning): *npasses receives their number; params (optional,
- * cap ints) 12 ints per pass {first input level l0, output level l1, output
+ * cap ints) 13 ints per pass {first input level l0, output level l1, output
  * rows per tile, samples per tile, 32-column chunks per shared row, shared
  * row pitch, shared rows of buffer X, of buffer Y, most entries of a tile,
- * largest head-row threshold, tiles, entries}.  A pass with 0 tiles is one
- * plain merge level; the others fuse levels l0+1..l1 in shared memory. */
+ * largest threshold, tiles, entries, level-0 rows per channel of an input
+ * segment (0: the pass reads a level plane)}.  A pass with 0 tiles is one
+ * plain merge level; the others fuse levels l0+1..l1 in shared memory; an
+ * input segment reads the filterbank's channels and forms level 0 itself. */
 bfs_status bfs_fdmt_plan_passes(const bfs_fdmt_plan* plan, int* npasses, int* params, int cap);
 /* One fused pass's tiles (8 ints each: first entry, input rows, then the
  * rows of levels l0+1.. up to 6 levels) and entries (4 ints each: input rows

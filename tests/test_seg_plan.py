@@ -14,7 +14,7 @@ from oracle import pyoracle
 
 P = ctypes.c_void_p
 TILE_INTS = 8
-PASS_INTS = 12
+PASS_INTS = 13
 
 
 def plan_passes(fmin, fmax, nchan, ncols, max_dt, fuse, seg_levels=0, seg_rows=0):
@@ -89,8 +89,9 @@ def emulate_seg(src, pr, tiles, ent, ncols, out_rows, fill=0.0):
     samples outside [0, ncols); fill=NaN shows that no written sample
     depends on them (the t >= shift test keeps them out)."""
     l0, l1, G, TT, nc, pitch, rx, ry, max_ent, max_thr = (int(v) for v in pr[:10])
-    m = l1 - l0
-    assert pitch == 32 * nc and TT % 32 == 0
+    r0c = int(pr[12])
+    m = l1 - l0 + (1 if r0c else 0)  # kernel levels above the input rows (an input
+    assert pitch == 32 * nc and TT % 32 == 0  # segment forms level 0 as its first)
     out = np.full((out_rows, ncols), np.nan, np.float32)
     cols = np.arange(nc * 32)
     ocols = np.arange(TT)
@@ -123,6 +124,24 @@ def emulate_seg(src, pr, tiles, ent, ncols, out_rows, fill=0.0):
                 q = e[:n[lev]]
                 rd = x if lev % 2 == 1 else y
                 c = ocols if lev == m else cols
+                if r0c and lev == 1:
+                    # level 0 from the channels: running mean of row r over
+                    # x[t-r .. t], one float32 rounding per operation, 0 before r
+                    for xo, _, thr, w in q:
+                        r, dst = (w >> 20) & 15, w & 0xFFFFF
+                        assert r < r0c
+                        ia = xo + cols
+                        assert (ia - r).min() >= 0 and ia.max() < rd.size
+                        v = rd[ia].copy()
+                        for k in range(1, r + 1):
+                            mm = v if k == 1 else (v * np.float32(k)).astype(np.float32)
+                            v = ((mm + rd[ia - k]).astype(np.float32) / np.float32(k + 1)).astype(np.float32)
+                        v = np.where(cols >= thr - t0, v, np.float32(0.0))
+                        idx = dst + cols
+                        assert idx.min() >= 0 and idx.max() < ry * pitch
+                        y[idx] = v
+                    e = e[n[lev]:]
+                    continue
                 ia = q[:, 0:1] + c[None, :]
                 ib = q[:, 1:2] + c[None, :]
                 assert ia.min() >= 0 and ia.max() < rd.size and ib.min() >= 0 and ib.max() < rd.size
@@ -145,9 +164,12 @@ def emulate_seg(src, pr, tiles, ent, ncols, out_rows, fill=0.0):
     return out
 
 
-def run_schedule(fmin, fmax, nchan, ncols, max_dt, fuse, seg_levels, seg_rows, seed):
+def run_schedule(fmin, fmax, nchan, ncols, max_dt, fuse, seg_levels, seg_rows, seed, with_zeros=False):
     k, rows, passes = plan_passes(fmin, fmax, nchan, ncols, max_dt, fuse, seg_levels, seg_rows)
     x = np.random.default_rng(seed).standard_normal((nchan, ncols)).astype(np.float32)
+    if with_zeros:  # signed zeros and tiny values through the level-0 means
+        x[:, ::7] = np.float32(-0.0)
+        x[::3, 5::11] = np.float32(1e-40)
     niter = rows.size - 1
     planes = level_planes(fmin, fmax, x, nchan, ncols, max_dt, niter)
     cur, lev = planes[k], k
@@ -155,7 +177,14 @@ def run_schedule(fmin, fmax, nchan, ncols, max_dt, fuse, seg_levels, seg_rows, s
     for pr, tiles, ent in passes:
         l0, l1 = int(pr[0]), int(pr[1])
         assert l0 == lev and l1 > l0
-        if len(tiles) == 0:
+        if int(pr[12]):  # input segment: reads the channels, forms level 0 itself
+            assert l0 == 0 and k == 0 and len(tiles)
+            fused += 1
+            strict = emulate_seg(x, pr, tiles, ent, ncols, int(rows[l1]), fill=np.nan)
+            cur = emulate_seg(x, pr, tiles, ent, ncols, int(rows[l1]))
+            assert np.array_equal(cur.view(np.uint32), planes[l1].view(np.uint32)), f"levels 1..{l1}"
+            assert np.array_equal(strict.view(np.uint32), cur.view(np.uint32))
+        elif len(tiles) == 0:
             assert l1 == l0 + 1
             a, b, s = pyoracle.fdmt_tables(fmin, fmax, nchan, max_dt, l1)
             cur = merge_level(cur, a, b, s)
@@ -185,6 +214,21 @@ def test_segment_emulation_matches_oracle(case):
     fmin, fmax, nchan, ncols, max_dt, fuse, seg_levels, seg_rows = case
     fused = run_schedule(fmin, fmax, nchan, ncols, max_dt, fuse, seg_levels, seg_rows, seed=nchan)
     assert fused >= 1
+
+
+@pytest.mark.parametrize("case", [
+    (1200.0, 1600.0, 64, 700, 64, 0, 3, 16),
+    (1100.0, 1500.0, 128, 513, 100, 0, 4, 0),
+    (1200.0, 1600.0, 99, 531, 99, 0, 2, 8),      # odd channel count: a carried level-1 row
+    (1200.0, 1328.0, 64, 1031, 200, 0, 3, 32),   # max delay > channels: 5 level-0 rows per channel
+])
+def test_input_segment_emulation_matches_oracle(case):
+    """No head: the first segment stages the channels and forms level 0 in
+    shared memory (no level-0 plane); signed zeros and subnormals included."""
+    fmin, fmax, nchan, ncols, max_dt, fuse, seg_levels, seg_rows = case
+    k, rows, passes = plan_passes(fmin, fmax, nchan, ncols, max_dt, fuse, seg_levels, seg_rows)
+    assert int(passes[0][0][12]) >= 1, "the first pass is an input segment"
+    run_schedule(fmin, fmax, nchan, ncols, max_dt, fuse, seg_levels, seg_rows, seed=nchan + 1, with_zeros=True)
 
 
 def test_segment_geometry_at_search_shapes():
