@@ -432,6 +432,14 @@ def run_ours(args):
         if all(str(b.nchan) in ratio for b in beams):
             traffic = sum(sb * ratio[str(b.nchan)] for sb, b in zip(sched, beams))
     compulsory = sum(4.0 * b.nsamp * (b.nchan + 3 * b.max_dt) for b in beams)
+    # the autotuner's schedules: beams per (head depth or input segment, HBM passes)
+    sched_counts = {}
+    for p in pipe.plans:
+        passes = p.passes()
+        first = "head %d" % p.info.fuse_depth if p.info.fuse_depth else (
+            "input segment" if passes and passes[0][2] > 0 else "level 0")
+        key = f"{first}, {p.info.hbm_passes} merge passes"
+        sched_counts[key] = sched_counts.get(key, 0) + 1
     pipe_bytes = fdmt_bytes + pipe.search_alg_bytes()
 
     # ---- end to end: pinned host inputs, copied every step ------------------
@@ -504,7 +512,7 @@ def run_ours(args):
                          "compulsory_io_bytes_per_step": compulsory,
                          "compulsory_io": "input read + FDMT output written + row statistics and "
                                           "boxcar reads of the output",
-                         "fdmt_ms_per_step": fdmt_ms,
+                         "fdmt_ms_per_step": fdmt_ms, "schedules": sched_counts,
                          "timed_in": "plain per-beam form (events around each beam's FDMT; "
                                      "same autotuned plans as the batched form)"},
             "plain": {"value": units / (plain_ms / 1e3), "ms_per_step": plain_ms,

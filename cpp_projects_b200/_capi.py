@@ -19,6 +19,7 @@ STATUS_NAMES = {0: "BFS_OK", 1: "BFS_ERR_ARG", 2: "BFS_ERR_CUDA", 3: "BFS_ERR_OV
 BFS_WIDTHS_POW2, BFS_WIDTHS_ALL = 0, 1
 BFS_FDMT_EXTERNAL_WS = 1
 BFS_FUSE_AUTOTUNE = -2
+BFS_SEG_SINGLE_BUFFER = 1
 BFS_PREC_F32, BFS_PREC_F16, BFS_PREC_BF16 = 0, 1, 2
 BFS_PLAN_KEITH, BFS_PLAN_PRAVIR = 0, 1
 
@@ -35,7 +36,7 @@ class FdmtDesc(ctypes.Structure):
                 ("precision", ctypes.c_int), ("fuse_depth", ctypes.c_int),
                 ("flags", ctypes.c_int), ("head_tile", ctypes.c_int), ("dt_min", ctypes.c_int),
                 ("dt_step", ctypes.c_int), ("tsamp", ctypes.c_float), ("seg_levels", ctypes.c_int),
-                ("seg_rows", ctypes.c_int), ("seg_threads", ctypes.c_int)]
+                ("seg_rows", ctypes.c_int), ("seg_threads", ctypes.c_int), ("seg_flags", ctypes.c_int)]
 
 
 class FdmtInfo(ctypes.Structure):

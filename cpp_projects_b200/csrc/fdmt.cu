@@ -851,49 +851,49 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 256 ? 2 : 1) k_fdmt_seg(co
         lo = __ldg(t);
         hi = __ldg(t + 1);
     };
-    auto issue = [&](int rt, int tt, int buf) {
+    const bool single = a.x1 == 0;  // one input buffer: load after merging
+    constexpr int inw = kWarps;     // every warp issues its share of the copies
+    const bool issuer = true;
+    const int it = threadIdx.x;
+    // entries of a tile into entry buffer eb (tile j uses buffer j % 3; single: 0)
+    auto issue_ent = [&](int rt, int eb) {
         int4 lo, hi;
         tile_rec(rt, lo, hi);
-        const int t0 = tt * kSegTile;
-        const int nin = lo.y;
-        // entries: the counts of levels 0..nlev (ent, n0, n1, n2 | n3, n4, n5, n6)
         const int nent = lo.y + lo.z + lo.w + (a.nlev >= 3 ? hi.x : 0) + (a.nlev >= 4 ? hi.y : 0) +
                          (a.nlev >= 5 ? hi.z : 0) + (a.nlev >= 6 ? hi.w : 0);
         const int4* ge = a.ent + lo.x;
-        const unsigned se = sbase + 4u * (a.ent_base + 4 * buf * a.max_ent);
+        const unsigned se = sbase + 4u * (a.ent_base + 4 * eb * a.max_ent);
+        for (int i = it; i < nent; i += 32 * inw) cp_async16(se + 16u * i, ge + i, 16);
+    };
+    // input rows of a tile into X buffer `buf`, its row entries read from
+    // entry buffer eb (already in shared memory)
+    auto issue_rows = [&](int rt, int tt, int buf, int eb) {
+        const int nin = __ldg(&a.tiles[rt].n[0]);
+        const int t0 = tt * kSegTile;
+        const int4* q4 = reinterpret_cast<const int4*>(sm + a.ent_base) + eb * a.max_ent;
         const unsigned x = sbase + 4u * (buf ? a.x1 : 0);
-        for (int i = threadIdx.x; i < nent; i += THREADS) cp_async16(se + 16u * i, ge + i, 16);
-        for (int r0 = warp; r0 < nin; r0 += 4 * kWarps) {
-            int4 q[4];
+        for (int r = warp; r < nin; r += inw) {
+            const int4 q = q4[r];
+            const int ts = t0 - q.y;  // the row's first sample
+            const float* src = a.in + static_cast<size_t>(q.x) * a.in_pitch;
+            const unsigned dst = x + 4u * q.w;
+            if (a.ones) {  // the all-ones image: 1 inside [0, ncols), 0 outside
+                float* d = sm + (buf ? a.x1 : 0) + q.w;
+                for (int c = lane; c < 32 * NC; c += 32) d[c] = (ts + c >= 0 && ts + c < a.ncols) ? 1.0f : 0.0f;
+            } else if (!a.vec) {  // unaligned rows: 4-byte copies
+                for (int c = lane; c < 32 * NC; c += 32) {
+                    const int t = ts + c;
+                    const bool in = t >= 0 && t < a.ncols;
+                    cp_async4(dst + 4u * c, in ? src + t : src, in ? 4 : 0);
+                }
+            } else if (ts >= 0 && ts + 4 * kPieces <= a.ncols) {  // the whole window lies in [0, ncols)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int r = r0 + j * kWarps;
-                q[j] = r < nin ? __ldg(ge + r) : make_int4(0, 0, 0, 0);
-            }
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                if (r0 + j * kWarps >= nin) break;
-                const int ts = t0 - q[j].y;  // the row's first sample
-                const float* src = a.in + static_cast<size_t>(q[j].x) * a.in_pitch;
-                const unsigned dst = x + 4u * q[j].w;
-                if (a.ones) {  // the all-ones image: 1 inside [0, ncols), 0 outside
-                    float* d = sm + (buf ? a.x1 : 0) + q[j].w;
-                    for (int c = lane; c < 32 * NC; c += 32) d[c] = (ts + c >= 0 && ts + c < a.ncols) ? 1.0f : 0.0f;
-                } else if (!a.vec) {  // unaligned rows: 4-byte copies
-                    for (int c = lane; c < 32 * NC; c += 32) {
-                        const int t = ts + c;
-                        const bool in = t >= 0 && t < a.ncols;
-                        cp_async4(dst + 4u * c, in ? src + t : src, in ? 4 : 0);
-                    }
-                } else if (ts >= 0 && ts + 4 * kPieces <= a.ncols) {  // the whole window lies in [0, ncols)
-#pragma unroll
-                    for (int pc = lane; pc < kPieces; pc += 32) cp_async16(dst + 16u * pc, src + ts + 4 * pc, 16);
-                } else {
-                    for (int pc = lane; pc < kPieces; pc += 32) {
-                        const int t = ts + 4 * pc;
-                        const int bytes = t < 0 ? 0 : 4 * max(0, min(4, a.ncols - t));
-                        cp_async16(dst + 16u * pc, bytes > 0 ? src + t : src, bytes);
-                    }
+                for (int pc = lane; pc < kPieces; pc += 32) cp_async16(dst + 16u * pc, src + ts + 4 * pc, 16);
+            } else {
+                for (int pc = lane; pc < kPieces; pc += 32) {
+                    const int t = ts + 4 * pc;
+                    const int bytes = t < 0 ? 0 : 4 * max(0, min(4, a.ncols - t));
+                    cp_async16(dst + 16u * pc, bytes > 0 ? src + t : src, bytes);
                 }
             }
         }
@@ -907,17 +907,39 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 256 ? 2 : 1) k_fdmt_seg(co
         tt += gq;
         if (rt >= a.nrt) { rt -= a.nrt; ++tt; }
     };
+    const int cw = warp, ncw = kWarps;  // merging warps
+    auto level_sync = [&]() { __syncthreads(); };
+    const int G = static_cast<int>(gridDim.x);
     int w = blockIdx.x;
     int rt = w % a.nrt, tt = w / a.nrt;  // this CTA's current tile
-    if (w < a.total) issue(rt, tt, 0);
-    for (int j = 0; w < a.total; ++j, w += gridDim.x) {
-        const int buf = j & 1;
+    // prologue: entries of the first two tiles, then the first tile's rows
+    if (w < a.total && issuer) {
+        issue_ent(rt, 0);
+        if (!single && w + G < a.total) {
+            int r1 = rt, t1 = tt;
+            step(r1, t1);
+            issue_ent(r1, 1);
+        }
         cp_async_wait_all();
-        __syncthreads();  // this tile's rows are in; every warp is done with the previous tile
+    }
+    __syncthreads();
+    if (w < a.total && issuer) issue_rows(rt, tt, 0, 0);
+    for (int j = 0; w < a.total; ++j, w += G) {
+        const int buf = single ? 0 : j & 1;
+        const int eb = single ? 0 : j % 3;
+        cp_async_wait_all();
+        __syncthreads();  // this tile's rows (and the next tile's entries) are in; the previous tile is done
         int rn = rt, tn = tt;
         step(rn, tn);
-        if (w + static_cast<int>(gridDim.x) < a.total) issue(rn, tn, buf ^ 1);
-
+        const bool more = w + G < a.total;
+        if (!single && issuer) {
+            if (w + 2 * G < a.total) {  // entries two tiles ahead
+                int r2 = rn, t2 = tn;
+                step(r2, t2);
+                issue_ent(r2, (j + 2) % 3);
+            }
+            if (more) issue_rows(rn, tn, buf ^ 1, (j + 1) % 3);
+        }
         int4 lo, hi;
         tile_rec(rt, lo, hi);
         const int nlv[kSegMaxLevels + 1] = {lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
@@ -925,7 +947,7 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 256 ? 2 : 1) k_fdmt_seg(co
         rt = rn;
         tt = tn;
         const int xo = buf ? a.x1 : 0;  // this tile's X buffer
-        const int4* e = reinterpret_cast<const int4*>(sm + a.ent_base) + buf * a.max_ent + nlv[0];
+        const int4* e = reinterpret_cast<const int4*>(sm + a.ent_base) + eb * a.max_ent + nlv[0];
         const bool fast = t0 >= a.max_thr;  // no sample of this tile precedes its head row's shift
 #pragma unroll
         for (int lev = 1; lev < kSegMaxLevels; ++lev) {
@@ -935,23 +957,23 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 256 ? 2 : 1) k_fdmt_seg(co
             const int wr = (lev & 1) ? a.y0 : xo;
             if (R0C > 0 && lev == 1) {  // input segment: level 0 from the staged channels
                 if (fast) {
-                    for (int r = warp; r < nl; r += kWarps) seg_level0_row<R0C, NC, true>(sm, rd, wr, e[r], lane, t0);
+                    for (int r = cw; r < nl; r += ncw) seg_level0_row<R0C, NC, true>(sm, rd, wr, e[r], lane, t0);
                 } else {
-                    for (int r = warp; r < nl; r += kWarps) seg_level0_row<R0C, NC, false>(sm, rd, wr, e[r], lane, t0);
+                    for (int r = cw; r < nl; r += ncw) seg_level0_row<R0C, NC, false>(sm, rd, wr, e[r], lane, t0);
                 }
             } else if (fast) {
-                for (int r = warp; r < nl; r += 2 * kWarps) {
-                    const int r1 = r + kWarps;
+                for (int r = cw; r < nl; r += 2 * ncw) {
+                    const int r1 = r + ncw;
                     seg_rows2<NC>(sm, rd, wr, e[r], e[r1 < nl ? r1 : r], r1 < nl, lane);
                 }
             } else {
-                for (int r = warp; r < nl; r += kWarps) {
+                for (int r = cw; r < nl; r += ncw) {
                     const int4 q = e[r];
                     seg_chunks<NC, false>(sm, rd, wr, q, 0, lane, q.z - t0);
                 }
             }
             e += nl;
-            __syncthreads();
+            level_sync();
         }
         // level l1: kSegTile samples per row, straight to HBM (q.w is the plane row)
         int nl = nlv[1];
@@ -959,7 +981,7 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 256 ? 2 : 1) k_fdmt_seg(co
         for (int i = 2; i <= kSegMaxLevels; ++i)
             if (i == a.nlev) nl = nlv[i];
         const int rd = (a.nlev & 1) ? xo : a.y0;
-        for (int r = warp; r < nl; r += kWarps) {
+        for (int r = cw; r < nl; r += ncw) {
             const int4 q = e[r];
             const int col = lane;
             const int pa = rd + q.x + col, pb = rd + q.y + col;
@@ -975,6 +997,13 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 256 ? 2 : 1) k_fdmt_seg(co
 #pragma unroll
             for (int k = 0; k < kOutCPH; ++k)
                 if (32 * k < lim) dst[32 * k] = (fast || col + 32 * k >= thr) ? __fadd_rn(va[k], vb[k]) : va[k];
+        }
+        if (single && more) {  // every warp is done with the buffers: load the next tile
+            __syncthreads();
+            issue_ent(rn, 0);
+            cp_async_wait_all();
+            __syncthreads();
+            issue_rows(rn, tn, 0, 0);
         }
     }
 }
@@ -1124,6 +1153,8 @@ static bfs_status build_passes(const bfs_fdmt_desc* desc, bfs_fdmt_plan* p) {
             kSegMaxLevels);
     BFS_ARG(desc->seg_rows >= 0, "seg_rows %d is negative", desc->seg_rows);
     const bool explicit_seg = desc->seg_levels >= 2 || desc->seg_rows > 0;
+    BFS_ARG((desc->seg_flags & ~BFS_SEG_SINGLE_BUFFER) == 0, "unknown seg_flags 0x%x", desc->seg_flags);
+    const bool single = (desc->seg_flags & BFS_SEG_SINGLE_BUFFER) != 0;
     BFS_ARG(desc->seg_threads == 0 || desc->seg_threads == 256 || desc->seg_threads == 512 ||
                 desc->seg_threads == 1024,
             "seg_threads %d is not 0, 256, 512 or 1024", desc->seg_threads);
@@ -1151,7 +1182,7 @@ static bfs_status build_passes(const bfs_fdmt_desc* desc, bfs_fdmt_plan* p) {
                 for (int G : {desc->seg_rows > 0 ? desc->seg_rows : 32, 16}) {
                     for (size_t limit : {kHeadSmemTwoPerSm, kHeadSmemMax}) {
                         SegPlan sp;
-                        if (!ok && build_seg_plan(h, 0, l1, G, kSegTile, limit, &sp, true)) {
+                        if (!ok && build_seg_plan(h, 0, l1, G, kSegTile, limit, &sp, true, single)) {
                             p->passes.push_back(std::move(sp));
                             ok = true;
                         }
@@ -1173,7 +1204,7 @@ static bfs_status build_passes(const bfs_fdmt_desc* desc, bfs_fdmt_plan* p) {
                 bool ok = false;
                 for (const auto& [G, limit] : rows_try) {
                     SegPlan sp;
-                    if (build_seg_plan(h, l0, l1, G, kSegTile, limit, &sp)) {
+                    if (build_seg_plan(h, l0, l1, G, kSegTile, limit, &sp, false, single)) {
                         p->passes.push_back(std::move(sp));
                         ok = true;
                         break;

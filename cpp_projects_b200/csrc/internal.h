@@ -178,6 +178,7 @@ struct SegPlan {
     int size_x = 0, size_y = 0;  // floats of a buffer: its rows, the -0.0 row, the guard row
     int max_thr = 0;             // tiles with t0 >= max_thr never need the t >= shift test
     int threads = 0;             // CTA size of its kernel (0: 256 when two CTAs fit an SM, else 512)
+    bool single = false;         // one input buffer: the next tile loads after this one is merged
     int r0c = 0;                 // input segment (levels 1..l1 straight from the channels):
                                  // level-0 rows per channel; 0 = the input is a level plane
     int max_in_rows = 0;         // most input rows of one tile
@@ -203,6 +204,6 @@ struct SegPlan {
 // kSegMaxChunks chunks per row or smem_limit bytes of shared memory (or, for
 // an input segment, a level-0 depth, shift or offset beyond its packing).
 bool build_seg_plan(const FdmtPlanHost& p, int l0, int l1, int rows, int tile, size_t smem_limit,
-                    SegPlan* out, bool from_input = false);
+                    SegPlan* out, bool from_input = false, bool single = false);
 
 }  // namespace bfs

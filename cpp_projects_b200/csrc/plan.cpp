@@ -218,7 +218,7 @@ bool build_head_plan(const FdmtPlanHost& p, int k, int tile, size_t smem_limit, 
 }
 
 bool build_seg_plan(const FdmtPlanHost& p, int l0, int l1, int G, int TT, size_t smem_limit,
-                    SegPlan* out, bool from_input) {
+                    SegPlan* out, bool from_input, bool single) {
     const int m = l1 - l0;
     if (m < 1 || m > kSegMaxLevels || l0 < 0 || l1 > p.niter || G < 1 || TT != kSegTile) return false;
     const int r0c = p.rows_per_chan0;
@@ -301,14 +301,18 @@ bool build_seg_plan(const FdmtPlanHost& p, int l0, int l1, int G, int TT, size_t
     s.size_x = (s.rows_x + 2) * s.pitch;
     s.size_y = (s.rows_y + 2) * s.pitch;
     s.y0 = s.size_x;
-    s.x1 = s.size_x + s.size_y;
-    s.ent_base = s.x1 + s.size_x;
+    s.single = single;
+    s.x1 = single ? 0 : s.size_x + s.size_y;  // single: X1 is X0
+    s.ent_base = single ? s.size_x + s.size_y : s.x1 + s.size_x;
     for (const auto& need : tiles) {
         int ne = 0;
         for (int i = 0; i <= mk; ++i) ne += static_cast<int>(need[i].size());
         s.max_ent = std::max(s.max_ent, ne);
     }
-    s.smem_bytes = static_cast<size_t>(s.ent_base) * sizeof(float) + 2 * static_cast<size_t>(s.max_ent) * 16;
+    // entries: one buffer (single), else three (tile j's, j+1's, and j+2's
+    // arriving two tiles ahead of use)
+    s.smem_bytes = static_cast<size_t>(s.ent_base) * sizeof(float) +
+                   (single ? 1 : 3) * static_cast<size_t>(s.max_ent) * 16;
     if (s.smem_bytes > smem_limit) return false;
     auto zero_of = [&](int i) { return ((i & 1) ? s.rows_y : s.rows_x) * s.pitch; };
     auto slot_of = [](const std::vector<Win>& v, int row) {

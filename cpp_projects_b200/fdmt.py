@@ -43,7 +43,8 @@ def autotune_desc(desc: "_capi.FdmtDesc") -> tuple["_capi.FdmtDesc", float]:
 class CFdmtGpu:
     def __init__(self, Fmin: float, Fmax: float, nchan: int, cols: int, imaxDt: int,
                  fuse_depth: int = -1, external_ws: bool = False, head_tile: int = 0,
-                 precision: int = 0, seg_levels: int = 0, seg_rows: int = 0, seg_threads: int = 0):
+                 precision: int = 0, seg_levels: int = 0, seg_rows: int = 0, seg_threads: int = 0,
+                 seg_flags: int = 0):
         self.m_Fmin = float(Fmin)
         self.m_Fmax = float(Fmax)
         self.m_nchan = int(nchan)
@@ -55,7 +56,8 @@ class CFdmtGpu:
                               precision=int(precision), fuse_depth=int(fuse_depth),
                               flags=_capi.BFS_FDMT_EXTERNAL_WS if external_ws else 0,
                               head_tile=int(head_tile), seg_levels=int(seg_levels),
-                              seg_rows=int(seg_rows), seg_threads=int(seg_threads))
+                              seg_rows=int(seg_rows), seg_threads=int(seg_threads),
+                              seg_flags=int(seg_flags))
         self._plan = ctypes.c_void_p()
         _capi.call("bfs_fdmt_plan_create", ctypes.byref(desc), ctypes.byref(self._plan))
         info = _capi.FdmtInfo()
@@ -128,13 +130,14 @@ class CFdmtGpu:
 
     # --- plan introspection ------------------------------------------------
     def passes(self) -> list[list[int]]:
-        """[l0, l1] of every merge pass after the head: a plain level (l1 =
-        l0 + 1) or a fused segment of levels l0+1..l1."""
+        """[l0, l1, r0c] of every merge pass after the head: a plain level
+        (l1 = l0 + 1) or a fused segment of levels l0+1..l1; r0c > 0 marks an
+        input segment (it reads the channels and forms level 0 itself)."""
         n = ctypes.c_int(0)
         _capi.call("bfs_fdmt_plan_passes", self._plan, ctypes.byref(n), None, 0)
         p = np.zeros(max(1, n.value) * 13, np.int32)
         _capi.call("bfs_fdmt_plan_passes", self._plan, ctypes.byref(n), p.ctypes.data_as(ctypes.c_void_p), p.size)
-        return [[int(p[13 * i]), int(p[13 * i + 1])] for i in range(n.value)]
+        return [[int(p[13 * i]), int(p[13 * i + 1]), int(p[13 * i + 12])] for i in range(n.value)]
 
     @property
     def sched_bytes(self) -> float:

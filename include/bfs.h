@@ -92,7 +92,11 @@ typedef struct bfs_fdmt_desc {
                           two CTAs per SM, of 64 / 32 / 16)                              */
     int seg_threads;   /* threads per CTA of the fused passes: 256, 512, 1024 (0: 256
                           when two CTAs fit an SM, else 512)                             */
+    int seg_flags;     /* BFS_SEG_SINGLE_BUFFER: one input buffer per CTA (the next
+                          tile loads after the current one is merged; half the shared
+                          memory, so two CTAs fit an SM)                                 */
 } bfs_fdmt_desc;
+enum { BFS_SEG_SINGLE_BUFFER = 1 };
 
 typedef struct bfs_fdmt_plan bfs_fdmt_plan;
 

@@ -39,15 +39,22 @@ def _want4096(ncols):
 # (fuse_depth, head_tile, seg_levels, seg_rows): the tuned choice, one pass per
 # level, fused segments of 2 / 3 / 4 levels with 16 or 32 rows per tile, with
 # and without a head, the wide head tile
-SCHEDULES = [(-2, 0, 0, 0), (3, 256, 1, 0), (3, 512, 3, 32), (3, 256, 4, 16), (0, 0, 3, 16),
-             (4, 256, 2, 16), (2, 256, 3, 32)]
+# (fuse_depth, head_tile, seg_levels, seg_rows, seg_threads, seg_flags): the
+# tuned choice, one pass per level, fused segments of 2 / 3 / 4 levels with 16
+# or 32 rows per tile, with and without a head (without: the first segment
+# forms level 0 from the channels), the wide head tile, CTAs of 256 / 512 /
+# 1024 threads, one input buffer per CTA
+SCHEDULES = [(-2, 0, 0, 0, 0, 0), (3, 256, 1, 0, 0, 0), (3, 512, 3, 32, 0, 0), (3, 256, 4, 16, 0, 0),
+             (0, 0, 3, 16, 0, 0), (4, 256, 2, 16, 0, 0), (2, 256, 3, 32, 0, 0), (0, 0, 4, 32, 1024, 0),
+             (0, 0, 3, 32, 256, 1), (3, 256, 3, 16, 512, 1)]
 
 
 @pytest.mark.parametrize("ncols", [8192, 5003])
 @pytest.mark.parametrize("sched", SCHEDULES)
 def test_fdmt_4096_channels_bit_exact(cuda, ncols, sched):
-    fuse, tile, seg, rows = sched
-    f = CFdmtGpu(*BAND, 4096, ncols, 4096, fuse_depth=fuse, head_tile=tile, seg_levels=seg, seg_rows=rows)
+    fuse, tile, seg, rows, threads, flags = sched
+    f = CFdmtGpu(*BAND, 4096, ncols, 4096, fuse_depth=fuse, head_tile=tile, seg_levels=seg, seg_rows=rows,
+                 seg_threads=threads, seg_flags=flags)
     d_out = torch.full((4096, ncols), float("nan"), device=cuda)
     f.process_image(torch.from_numpy(_x4096(ncols)).to(cuda), d_out, False)
     assert np.array_equal(_bits(d_out.cpu().numpy()), _bits(_want4096(ncols)))

@@ -245,7 +245,7 @@ def test_segment_geometry_at_search_shapes():
                 continue
             l0, l1, G, TT, nc, pitch, rx, ry, max_ent = (int(v) for v in pr[:9])
             m = l1 - l0
-            smem = ((2 * (rx + 2) + ry + 2) * pitch) * 4 + 2 * max_ent * 16
+            smem = ((2 * (rx + 2) + ry + 2) * pitch) * 4 + 3 * max_ent * 16
             assert smem <= 227 * 1024 and nc in (9, 10, 12)
             seen = np.zeros(int(rows[l1]), np.int64)
             for tile in tiles:
