@@ -4,6 +4,7 @@
     python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
                     [--workload config2|config0|config1|config3|config4|config4fwd]
                     [--form both|batched] [--no-e2e] [--no-cpu-baseline] [--dry-run]
+                    [--save-schedules FILE | --schedules FILE]
 
 --gpus N without torchrun relaunches this script as N ranks through
 torch.distributed.run (127.0.0.1); under torchrun the ranks come from the
@@ -81,6 +82,11 @@ def parse_args(argv=None):
     ap.add_argument("--form", choices=["both", "batched"], default="both",
                     help="batched: time only the batched form (profiling runs; no plain-form "
                          "numbers, no FDMT roofline)")
+    ap.add_argument("--save-schedules", metavar="FILE",
+                    help="write the autotuner's FDMT schedule of every beam (JSON)")
+    ap.add_argument("--schedules", metavar="FILE",
+                    help="use these FDMT schedules (from --save-schedules) instead of autotuning: "
+                         "a profiled run then executes the kernels an unprofiled run chose")
     return ap.parse_args(argv)
 
 
@@ -336,7 +342,8 @@ def run_reference(args):
 def run_ours(args):
     import torch
 
-    from cpp_projects_b200.pipeline import BatchedSearch, BeamShape, SearchPipeline, device_filterbank
+    from cpp_projects_b200.pipeline import (SCHEDULE_FIELDS, BatchedSearch, BeamShape, SearchPipeline,
+                                            device_filterbank, tuned_schedule)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -354,14 +361,24 @@ def run_ours(args):
     beams = beams_for(args.workload, rank)
     shapes = [BeamShape(b.nchan, b.nsamp, b.fmin, b.fmax, b.max_dt) for b in beams]
     capacity = (1 << 26) if args.workload == "config2" else (1 << 24)
-    # both forms use the autotuned FDMT plans (fusion depth and head tile per shape)
+    schedules = None
+    if args.schedules:
+        schedules = json.loads(Path(args.schedules).read_text())["schedules"]
+        if len(schedules) != len(shapes):
+            raise SystemExit(f"{args.schedules}: {len(schedules)} schedules for {len(shapes)} beams")
+    # both forms use the same FDMT plans: autotuned per shape, or the given schedules
     pipe = SearchPipeline(shapes, widths_mode=SEARCH["widths_mode"], param=SEARCH["param"],
                           thr=SEARCH["thr"], metrics=SEARCH["metrics"], capacity=capacity,
-                          device=dev, fuse_depth=-2)
+                          device=dev, fuse_depth=-2, schedules=schedules)
+    if schedules is None:
+        schedules = [tuned_schedule(s) for s in shapes]
+    if args.save_schedules and rank == 0:
+        Path(args.save_schedules).write_text(json.dumps({"fields": list(SCHEDULE_FIELDS),
+                                                         "schedules": schedules}))
     # the batch holds every beam's candidates at once (config2: ~96M)
     batch = BatchedSearch(shapes, widths_mode=SEARCH["widths_mode"], param=SEARCH["param"],
                           thr=SEARCH["thr"], metrics=SEARCH["metrics"], capacity=capacity * 2,
-                          fuse_depth=-2, use_graph=True)
+                          use_graph=True, schedules=schedules)
     inputs = [device_filterbank(b.nchan, b.nsamp, b.fmin, b.fmax, b.seed, b.pulses, dev, gain=b.gain)
               for b in beams]
     torch.cuda.synchronize()

@@ -8,11 +8,16 @@
 // L/Clusterization/Clusterization.cu:17-54).  Here:
 //   stage 1 (graph)  for each beam: fused/plain FDMT into a shared DM-time
 //                    plane, row statistics, and the boxcar appending to one
-//                    device-wide candidate array with a shared atomic counter,
-//                    each candidate tagged with its beam — no host sync;
-//   stage 2          one read of the counter, one canonical sort over all
-//                    beams (beam, row, sample, width), one 3-pass clustering
-//                    whose initial groups are the beams, one delegate sort by
+//                    device-wide candidate array with a shared atomic counter
+//                    — no host sync.  Width sets with an ordered boxcar write
+//                    each tile's candidates as one block in canonical order
+//                    and record (first, count) per (beam, row, tile); others
+//                    tag every candidate with its beam;
+//   stage 2          one read of the counter, the canonical order over all
+//                    beams (beam, row, sample, width) — a scan of the record
+//                    counts and one move of every block, or a radix sort of
+//                    the tagged candidates —, one 3-pass clustering whose
+//                    initial groups are the beams, one delegate sort by
 //                    (beam, mt, group), one copy of the delegates to the host.
 // Plans are autotuned per shape and share one workspace; the DM-time plane
 // and statistics buffers are shared (the graph serialises the beams on one
@@ -34,6 +39,15 @@ bfs_status launch_boxcar(const float* d_plane, int rows, int cols, const float* 
 bfs_status sort_tagged_candidates(const bfs_cand* d_c, const int* d_tags, unsigned n, int max_rows,
                                   int max_cols, int max_tag, int mode, int param, bfs_cand* d_dst,
                                   int* d_tdst, cudaStream_t s);
+bool boxcar_ordered_supported(int mode, int param);
+long long boxcar_ordered_records(int rows, int cols);
+bfs_status launch_boxcar_ordered(const float* d_plane, int rows, int cols, const float* d_stats, float thr,
+                                 const float* d_thr, int mode, int param, int snr_fast, bfs_cand* d_out,
+                                 unsigned capacity, unsigned* d_count, unsigned* rec_first, unsigned* rec_count,
+                                 cudaStream_t s);
+bfs_status compact_ordered(const bfs_cand* src, const unsigned* rec_first, const unsigned* rec_count,
+                           long long nrec, const long long* beam_rec, int nb, bfs_cand* dst, int* tags,
+                           cudaStream_t s);
 }  // namespace bfs
 
 struct bfs_batch {
@@ -50,7 +64,13 @@ struct bfs_batch {
     float* plane = nullptr;
     float* stats = nullptr;
     bfs_cand* cands = nullptr;     // boxcar output (arrival order)
-    int* tags = nullptr;
+    int* tags = nullptr;           // (tagged-sort path) each candidate's beam
+    // ordered path: per-tile records of the boxcar's canonical blocks
+    bool ordered = false;
+    long long nrec = 0;
+    std::vector<long long> rec0;   // first record of each beam (+ the total)
+    unsigned* rec = nullptr;       // first[nrec], count[nrec]
+    long long* d_beam_rec = nullptr;
     bfs_cand* sorted = nullptr;    // canonical order
     int* sorted_tags = nullptr;
     unsigned* d_count = nullptr;
@@ -76,7 +96,8 @@ struct bfs_batch {
         for (cudaEvent_t e : events) cudaEventDestroy(e);
         for (auto* p : plans) bfs_fdmt_plan_destroy(p);
         for (void* p : {ws, static_cast<void*>(plane), static_cast<void*>(stats), static_cast<void*>(cands),
-                        static_cast<void*>(tags), static_cast<void*>(sorted), static_cast<void*>(sorted_tags),
+                        static_cast<void*>(tags), static_cast<void*>(rec), static_cast<void*>(d_beam_rec),
+                        static_cast<void*>(sorted), static_cast<void*>(sorted_tags),
                         static_cast<void*>(d_count), static_cast<void*>(perm), static_cast<void*>(offsets),
                         static_cast<void*>(delegates)})
             if (p) cudaFree(p);
@@ -177,12 +198,25 @@ extern "C" bfs_status bfs_batch_create(const bfs_batch_desc* desc, bfs_batch** o
         b->max_cols = std::max(b->max_cols, d.ncols);
     }
     BFS_ARG(b->max_rows <= 65535, "max_dt above 65535");
+    b->ordered = boxcar_ordered_supported(b->widths_mode, b->param);
+    if (b->ordered) {
+        for (const bfs_fdmt_desc& d : b->beams) {
+            b->rec0.push_back(b->nrec);
+            b->nrec += boxcar_ordered_records(d.max_dt, d.ncols);
+        }
+        b->rec0.push_back(b->nrec);
+        BFS_ARG(b->nrec < (1ll << 31), "too many boxcar tiles in the batch (%lld)", b->nrec);
+        BFS_CUDA(cudaMalloc(&b->rec, sizeof(unsigned) * 2 * b->nrec));
+        BFS_CUDA(cudaMalloc(&b->d_beam_rec, sizeof(long long) * b->rec0.size()));
+        BFS_CUDA(cudaMemcpy(b->d_beam_rec, b->rec0.data(), sizeof(long long) * b->rec0.size(),
+                            cudaMemcpyHostToDevice));
+    }
     BFS_CUDA(cudaMalloc(&b->ws, b->ws_bytes ? b->ws_bytes : 256));
     BFS_CUDA(cudaMalloc(&b->plane, plane * sizeof(float)));
     BFS_CUDA(cudaMalloc(&b->stats, 2 * static_cast<size_t>(b->max_rows) * sizeof(float)));
     const size_t cap = b->capacity;
     BFS_CUDA(cudaMalloc(&b->cands, cap * sizeof(bfs_cand)));
-    BFS_CUDA(cudaMalloc(&b->tags, cap * sizeof(int)));
+    if (!b->ordered) BFS_CUDA(cudaMalloc(&b->tags, cap * sizeof(int)));
     BFS_CUDA(cudaMalloc(&b->sorted, cap * sizeof(bfs_cand)));
     BFS_CUDA(cudaMalloc(&b->sorted_tags, cap * sizeof(int)));
     BFS_CUDA(cudaMalloc(&b->d_count, sizeof(unsigned)));
@@ -198,6 +232,18 @@ extern "C" bfs_status bfs_batch_destroy(bfs_batch* b) {
     return BFS_OK;
 }
 
+// Boxcar of beam i over the shared plane: ordered blocks + records, or
+// atomic appends tagged with the beam.
+static bfs_status beam_boxcar(bfs_batch* b, int i, cudaStream_t s) {
+    const bfs_fdmt_desc& d = b->beams[i];
+    if (b->ordered)
+        return launch_boxcar_ordered(b->plane, d.max_dt, d.ncols, b->stats, b->thr, nullptr, b->widths_mode,
+                                     b->param, 0, b->cands, b->capacity, b->d_count, b->rec + b->rec0[i],
+                                     b->rec + b->nrec + b->rec0[i], s);
+    return launch_boxcar(b->plane, d.max_dt, d.ncols, b->stats, b->thr, nullptr, b->widths_mode, b->param, 0,
+                         b->cands, b->capacity, b->d_count, s, i, b->tags);
+}
+
 // Stage 1 for every beam, enqueued on s (captured or eager).
 static bfs_status enqueue_stage1(bfs_batch* b, const float* const* d_inputs, cudaStream_t s) {
     BFS_CUDA(cudaMemsetAsync(b->d_count, 0, sizeof(unsigned), s));
@@ -207,9 +253,7 @@ static bfs_status enqueue_stage1(bfs_batch* b, const float* const* d_inputs, cud
         if (st != BFS_OK) return st;
         st = launch_row_stats(b->plane, d.max_dt, d.ncols, b->stats, 0, s);
         if (st != BFS_OK) return st;
-        st = launch_boxcar(b->plane, d.max_dt, d.ncols, b->stats, b->thr, nullptr, b->widths_mode,
-                           b->param, 0, b->cands, b->capacity, b->d_count, s, static_cast<int>(i),
-                           b->tags);
+        st = beam_boxcar(b, static_cast<int>(i), s);
         if (st != BFS_OK) return st;
     }
     return BFS_OK;
@@ -274,8 +318,7 @@ static bfs_status enqueue_host_stage1(bfs_batch* b, const float* const* h_inputs
         if (st != BFS_OK) return st;
         st = launch_row_stats(b->plane, d.max_dt, d.ncols, b->stats, 0, cs);
         if (st != BFS_OK) return st;
-        st = launch_boxcar(b->plane, d.max_dt, d.ncols, b->stats, b->thr, nullptr, b->widths_mode,
-                           b->param, 0, b->cands, b->capacity, b->d_count, cs, i, b->tags);
+        st = beam_boxcar(b, i, cs);
         if (st != BFS_OK) return st;
     }
     // the copy stream joins the compute stream (required to end a capture)
@@ -351,8 +394,12 @@ static bfs_status batch_stage2(bfs_batch* b, void* stream) {
     b->h_beam_first.assign(nb, 0); b->h_beam_count.assign(nb, 0); b->h_beam_cands.assign(nb, 0);
     b->n_groups = 0;
     if (count == 0) return BFS_OK;
-    bfs_status st = sort_tagged_candidates(b->cands, b->tags, count, b->max_rows, b->max_cols, nb - 1,
-                                           b->widths_mode, b->param, b->sorted, b->sorted_tags, s);
+    // canonical order (beam, row, sample, width)
+    bfs_status st = b->ordered
+        ? compact_ordered(b->cands, b->rec, b->rec + b->nrec, b->nrec, b->d_beam_rec, nb, b->sorted,
+                          b->sorted_tags, s)
+        : sort_tagged_candidates(b->cands, b->tags, count, b->max_rows, b->max_cols, nb - 1, b->widths_mode,
+                                 b->param, b->sorted, b->sorted_tags, s);
     if (st != BFS_OK) return st;
     uint32_t ng = 0;
     st = bfs_cluster_grouped(b->sorted, count, b->sorted_tags, static_cast<uint32_t>(nb), b->metrics,

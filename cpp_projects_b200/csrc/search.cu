@@ -19,6 +19,7 @@
 // so the list is then sorted by the canonical key (mdt, mt, width) — the
 // reference's heap order — with a stable device radix sort.
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <cmath>
 
@@ -307,6 +308,291 @@ k_boxcar_reg(const float* __restrict__ plane, int rows, int cols, const float* _
                                          d_count, tag, tags);
 }
 
+// ---- ordered boxcar over row pairs -------------------------------------------
+// The register-blocked boxcar for two rows at once, writing the candidates
+// of every warp's tile as one block in canonical order.  Each warp owns
+// kPairWarpTile consecutive starts of rows 2y and 2y + 1 and stages them
+// (with the WMAX - 1 samples after them) interleaved in its own shared
+// region: position p holds {row 2y, row 2y + 1} at sample tw + p, so one
+// packed add.rn.f32x2 advances the running sums of both rows at one start —
+// each half is rounded as one __fadd_rn, so the sums are the reference's
+// sequential sums bit for bit.  Per width the warp first asks whether any
+// of its sums exceeds the width's lower bound of passing sums (a
+// three-input max tree and one vote); only then are exact quotients
+// evaluated.  Pass 1 keeps the passing windows as bits (start j, width code
+// c) -> bit 8 j + c, which orders them by (start, width); a warp scan of the
+// lanes' counts and one atomicAdd give the warp its block (row 2y's
+// candidates, then row 2y + 1's).  Warps with candidates then run the width
+// loop again (pass 2, the same packed adds) and write each passing window
+// at its position in the block.  The warps never wait for one another.
+// Record (row, warp tile i) = {first index, count} of row `row`'s block in
+// warp tile i (index row * ceil(cols / kPairWarpTile) + i), so a scan of
+// the counts in record order gives every candidate its canonical position
+// (compact_ordered).
+constexpr int kPairStarts = 8;                            // starts per lane
+constexpr int kPairWarpTile = 32 * kPairStarts;           // starts per warp
+constexpr int kPairWarps = 4;
+constexpr int kPairThreads = 32 * kPairWarps;
+constexpr int kPairTile = kPairWarps * kPairWarpTile;     // starts per CTA
+
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+    unsigned long long d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+    return d;
+}
+__device__ __forceinline__ void unpack2(unsigned long long v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+// both halves rounded to nearest, each exactly as __fadd_rn
+__device__ __forceinline__ unsigned long long add2_rn(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+// The width loop of one lane: kPairStarts starts from tb in both rows (win4
+// = the lane's first staged pair of positions).  pass[r] gets bit 8 j + c
+// for every passing window (start j, width code c) of row r, and snr[64 r +
+// 8 j + c] its S/N.  edge: some window may leave the row (tested per window).
+template <int MODE, int WMAX>
+__device__ __forceinline__ void pair_widths(const float4* __restrict__ win4, int tb, int cols, bool edge,
+                                            float thr, float thr_lo, int snr_fast, const WidthConsts& wc,
+                                            unsigned long long (&pass)[2], float (&snr)[128]) {
+    constexpr int S = kPairStarts;
+    constexpr int kPos = S + WMAX - 1;   // positions this lane reads
+    constexpr int kVec = (kPos + 1) / 2; // float4s (two positions each)
+    unsigned long long win[2 * kVec];
+    unsigned long long sum[S];
+#pragma unroll
+    for (int v = 0; v < S / 2; ++v) {
+        const float4 q = win4[v];
+        win[2 * v] = pack2(q.x, q.y);
+        win[2 * v + 1] = pack2(q.z, q.w);
+    }
+#pragma unroll
+    for (int j = 0; j < S; ++j) sum[j] = 0ull;   // +0.0 in both halves
+#pragma unroll
+    for (int w = 1; w <= WMAX; ++w) {
+        // step w reads positions w - 1 .. w + S - 2: fetch the pair that
+        // starts at position w + S - 2 when the step first reaches it
+        constexpr int kFirst = S / 2;
+        if (((w + S - 2) & 1) == 0 && (w + S - 2) / 2 >= kFirst && (w + S - 2) / 2 < kVec) {
+            const float4 q = win4[(w + S - 2) / 2];
+            win[w + S - 2] = pack2(q.x, q.y);
+            win[w + S - 1] = pack2(q.z, q.w);
+        }
+#pragma unroll
+        for (int j = 0; j < S; ++j) sum[j] = add2_rn(sum[j], win[j + w - 1]);
+        if (MODE == 0 && (w & (w - 1)) != 0) continue;
+        const float sq = wc.sq[w];
+        // RN(sum / sq) > thr needs sum > RN(RN(thr sq) (1 - 1e-5)) for thr > 0
+        const float lim = thr_lo > -INFINITY ? __fmul_rn(__fmul_rn(thr, sq), 0.99999f) : -INFINITY;
+        float h[2 * S];
+#pragma unroll
+        for (int j = 0; j < S; ++j) unpack2(sum[j], h[2 * j], h[2 * j + 1]);
+        float mx = max3f(h[0], h[1], h[2]);
+#pragma unroll
+        for (int k = 3; k + 1 < 2 * S; k += 2) mx = max3f(mx, h[k], h[k + 1]);
+        mx = fmaxf(mx, h[2 * S - 1]);
+        if (!__any_sync(0xffffffffu, mx > lim)) continue;
+        const int code = (MODE == 1) ? w - 1 : 31 - __clz(w);
+        // windows inside the row: starts j < inside
+        const int inside = edge ? cols - (tb + w - 1) : S;
+#pragma unroll
+        for (int j = 0; j < S; ++j) {
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                const float sj = h[2 * j + r];
+                if (sj > lim && j < inside) {
+                    const float q = snr_fast ? __fdividef(sj, sq) : __fdiv_rn(sj, sq);
+                    if (q > thr) {
+                        pass[r] |= 1ull << (8 * j + code);
+                        snr[64 * r + 8 * j + code] = q;
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <int MODE, int WMAX>
+__global__ void __launch_bounds__(kPairThreads, WMAX <= 8 ? 8 : WMAX <= 32 ? 6 : WMAX <= 64 ? 4 : 2)
+k_boxcar_pair(const float* __restrict__ plane, int rows, int cols, const float* __restrict__ stats,
+              const float* __restrict__ d_thr, float thr_host, float thr_lo_host, int snr_fast, int vec,
+              bfs_cand* __restrict__ out, unsigned capacity, unsigned* __restrict__ d_count,
+              unsigned* __restrict__ rec_first, unsigned* __restrict__ rec_count, const WidthConsts wc) {
+    // staged positions of a warp: every start's windows, a multiple of 4
+    constexpr int kSpan = (kPairWarpTile + WMAX - 1 + 3) / 4 * 4;
+    __shared__ float4 tile4[kPairWarps][kSpan / 2];   // kSpan positions x {row 0, row 1}
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wt = blockIdx.x * kPairWarps + warp;     // warp tile
+    const int tw = wt * kPairWarpTile;
+    if (tw >= cols) return;                            // warp-uniform; no other warp is waited for
+    const int row0 = 2 * static_cast<int>(blockIdx.y);
+    const bool has1 = row0 + 1 < rows;
+    const float* x0 = plane + static_cast<size_t>(row0) * cols;
+    const float* x1 = has1 ? x0 + cols : x0;
+    float m0 = 0.0f, s0 = 1.0f, m1 = 0.0f, s1 = 1.0f;
+    if (stats) {
+        m0 = stats[row0]; s0 = stats[rows + row0];
+        if (has1) { m1 = stats[row0 + 1]; s1 = stats[rows + row0 + 1]; }
+    }
+    auto nz = [&](float v, float m, float s) { return stats ? norm_sample(v, m, s) : v; };
+    float4* t4 = tile4[warp];
+    float* tile = reinterpret_cast<float*>(t4);        // position p, row r at 2 p + r
+    const bool interior = tw + kSpan <= cols;
+    if (interior && vec) {
+        // 16-byte loads of both rows, every load in flight before the first use
+        constexpr int kQ = kSpan / 4;                   // float4s per row
+        constexpr int kPer = (kQ + 31) / 32;
+        float4 a[kPer], b[kPer];
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            const int q = lane + 32 * k;
+            if (k < kPer - 1 || q < kQ) {
+                a[k] = __ldg(reinterpret_cast<const float4*>(x0 + tw) + q);
+                b[k] = has1 ? __ldg(reinterpret_cast<const float4*>(x1 + tw) + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            const int q = lane + 32 * k;
+            if (k < kPer - 1 || q < kQ) {
+                const float b0 = has1 ? nz(b[k].x, m1, s1) : 0.0f, b1 = has1 ? nz(b[k].y, m1, s1) : 0.0f;
+                const float b2 = has1 ? nz(b[k].z, m1, s1) : 0.0f, b3 = has1 ? nz(b[k].w, m1, s1) : 0.0f;
+                t4[2 * q] = make_float4(nz(a[k].x, m0, s0), b0, nz(a[k].y, m0, s0), b1);
+                t4[2 * q + 1] = make_float4(nz(a[k].z, m0, s0), b2, nz(a[k].w, m0, s0), b3);
+            }
+        }
+    } else if (interior) {
+        // 4-byte loads (rows not 16-byte aligned), all in flight first
+        constexpr int kPer = (kSpan + 31) / 32;
+        float a[kPer], b[kPer];
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            const int p = lane + 32 * k;
+            if (k < kPer - 1 || p < kSpan) {
+                a[k] = __ldg(x0 + tw + p);
+                b[k] = has1 ? __ldg(x1 + tw + p) : 0.0f;
+            }
+        }
+        float2* t2 = reinterpret_cast<float2*>(t4);
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            const int p = lane + 32 * k;
+            if (k < kPer - 1 || p < kSpan) t2[p] = make_float2(nz(a[k], m0, s0), has1 ? nz(b[k], m1, s1) : 0.0f);
+        }
+    } else {
+        for (int p = lane; p < kSpan; p += 32) {
+            const int t = tw + p;
+            const bool in = t < cols;
+            tile[2 * p] = in ? nz(__ldg(x0 + t), m0, s0) : 0.0f;
+            tile[2 * p + 1] = (in && has1) ? nz(__ldg(x1 + t), m1, s1) : 0.0f;
+        }
+    }
+    __syncwarp();
+    float thr = thr_host, thr_lo = thr_lo_host;
+    if (d_thr) {
+        thr = __ldg(d_thr);
+        thr_lo = thr > 0.0f ? thr * 0.99999f : -INFINITY;
+    }
+    const int p0 = lane * kPairStarts;
+    const int tb = tw + p0;
+    const float4* win4 = t4 + p0 / 2;
+    unsigned long long pass[2] = {0ull, 0ull};
+    float snr[128];   // S/N of the passing windows (indexed like their bits)
+    pair_widths<MODE, WMAX>(win4, tb, cols, !interior, thr, thr_lo, snr_fast, wc, pass, snr);
+    if (!has1) pass[1] = 0ull;
+
+    // the warp's block: row 0's candidates, then row 1's, lanes in order
+    const unsigned c0 = __popcll(pass[0]), c1 = __popcll(pass[1]);
+    unsigned i0 = c0, i1 = c1;   // inclusive scans over the lanes
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const unsigned u0 = __shfl_up_sync(0xffffffffu, i0, d), u1 = __shfl_up_sync(0xffffffffu, i1, d);
+        if (lane >= d) { i0 += u0; i1 += u1; }
+    }
+    const unsigned tot0 = __shfl_sync(0xffffffffu, i0, 31), tot1 = __shfl_sync(0xffffffffu, i1, 31);
+    unsigned first = 0;
+    if (lane == 0) {
+        first = (tot0 + tot1) ? atomicAdd(d_count, tot0 + tot1) : 0u;
+        const int nwt = (cols + kPairWarpTile - 1) / kPairWarpTile;
+        const size_t rec = static_cast<size_t>(row0) * nwt + wt;
+        rec_first[rec] = first;
+        rec_count[rec] = tot0;
+        if (has1) {
+            rec_first[rec + nwt] = first + tot0;
+            rec_count[rec + nwt] = tot1;
+        }
+    }
+    if (tot0 + tot1 == 0) return;   // warp-uniform
+    first = __shfl_sync(0xffffffffu, first, 0);
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        unsigned idx = first + (r ? tot0 + i1 - c1 : i0 - c0);
+        unsigned long long m = pass[r];
+        while (m) {   // bit order = (start, width) order
+            const int bit = __ffsll(static_cast<long long>(m)) - 1;
+            m &= m - 1;
+            if (idx < capacity) {
+                const int code = bit & 7;
+                bfs_cand c;
+                c.mt = tb + (bit >> 3); c.mdt = row0 + r; c.mwidth = MODE == 1 ? code + 1 : code;
+                c.msnr = snr[64 * r + bit];
+                out[idx] = c;
+            }
+            ++idx;
+        }
+    }
+}
+
+// Candidates of records [0, nrec) moved to their canonical positions
+// (pos = exclusive scan of the counts); tags[pos..] = the record's beam when
+// tags is given (beam b owns records [beam_rec[b], beam_rec[b + 1])).  A warp
+// takes 32 consecutive records and copies each non-empty one with all lanes.
+__global__ void k_compact_records(const bfs_cand* __restrict__ src, const unsigned* __restrict__ rec_first,
+                                  const unsigned* __restrict__ rec_count, const unsigned* __restrict__ rec_pos,
+                                  long long nrec, const long long* __restrict__ beam_rec, int nb,
+                                  bfs_cand* __restrict__ dst, int* __restrict__ tags) {
+    const long long r = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    unsigned n = 0, from = 0, to = 0;
+    int beam = 0;
+    if (r < nrec) {
+        n = rec_count[r];
+        if (n) {
+            from = rec_first[r];
+            to = rec_pos[r];
+            if (tags) {   // last beam whose first record is <= r
+                int lo = 0, hi = nb - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (beam_rec[mid] <= r) lo = mid; else hi = mid - 1;
+                }
+                beam = lo;
+            }
+        }
+    }
+    unsigned todo = __ballot_sync(0xffffffffu, n != 0);
+    while (todo) {
+        const int src_lane = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const unsigned cn = __shfl_sync(0xffffffffu, n, src_lane);
+        const unsigned cf = __shfl_sync(0xffffffffu, from, src_lane);
+        const unsigned ct = __shfl_sync(0xffffffffu, to, src_lane);
+        const int cb = __shfl_sync(0xffffffffu, beam, src_lane);
+        for (unsigned i = lane; i < cn; i += 32) {
+            dst[ct + i] = src[cf + i];
+            if (tags) tags[ct + i] = cb;
+        }
+    }
+}
+
 // Canonical key of a candidate: (row * cols + start) << wbits | width code,
 // with the width code 0..Q (pow2 mode) or w-1 (all-widths mode).
 __device__ __forceinline__ unsigned long long cand_key(const bfs_cand& v, int cols, int mode, int wbits) {
@@ -562,6 +848,101 @@ bfs_status launch_boxcar(const float* d_plane, int rows, int cols, const float* 
     return BFS_OK;
 }
 
+// Whether launch_boxcar_ordered handles a width set (pow2 up to 128 or every
+// width up to 8: at most 8 width codes per start).
+bool boxcar_ordered_supported(int mode, int param) {
+    if (mode == BFS_WIDTHS_POW2) return param >= 0 && param <= 7;
+    if (mode == BFS_WIDTHS_ALL) return param >= 1 && param <= 8;
+    return false;
+}
+
+long long boxcar_ordered_records(int rows, int cols) {
+    return static_cast<long long>(rows) * ((cols + kPairWarpTile - 1) / kPairWarpTile);
+}
+
+// The boxcar with canonical per-tile output (k_boxcar_pair): candidates go to
+// d_out in blocks, one per (row, warp tile), each in canonical order; records
+// rec_first / rec_count (boxcar_ordered_records entries, (row, tile) order)
+// locate the blocks for compact_ordered.
+bfs_status launch_boxcar_ordered(const float* d_plane, int rows, int cols, const float* d_stats, float thr,
+                                 const float* d_thr, int mode, int param, int snr_fast, bfs_cand* d_out,
+                                 unsigned capacity, unsigned* d_count, unsigned* rec_first, unsigned* rec_count,
+                                 cudaStream_t s) {
+    BFS_ARG(d_plane && d_count && rec_first && rec_count, "null argument");
+    BFS_ARG(rows >= 1 && cols >= 1, "bad shape %dx%d", rows, cols);
+    BFS_ARG((rows + 1) / 2 <= 65535, "rows > 131070 not supported");
+    BFS_ARG(capacity == 0 || d_out, "d_out is null");
+    BFS_ARG(boxcar_ordered_supported(mode, param), "width set (%d, %d) has no ordered kernel", mode, param);
+    const float thr_lo = thr > 0.0f ? thr * 0.99999f : -INFINITY;
+    const int vec = (cols % 4 == 0) && (reinterpret_cast<uintptr_t>(d_plane) % 16 == 0);
+    WidthConsts wc;
+    for (int w = 0; w <= kRegMaxW; ++w) wc.sq[w] = std::sqrt(static_cast<float>(w));  // IEEE-correct on the host
+    const dim3 grid((cols + kPairTile - 1) / kPairTile, (rows + 1) / 2);
+#define BFS_BOX_PAIR(M, W) k_boxcar_pair<M, W><<<grid, kPairThreads, 0, s>>>(                               \
+        d_plane, rows, cols, d_stats, d_thr, thr, thr_lo, snr_fast, vec, d_out, capacity, d_count, rec_first, \
+        rec_count, wc)
+    if (mode == BFS_WIDTHS_POW2) {
+        switch (param) {
+            case 0: BFS_BOX_PAIR(0, 1); break;
+            case 1: BFS_BOX_PAIR(0, 2); break;
+            case 2: BFS_BOX_PAIR(0, 4); break;
+            case 3: BFS_BOX_PAIR(0, 8); break;
+            case 4: BFS_BOX_PAIR(0, 16); break;
+            case 5: BFS_BOX_PAIR(0, 32); break;
+            case 6: BFS_BOX_PAIR(0, 64); break;
+            default: BFS_BOX_PAIR(0, 128); break;
+        }
+    } else {
+        switch (param) {
+            case 1: BFS_BOX_PAIR(1, 1); break;
+            case 2: BFS_BOX_PAIR(1, 2); break;
+            case 3: BFS_BOX_PAIR(1, 3); break;
+            case 4: BFS_BOX_PAIR(1, 4); break;
+            case 5: BFS_BOX_PAIR(1, 5); break;
+            case 6: BFS_BOX_PAIR(1, 6); break;
+            case 7: BFS_BOX_PAIR(1, 7); break;
+            default: BFS_BOX_PAIR(1, 8); break;
+        }
+    }
+#undef BFS_BOX_PAIR
+    BFS_LAUNCH_CHECK("k_boxcar_pair");
+    return BFS_OK;
+}
+
+// The candidates of nrec records (blocks in src written by
+// launch_boxcar_ordered, every count summing to at most the capacity src was
+// written with) in canonical order in dst; tags (optional) = each candidate's
+// beam, beam b owning records [beam_rec[b], beam_rec[b + 1]) (beam_rec on the
+// device, nb + 1 entries).  Scratch from the stream-ordered pool.
+bfs_status compact_ordered(const bfs_cand* src, const unsigned* rec_first, const unsigned* rec_count,
+                           long long nrec, const long long* beam_rec, int nb, bfs_cand* dst, int* tags,
+                           cudaStream_t s) {
+    if (nrec <= 0) return BFS_OK;
+    BFS_ARG(nrec < (1ll << 31), "too many boxcar tiles (%lld)", nrec);
+    BFS_ARG(!tags || (beam_rec && nb >= 1), "tags need the beams' record offsets");
+    const int th = 256;
+    const long long blocks = (nrec + th - 1) / th;
+    BFS_ARG(blocks < (1ll << 31), "too many boxcar tiles (%lld)", nrec);
+    unsigned* pos = nullptr;
+    void* tmp = nullptr;
+    size_t tmp_bytes = 0;
+    BFS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, rec_count, pos, static_cast<int>(nrec), s));
+    bfs_status st = stream_alloc(reinterpret_cast<void**>(&pos), sizeof(unsigned) * nrec, s);
+    if (st == BFS_OK) st = stream_alloc(&tmp, tmp_bytes ? tmp_bytes : 16, s);
+    if (st == BFS_OK) {
+        cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, rec_count, pos, static_cast<int>(nrec), s);
+        if (e == cudaSuccess) {
+            k_compact_records<<<static_cast<unsigned>(blocks), th, 0, s>>>(src, rec_first, rec_count, pos, nrec,
+                                                                            beam_rec, nb, dst, tags);
+            e = cudaGetLastError();
+        }
+        if (e != cudaSuccess) st = fail(BFS_ERR_CUDA, "candidate compaction: %s", cudaGetErrorString(e));
+    }
+    if (pos) cudaFreeAsync(pos, s);
+    if (tmp) cudaFreeAsync(tmp, s);
+    return st;
+}
+
 }  // namespace bfs
 
 using namespace bfs;
@@ -594,12 +975,27 @@ extern "C" bfs_status bfs_boxcar_gather(const float* d_plane, int rows, int cols
                                         int widths_mode, int param, int snr_fast, bfs_cand* d_out,
                                         uint32_t capacity, uint32_t* h_count, void* stream) {
     BFS_ARG(h_count != nullptr, "h_count is null");
+    BFS_ARG(d_plane != nullptr, "null argument");
+    BFS_ARG(rows >= 1 && cols >= 1 && rows <= 65535, "bad shape %dx%d", rows, cols);
     cudaStream_t s = as_stream(stream);
+    // width sets with an ordered kernel: candidates come out in per-tile
+    // canonical blocks, then one scan + move puts them in canonical order;
+    // others: atomic appends, then a radix sort by the canonical key
+    const bool ordered = boxcar_ordered_supported(widths_mode, param);
+    const long long nrec = ordered ? boxcar_ordered_records(rows, cols) : 0;
     unsigned* d_count = nullptr;
+    unsigned* rec = nullptr;   // first[nrec], count[nrec]
     BFS_TRY_ST(stream_alloc(reinterpret_cast<void**>(&d_count), sizeof(unsigned), s));
-    BFS_CUDA(cudaMemsetAsync(d_count, 0, sizeof(unsigned), s));
-    bfs_status st = launch_boxcar(d_plane, rows, cols, d_stats, thr, d_thr, widths_mode, param,
-                                  snr_fast, d_out, capacity, d_count, s, 0, nullptr);
+    bfs_status st = ordered ? stream_alloc(reinterpret_cast<void**>(&rec), sizeof(unsigned) * 2 * nrec, s) : BFS_OK;
+    if (st == BFS_OK) {
+        cudaError_t e = cudaMemsetAsync(d_count, 0, sizeof(unsigned), s);
+        if (e != cudaSuccess) st = fail(BFS_ERR_CUDA, "cudaMemsetAsync: %s", cudaGetErrorString(e));
+    }
+    if (st == BFS_OK)
+        st = ordered ? launch_boxcar_ordered(d_plane, rows, cols, d_stats, thr, d_thr, widths_mode, param, snr_fast,
+                                             d_out, capacity, d_count, rec, rec + nrec, s)
+                     : launch_boxcar(d_plane, rows, cols, d_stats, thr, d_thr, widths_mode, param,
+                                     snr_fast, d_out, capacity, d_count, s, 0, nullptr);
     unsigned count = 0;
     if (st == BFS_OK) {
         cudaError_t e = cudaMemcpyAsync(&count, d_count, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
@@ -608,10 +1004,24 @@ extern "C" bfs_status bfs_boxcar_gather(const float* d_plane, int rows, int cols
                                         cudaGetErrorString(e));
     }
     cudaFreeAsync(d_count, s);
-    if (st != BFS_OK) return st;
-    *h_count = count;
-    const unsigned n = count < capacity ? count : capacity;
-    st = sort_candidates_canonical(d_out, n, rows, cols, widths_mode, param, s);
+    if (st == BFS_OK) {
+        *h_count = count;
+        const unsigned n = count < capacity ? count : capacity;
+        if (ordered && count <= capacity && count >= 2) {
+            bfs_cand* tmp = nullptr;
+            st = stream_alloc(reinterpret_cast<void**>(&tmp), sizeof(bfs_cand) * count, s);
+            if (st == BFS_OK) st = compact_ordered(d_out, rec, rec + nrec, nrec, nullptr, 0, tmp, nullptr, s);
+            if (st == BFS_OK) {
+                cudaError_t e = cudaMemcpyAsync(d_out, tmp, sizeof(bfs_cand) * count, cudaMemcpyDeviceToDevice, s);
+                if (e != cudaSuccess) st = fail(BFS_ERR_CUDA, "cudaMemcpyAsync: %s", cudaGetErrorString(e));
+            }
+            if (tmp) cudaFreeAsync(tmp, s);
+        } else if (!ordered || count > capacity) {
+            // (ordered overflow: the blocks that fit, sorted)
+            st = sort_candidates_canonical(d_out, n, rows, cols, widths_mode, param, s);
+        }
+    }
+    if (rec) cudaFreeAsync(rec, s);
     if (st != BFS_OK) return st;
     if (count > capacity)
         return fail(BFS_ERR_OVERFLOW, "%u candidates found, capacity %u", count, capacity);

@@ -28,6 +28,28 @@ def fdmt_launches(plan: CFdmtGpu) -> int:
     return 1 + plan.info.hbm_passes
 
 
+# An FDMT schedule: (fuse_depth, head_tile, seg_levels, seg_rows, seg_threads,
+# seg_flags), the fields of bfs_fdmt_desc that fix the kernels a plan runs.
+SCHEDULE_FIELDS = ("fuse_depth", "head_tile", "seg_levels", "seg_rows", "seg_threads", "seg_flags")
+
+
+def tuned_schedule(shape: "BeamShape") -> tuple:
+    """The autotuner's schedule for `shape` on the current device (its cached
+    choice once a plan of that shape was created with fuse_depth -2)."""
+    from . import _capi
+    from .fdmt import autotune_desc
+    d = _capi.FdmtDesc(fmin=shape.fmin, fmax=shape.fmax, nchan=shape.nchan, ncols=shape.nsamp,
+                       max_dt=shape.max_dt, fuse_depth=_capi.BFS_FUSE_AUTOTUNE)
+    t, _ = autotune_desc(d)
+    return tuple(int(getattr(t, f)) for f in SCHEDULE_FIELDS)
+
+
+def _schedule_kwargs(schedules, i: int, fuse_depth: int) -> dict:
+    if schedules is None:
+        return {"fuse_depth": fuse_depth}
+    return dict(zip(SCHEDULE_FIELDS, (int(v) for v in schedules[i])))
+
+
 @dataclass
 class BeamShape:
     nchan: int
@@ -47,13 +69,19 @@ class BeamResult:
 class SearchPipeline:
     def __init__(self, shapes: list[BeamShape], widths_mode: int = 0, param: int = 5,
                  thr: float = 7.0, metrics=(16, 8, 1 << 30), capacity: int = 1 << 26,
-                 device: torch.device | str = "cuda:0", fuse_depth: int = -1, precision: int = 0):
+                 device: torch.device | str = "cuda:0", fuse_depth: int = -1, precision: int = 0,
+                 schedules: list | None = None):
+        """`schedules`: one SCHEDULE_FIELDS tuple per beam, used instead of
+        `fuse_depth` (e.g. the schedules an earlier run's autotuner chose)."""
         self.device = torch.device(device)
         self.shapes = list(shapes)
+        if schedules is not None and len(schedules) != len(self.shapes):
+            raise ValueError("one schedule per beam")
         self.widths_mode, self.param, self.thr = widths_mode, param, float(thr)
         self.metrics = tuple(int(m) for m in metrics)
-        self.plans = [CFdmtGpu(s.fmin, s.fmax, s.nchan, s.nsamp, s.max_dt, fuse_depth=fuse_depth,
-                               external_ws=True, precision=precision) for s in self.shapes]
+        self.plans = [CFdmtGpu(s.fmin, s.fmax, s.nchan, s.nsamp, s.max_dt, external_ws=True, precision=precision,
+                               **_schedule_kwargs(schedules, i, fuse_depth))
+                      for i, s in enumerate(self.shapes)]
         ws = max(p.workspace_size() for p in self.plans)
         self.workspace = torch.empty(ws, dtype=torch.uint8, device=self.device)
         plane = max(s.max_dt * s.nsamp for s in self.shapes)
@@ -118,15 +146,20 @@ class BatchedSearch:
 
     def __init__(self, shapes: list[BeamShape], widths_mode: int = 0, param: int = 5,
                  thr: float = 7.0, metrics=(16, 8, 1 << 30), capacity: int = 1 << 26,
-                 fuse_depth: int = -2, use_graph: bool = True, precision: int = 0):
+                 fuse_depth: int = -2, use_graph: bool = True, precision: int = 0,
+                 schedules: list | None = None):
+        """`schedules`: as for SearchPipeline."""
         import ctypes
         from . import _capi
         self._capi = _capi
         self.shapes = list(shapes)
+        if schedules is not None and len(schedules) != len(self.shapes):
+            raise ValueError("one schedule per beam")
         descs = (_capi.FdmtDesc * len(shapes))()
-        for d, sh in zip(descs, shapes):
+        for i, (d, sh) in enumerate(zip(descs, shapes)):
             d.fmin, d.fmax, d.nchan, d.ncols, d.max_dt = sh.fmin, sh.fmax, sh.nchan, sh.nsamp, sh.max_dt
-            d.fuse_depth = fuse_depth
+            for f, v in _schedule_kwargs(schedules, i, fuse_depth).items():
+                setattr(d, f, v)
             d.precision = precision
         bd = _capi.BatchDesc(nbeams=len(shapes), beams=descs, widths_mode=widths_mode, param=param,
                              thr=thr, capacity=capacity, use_graph=1 if use_graph else 0)

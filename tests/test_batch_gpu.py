@@ -55,3 +55,24 @@ def test_host_input_form_equals_device_form(cuda):
             assert np.array_equal(g.group_sizes, w.group_sizes)
     assert all(torch.equal(d, x) for d, x in zip(dev, inputs))
 
+
+
+def test_explicit_schedules_equal_autotuned(cuda):
+    """Plans built from saved schedules (what a profiled run replays) run the
+    autotuner's kernels: same passes, same results."""
+    from cpp_projects_b200.pipeline import tuned_schedule
+    beams = _beams()[:3]
+    shapes = [BeamShape(b.nchan, b.nsamp, b.fmin, b.fmax, b.max_dt) for b in beams]
+    inputs = [device_filterbank(b.nchan, b.nsamp, b.fmin, b.fmax, b.seed, b.pulses, cuda) for b in beams]
+    auto = SearchPipeline(shapes, thr=6.0, capacity=1 << 22, device=cuda, fuse_depth=-2)
+    scheds = [tuned_schedule(s) for s in shapes]
+    fixed = SearchPipeline(shapes, thr=6.0, capacity=1 << 22, device=cuda, schedules=scheds)
+    for a, f in zip(auto.plans, fixed.plans):
+        assert a.passes() == f.passes() and a.info.fuse_depth == f.info.fuse_depth
+    want = auto.run(inputs)
+    got = BatchedSearch(shapes, thr=6.0, capacity=1 << 22, schedules=scheds).run(inputs)
+    for w, g in zip(want, got):
+        assert g.n_candidates == w.n_candidates
+        assert np.array_equal(g.delegates.view(np.uint32).reshape(-1), w.delegates.view(np.uint32).reshape(-1))
+    with pytest.raises(ValueError):
+        SearchPipeline(shapes, device=cuda, schedules=scheds[:1])
