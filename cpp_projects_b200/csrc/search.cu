@@ -355,22 +355,30 @@ __device__ __forceinline__ float max3f(float a, float b, float c) {
     return d;
 }
 
+// Shared layout of a warp's staged tile: logical float4 f (positions 2f,
+// 2f + 1 of both rows) sits at f + f / 4, one float4 of padding after every
+// four, so the eight lanes of a quarter warp — whose windows start 4 float4s
+// apart — read eight different bank groups.
+__device__ __forceinline__ int pad4(int f) { return f + (f >> 2); }
+
 // The width loop of one lane: kPairStarts starts from tb in both rows (win4
-// = the lane's first staged pair of positions).  pass[r] gets bit 8 j + c
+// = the warp's staged tile, f0 = the lane's first logical float4).  pass[r] gets bit 8 j + c
 // for every passing window (start j, width code c) of row r, and snr[64 r +
 // 8 j + c] its S/N.  edge: some window may leave the row (tested per window).
 template <int MODE, int WMAX>
-__device__ __forceinline__ void pair_widths(const float4* __restrict__ win4, int tb, int cols, bool edge,
+__device__ __forceinline__ void pair_widths(const float4* __restrict__ win4, int f0, int tb, int cols, bool edge,
                                             float thr, float thr_lo, int snr_fast, const WidthConsts& wc,
                                             unsigned long long (&pass)[2], float (&snr)[128]) {
     constexpr int S = kPairStarts;
     constexpr int kPos = S + WMAX - 1;   // positions this lane reads
     constexpr int kVec = (kPos + 1) / 2; // float4s (two positions each)
+    constexpr int kAhead = 4;            // window pairs are read this many steps before use
     unsigned long long win[2 * kVec];
     unsigned long long sum[S];
+    constexpr int kPre = (S + kAhead + 1) / 2 < kVec ? (S + kAhead + 1) / 2 : kVec;
 #pragma unroll
-    for (int v = 0; v < S / 2; ++v) {
-        const float4 q = win4[v];
+    for (int v = 0; v < kPre; ++v) {
+        const float4 q = win4[pad4(f0 + v)];
         win[2 * v] = pack2(q.x, q.y);
         win[2 * v + 1] = pack2(q.z, q.w);
     }
@@ -378,13 +386,13 @@ __device__ __forceinline__ void pair_widths(const float4* __restrict__ win4, int
     for (int j = 0; j < S; ++j) sum[j] = 0ull;   // +0.0 in both halves
 #pragma unroll
     for (int w = 1; w <= WMAX; ++w) {
-        // step w reads positions w - 1 .. w + S - 2: fetch the pair that
-        // starts at position w + S - 2 when the step first reaches it
-        constexpr int kFirst = S / 2;
-        if (((w + S - 2) & 1) == 0 && (w + S - 2) / 2 >= kFirst && (w + S - 2) / 2 < kVec) {
-            const float4 q = win4[(w + S - 2) / 2];
-            win[w + S - 2] = pack2(q.x, q.y);
-            win[w + S - 1] = pack2(q.z, q.w);
+        // step w reads positions w - 1 .. w + S - 2; the pair starting at
+        // position w + S - 2 + kAhead is fetched now, kAhead steps early
+        const int pn = w + S - 2 + kAhead;
+        if ((pn & 1) == 0 && pn / 2 >= kPre && pn / 2 < kVec) {
+            const float4 q = win4[pad4(f0 + pn / 2)];
+            win[pn] = pack2(q.x, q.y);
+            win[pn + 1] = pack2(q.z, q.w);
         }
 #pragma unroll
         for (int j = 0; j < S; ++j) sum[j] = add2_rn(sum[j], win[j + w - 1]);
@@ -392,23 +400,27 @@ __device__ __forceinline__ void pair_widths(const float4* __restrict__ win4, int
         const float sq = wc.sq[w];
         // RN(sum / sq) > thr needs sum > RN(RN(thr sq) (1 - 1e-5)) for thr > 0
         const float lim = thr_lo > -INFINITY ? __fmul_rn(__fmul_rn(thr, sq), 0.99999f) : -INFINITY;
-        float h[2 * S];
+        float h[2 * S], hm[S];
 #pragma unroll
-        for (int j = 0; j < S; ++j) unpack2(sum[j], h[2 * j], h[2 * j + 1]);
-        float mx = max3f(h[0], h[1], h[2]);
+        for (int j = 0; j < S; ++j) {
+            unpack2(sum[j], h[2 * j], h[2 * j + 1]);
+            hm[j] = fmaxf(h[2 * j], h[2 * j + 1]);   // both rows at start j
+        }
+        float mx = max3f(hm[0], hm[1], hm[2]);
 #pragma unroll
-        for (int k = 3; k + 1 < 2 * S; k += 2) mx = max3f(mx, h[k], h[k + 1]);
-        mx = fmaxf(mx, h[2 * S - 1]);
+        for (int k = 3; k + 1 < S; k += 2) mx = max3f(mx, hm[k], hm[k + 1]);
+        if (S % 2 == 0) mx = fmaxf(mx, hm[S - 1]);
         if (!__any_sync(0xffffffffu, mx > lim)) continue;
         const int code = (MODE == 1) ? w - 1 : 31 - __clz(w);
         // windows inside the row: starts j < inside
         const int inside = edge ? cols - (tb + w - 1) : S;
 #pragma unroll
         for (int j = 0; j < S; ++j) {
+            if (!(hm[j] > lim) || j >= inside) continue;
 #pragma unroll
             for (int r = 0; r < 2; ++r) {
                 const float sj = h[2 * j + r];
-                if (sj > lim && j < inside) {
+                if (sj > lim) {
                     const float q = snr_fast ? __fdividef(sj, sq) : __fdiv_rn(sj, sq);
                     if (q > thr) {
                         pass[r] |= 1ull << (8 * j + code);
@@ -428,7 +440,8 @@ k_boxcar_pair(const float* __restrict__ plane, int rows, int cols, const float* 
               unsigned* __restrict__ rec_first, unsigned* __restrict__ rec_count, const WidthConsts wc) {
     // staged positions of a warp: every start's windows, a multiple of 4
     constexpr int kSpan = (kPairWarpTile + WMAX - 1 + 3) / 4 * 4;
-    __shared__ float4 tile4[kPairWarps][kSpan / 2];   // kSpan positions x {row 0, row 1}
+    constexpr int kF4 = kSpan / 2;                      // logical float4s (kSpan positions x 2 rows)
+    __shared__ float4 tile4[kPairWarps][kF4 + kF4 / 4]; // padded (pad4)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wt = blockIdx.x * kPairWarps + warp;     // warp tile
     const int tw = wt * kPairWarpTile;
@@ -444,7 +457,7 @@ k_boxcar_pair(const float* __restrict__ plane, int rows, int cols, const float* 
     }
     auto nz = [&](float v, float m, float s) { return stats ? norm_sample(v, m, s) : v; };
     float4* t4 = tile4[warp];
-    float* tile = reinterpret_cast<float*>(t4);        // position p, row r at 2 p + r
+    float* tile = reinterpret_cast<float*>(t4);        // position p, row r at 4 pad4(p / 2) + 2 (p % 2) + r
     const bool interior = tw + kSpan <= cols;
     if (interior && vec) {
         // 16-byte loads of both rows, every load in flight before the first use
@@ -465,8 +478,8 @@ k_boxcar_pair(const float* __restrict__ plane, int rows, int cols, const float* 
             if (k < kPer - 1 || q < kQ) {
                 const float b0 = has1 ? nz(b[k].x, m1, s1) : 0.0f, b1 = has1 ? nz(b[k].y, m1, s1) : 0.0f;
                 const float b2 = has1 ? nz(b[k].z, m1, s1) : 0.0f, b3 = has1 ? nz(b[k].w, m1, s1) : 0.0f;
-                t4[2 * q] = make_float4(nz(a[k].x, m0, s0), b0, nz(a[k].y, m0, s0), b1);
-                t4[2 * q + 1] = make_float4(nz(a[k].z, m0, s0), b2, nz(a[k].w, m0, s0), b3);
+                t4[pad4(2 * q)] = make_float4(nz(a[k].x, m0, s0), b0, nz(a[k].y, m0, s0), b1);
+                t4[pad4(2 * q + 1)] = make_float4(nz(a[k].z, m0, s0), b2, nz(a[k].w, m0, s0), b3);
             }
         }
     } else if (interior) {
@@ -485,14 +498,16 @@ k_boxcar_pair(const float* __restrict__ plane, int rows, int cols, const float* 
 #pragma unroll
         for (int k = 0; k < kPer; ++k) {
             const int p = lane + 32 * k;
-            if (k < kPer - 1 || p < kSpan) t2[p] = make_float2(nz(a[k], m0, s0), has1 ? nz(b[k], m1, s1) : 0.0f);
+            if (k < kPer - 1 || p < kSpan)
+                t2[2 * pad4(p >> 1) + (p & 1)] = make_float2(nz(a[k], m0, s0), has1 ? nz(b[k], m1, s1) : 0.0f);
         }
     } else {
         for (int p = lane; p < kSpan; p += 32) {
             const int t = tw + p;
             const bool in = t < cols;
-            tile[2 * p] = in ? nz(__ldg(x0 + t), m0, s0) : 0.0f;
-            tile[2 * p + 1] = (in && has1) ? nz(__ldg(x1 + t), m1, s1) : 0.0f;
+            const int e = 4 * pad4(p >> 1) + 2 * (p & 1);
+            tile[e] = in ? nz(__ldg(x0 + t), m0, s0) : 0.0f;
+            tile[e + 1] = (in && has1) ? nz(__ldg(x1 + t), m1, s1) : 0.0f;
         }
     }
     __syncwarp();
@@ -503,10 +518,10 @@ k_boxcar_pair(const float* __restrict__ plane, int rows, int cols, const float* 
     }
     const int p0 = lane * kPairStarts;
     const int tb = tw + p0;
-    const float4* win4 = t4 + p0 / 2;
+    const int f0 = p0 / 2;
     unsigned long long pass[2] = {0ull, 0ull};
     float snr[128];   // S/N of the passing windows (indexed like their bits)
-    pair_widths<MODE, WMAX>(win4, tb, cols, !interior, thr, thr_lo, snr_fast, wc, pass, snr);
+    pair_widths<MODE, WMAX>(t4, f0, tb, cols, !interior, thr, thr_lo, snr_fast, wc, pass, snr);
     if (!has1) pass[1] = 0ull;
 
     // the warp's block: row 0's candidates, then row 1's, lanes in order
