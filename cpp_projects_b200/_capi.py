@@ -156,6 +156,7 @@ _SIGNATURES = {
     "bfs_chunk_forward_fft": (_I, [_P, _P, _P]),
     "bfs_chunk_voltages": (_I, [_P, _P, ctypes.c_double, _P, _P]),
     "bfs_chunk_detect": (_I, [_P, _P, ctypes.c_double, _P, _P]),
+    "bfs_chunk_detect_spectrum": (_I, [_P, _P, ctypes.c_double, _P, _P]),
     "bfs_chunk_process": (_I, [_P, _P, _P, _I, _P, _P]),
     "bfs_chunk_unpack_fft": (_I, [_P, _P, _P, _P]),
     "bfs_chunk_process_raw": (_I, [_P, _P, _P, _P, _I, _P, _P]),

@@ -103,6 +103,12 @@ class CChunk_gpu:
         _capi.call("bfs_chunk_detect", self._h, dev_ptr(d_volt, torch.float32), ctypes.c_double(dm),
                    dev_ptr(d_plane, torch.float32), stream_handle(stream))
 
+    def detect_spectrum(self, d_spec, dm: float, d_plane, stream=None):
+        """voltages + detect in one call (the voltages are not stored where
+        the own sub-band transform applies)."""
+        _capi.call("bfs_chunk_detect_spectrum", self._h, dev_ptr(d_spec, torch.float32), ctypes.c_double(dm),
+                   dev_ptr(d_plane, torch.float32), stream_handle(stream))
+
     def process(self, pcmparrRawSignalCur: torch.Tensor, stream=None) -> torch.Tensor:
         """CChunkB::process: returns (ndm, max_dt, msamp) normalised FDMT planes."""
         dms = np.ascontiguousarray(self.m_coh_dm_Vector, np.float64)

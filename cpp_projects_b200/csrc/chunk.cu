@@ -18,9 +18,14 @@
 //
 // Differences in form: detection, roll, unpadding, reversal and the
 // dedispersion shift are ONE gather kernel here (one read of the voltages,
-// one write of the plane) instead of three passes; the FFTs are cuFFT with
-// the reference's sizes; the chirp phase is FP64 (modf before sincospi) and
-// the complex multiply FP32 without FMA contraction.
+// one write of the plane) instead of three passes; the chirp phase is FP64
+// (modf before sincospi) and the complex multiply FP32 without FMA
+// contraction.  For nbin = 2^20 the forward FFT is this library's own, fused
+// with the unpack; for mbin = 32768 the chirp, the inverse sub-band
+// transforms and the detection are two passes of this library's own
+// (subband_ifft: the chirp applied on load from a per-DM table, the detected
+// plane written by the second pass); other sizes use cuFFT with the
+// reference's sizes.
 #include <cufft.h>
 
 #include <cmath>
@@ -43,10 +48,14 @@ struct bfs_chunk {
     float* norm = nullptr;   // max_dt x msamp FDMT of the mask
     float* buff = nullptr;   // 4 + 2 rows statistics
     int* d_shift = nullptr;  // rows dedispersion shifts
+    // chirp factors per coherent DM ([chan][sub-band][mbin]) for the own
+    // sub-band transforms, the most recent kChirpCache DMs
+    std::vector<std::pair<double, float2*>> chirps;
     ~bfs_chunk() {
         if (have_fwd) cufftDestroy(fwd);
         if (have_inv) cufftDestroy(inv);
         if (fdmt) bfs_fdmt_plan_destroy(fdmt);
+        for (auto& c : chirps) cudaFree(c.second);
         for (void* p : {static_cast<void*>(volt), static_cast<void*>(plane), static_cast<void*>(mask),
                         static_cast<void*>(norm), static_cast<void*>(buff), static_cast<void*>(d_shift)})
             if (p) cudaFree(p);
@@ -54,6 +63,10 @@ struct bfs_chunk {
 };
 
 namespace bfs {
+bool subband_ifft_supported(int nbin, int len_sft, int npol);
+bfs_status subband_ifft(const float2* spec, const float2* chirp, float2* z, float* plane, const int* shift,
+                        int npol2, int nfft, int nchan, int len_sft, int nbin, int nov_pc, int mbin_adj, int msamp,
+                        cudaStream_t s);
 bool fft_fused_supported(int nbin, int npol);
 bfs_status fft_forward_guppi(const signed char* raw, float2* tmp, float2* x, long long nsamp, int noverlap,
                              int nfft, int nchan, int npol, cudaStream_t s);
@@ -80,15 +93,10 @@ __global__ void k_unpack_guppi(const signed char* __restrict__ raw, float2* __re
     }
 }
 
-// Chirp: one thread per (bin of the mbin sub-band, sub-band, coarse channel);
-// the factor is evaluated in FP64 and applied to every polarisation and FFT
-// segment at the fft-shifted position of the nbin spectrum.
-__global__ void k_chirp(const float2* __restrict__ in, float2* __restrict__ out, double dm, int nchan,
-                        int len_sft, int mbin, int nbin, int nseg, double fmin, double bw_sub,
-                        double bw_chan) {
-    const int ibin = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ibin >= mbin) return;
-    const int isft = blockIdx.y, ichan = blockIdx.z;
+// The chirp factor of bin ibin of sub-band isft of coarse channel ichan:
+// phase in FP64 (modf before sincospi), taper, 1/nbin, rounded to float.
+__device__ __forceinline__ float2 chirp_factor(double dm, int ichan, int isft, int ibin, int len_sft, int mbin,
+                                               int nbin, double fmin, double bw_sub, double bw_chan) {
     // centre of the fine channel, rounded to float as the reference stores it
     const float f0 = static_cast<float>(fmin + bw_sub * (0.5 + ichan) +
                                         bw_chan * (isft - len_sft / 2.0 + 0.5));
@@ -100,17 +108,39 @@ __global__ void k_chirp(const float2* __restrict__ in, float2* __restrict__ out,
     const double frac = -modf(phase, &whole) * 2.0;
     double sn, cs;
     sincospi(frac, &sn, &cs);
-    const float cx = static_cast<float>(cs * taper / static_cast<double>(nbin));
-    const float cy = static_cast<float>(sn * taper / static_cast<double>(nbin));
+    return make_float2(static_cast<float>(cs * taper / static_cast<double>(nbin)),
+                       static_cast<float>(sn * taper / static_cast<double>(nbin)));
+}
+
+// Chirp: one thread per (bin of the mbin sub-band, sub-band, coarse channel);
+// the factor is applied to every polarisation and FFT segment at the
+// fft-shifted position of the nbin spectrum.
+__global__ void k_chirp(const float2* __restrict__ in, float2* __restrict__ out, double dm, int nchan,
+                        int len_sft, int mbin, int nbin, int nseg, double fmin, double bw_sub,
+                        double bw_chan) {
+    const int ibin = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ibin >= mbin) return;
+    const int isft = blockIdx.y, ichan = blockIdx.z;
+    const float2 cf = chirp_factor(dm, ichan, isft, ibin, len_sft, mbin, nbin, fmin, bw_sub, bw_chan);
     const size_t pos = static_cast<size_t>(ichan) * nbin + (isft * mbin + ibin + nbin / 2) % nbin;
     const size_t stride = static_cast<size_t>(nbin) * nchan;
     for (int i = 0; i < nseg; ++i) {
         const float2 a = in[pos + i * stride];
         float2 o;
-        o.x = __fsub_rn(__fmul_rn(a.x, cx), __fmul_rn(a.y, cy));
-        o.y = __fadd_rn(__fmul_rn(a.x, cy), __fmul_rn(a.y, cx));
+        o.x = __fsub_rn(__fmul_rn(a.x, cf.x), __fmul_rn(a.y, cf.y));
+        o.y = __fadd_rn(__fmul_rn(a.x, cf.y), __fmul_rn(a.y, cf.x));
         out[pos + i * stride] = o;
     }
+}
+
+// The factors alone: tab[(ichan len_sft + isft) mbin + ibin].
+__global__ void k_chirp_table(float2* __restrict__ tab, double dm, int len_sft, int mbin, int nbin, double fmin,
+                              double bw_sub, double bw_chan) {
+    const int ibin = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ibin >= mbin) return;
+    const int isft = blockIdx.y, ichan = blockIdx.z;
+    tab[(static_cast<size_t>(ichan) * len_sft + isft) * mbin + ibin] =
+        chirp_factor(dm, ichan, isft, ibin, len_sft, mbin, nbin, fmin, bw_sub, bw_chan);
 }
 
 // Power detection + roll by nbin/2 + unpadding + frequency reversal +
@@ -290,9 +320,57 @@ extern "C" bfs_status bfs_chunk_forward_fft(bfs_chunk* c, void* d_cplx, void* st
                        "cufftExecC2C(forward)");
 }
 
+constexpr size_t kChirpCache = 4;
+
+// Whether the DM loop runs the own sub-band transforms (chirp table + two
+// passes) for these buffers.
+static bool own_subband(const bfs_chunk* c, const void* d_spec) {
+    return subband_ifft_supported(c->d.nbin, c->d.len_sft, c->d.npol) &&
+           reinterpret_cast<uintptr_t>(d_spec) % 16 == 0;
+}
+
+// The chirp table of one coherent DM (computed on first use, kept for the
+// chunk's most recent DMs).
+static bfs_status chirp_table(bfs_chunk* c, double dm, const float2** out, cudaStream_t s) {
+    for (auto& e : c->chirps)
+        if (e.first == dm) { *out = e.second; return BFS_OK; }
+    const bfs_chunk_desc& d = c->d;
+    float2* tab = nullptr;
+    if (c->chirps.size() >= kChirpCache) {   // reuse the oldest table's memory
+        BFS_CUDA(cudaStreamSynchronize(s));
+        tab = c->chirps.front().second;
+        c->chirps.erase(c->chirps.begin());
+    } else {
+        BFS_CUDA(cudaMalloc(&tab, sizeof(float2) * static_cast<size_t>(d.nchan) * d.len_sft * c->mbin));
+    }
+    c->chirps.emplace_back(dm, tab);
+    const double bw = static_cast<double>(d.fmax - d.fmin);
+    const double bw_sub = bw / d.nchan;
+    const double bw_chan = bw_sub / d.len_sft;
+    dim3 grid((c->mbin + 255) / 256, d.len_sft, d.nchan);
+    BFS_ARG(grid.y <= 65535 && grid.z <= 65535, "too many sub-bands or channels");
+    k_chirp_table<<<grid, 256, 0, s>>>(tab, dm, d.len_sft, c->mbin, d.nbin, static_cast<double>(d.fmin), bw_sub,
+                                       bw_chan);
+    BFS_LAUNCH_CHECK("k_chirp_table");
+    *out = tab;
+    return BFS_OK;
+}
+
 static bfs_status chunk_voltages(bfs_chunk* c, const void* d_spec, double dm, float2* d_volt,
                                  cudaStream_t s) {
     const bfs_chunk_desc& d = c->d;
+    // (the first pass reads all of a sub-band while writing it: not in place)
+    const char* sp = static_cast<const char*>(d_spec);
+    const char* vp = reinterpret_cast<const char*>(d_volt);
+    const size_t bytes = sizeof(float2) * static_cast<size_t>(c->cplx_len);
+    const bool apart = vp + bytes <= sp || sp + bytes <= vp;
+    if (apart && own_subband(c, d_spec)) {
+        const float2* tab = nullptr;
+        bfs_status st = chirp_table(c, dm, &tab, s);
+        if (st != BFS_OK) return st;
+        return subband_ifft(static_cast<const float2*>(d_spec), tab, d_volt, nullptr, nullptr, d.npol / 2, d.nfft,
+                            d.nchan, d.len_sft, d.nbin, c->nov_pc, c->mbin_adj, c->msamp, s);
+    }
     // band arithmetic as in CChunk_fly_gpu::elementWiseMult (Chunk_fly_gpu.cu:96-99)
     const double bw = static_cast<double>(d.fmax - d.fmin);
     const double bw_sub = bw / d.nchan;
@@ -355,6 +433,39 @@ static bfs_status chunk_detect(bfs_chunk* c, const float2* d_volt, double dm, fl
     return BFS_OK;
 }
 
+// The detected plane of one DM straight from the spectrum: the own two-pass
+// chirp + sub-band transforms + detection when the geometry has them (the
+// voltages never stored), else voltages into c->volt and the gather.
+static bfs_status chunk_detect_spectrum(bfs_chunk* c, const void* d_spec, double dm, float* d_plane,
+                                        cudaStream_t s) {
+    if (!own_subband(c, d_spec)) {
+        bfs_status st = chunk_voltages(c, d_spec, dm, c->volt, s);
+        if (st != BFS_OK) return st;
+        return chunk_detect(c, c->volt, dm, d_plane, s);
+    }
+    std::vector<int> sh;
+    chunk_shifts(c, dm, sh);
+    BFS_CUDA(cudaMemcpyAsync(c->d_shift, sh.data(), sizeof(int) * sh.size(), cudaMemcpyHostToDevice, s));
+    const float2* tab = nullptr;
+    bfs_status st = chirp_table(c, dm, &tab, s);
+    if (st == BFS_OK) {
+        const bfs_chunk_desc& d = c->d;
+        st = subband_ifft(static_cast<const float2*>(d_spec), tab, c->volt, d_plane, c->d_shift, d.npol / 2, d.nfft,
+                          d.nchan, d.len_sft, d.nbin, c->nov_pc, c->mbin_adj, c->msamp, s);
+    }
+    // the host vector must outlive the (pageable, staged) copy
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (st == BFS_OK && e != cudaSuccess) st = fail(BFS_ERR_CUDA, "cudaStreamSynchronize: %s", cudaGetErrorString(e));
+    return st;
+}
+
+extern "C" bfs_status bfs_chunk_detect_spectrum(bfs_chunk* c, const void* d_spec, double dm, float* d_plane,
+                                                void* stream) {
+    BFS_ARG(c && d_spec && d_plane, "null argument");
+    BFS_ARG(cplx_aligned(d_spec), "d_spec must be 8-byte aligned");
+    return chunk_detect_spectrum(c, d_spec, dm, d_plane, as_stream(stream));
+}
+
 extern "C" bfs_status bfs_chunk_detect(bfs_chunk* c, const void* d_volt, double dm, float* d_plane,
                                        void* stream) {
     BFS_ARG(c && d_volt && d_plane, "null argument");
@@ -386,9 +497,7 @@ static bfs_status chunk_dm_loop(bfs_chunk* c, const void* d_cplx, const double* 
     bfs_status st = BFS_OK;
     const size_t plane_out = static_cast<size_t>(c->d.max_dt) * c->msamp;
     for (int i = 0; i < ndm; ++i) {
-        st = chunk_voltages(c, d_cplx, dms[i], c->volt, s);
-        if (st != BFS_OK) return st;
-        st = chunk_detect(c, c->volt, dms[i], c->plane, s);
+        st = chunk_detect_spectrum(c, d_cplx, dms[i], c->plane, s);
         if (st != BFS_OK) return st;
         st = bfs_preproc_calc_fdmt_inputs(c->plane, c->rows, c->msamp, c->buff, c->mask, stream);
         if (st != BFS_OK) return st;

@@ -498,13 +498,22 @@ bfs_status bfs_chunk_unpack(bfs_chunk* chunk, const int8_t* d_raw, void* d_cplx,
 bfs_status bfs_chunk_forward_fft(bfs_chunk* chunk, void* d_cplx, void* stream);
 /* Coherently dedispersed voltages for one DM: chirp (FP64 phase) + inverse
  * FFTs of length mbin (Chunk_fly_gpu.cu:94-163, Chunk_gpu.cu:284-288).
- * d_spec is not modified. */
+ * d_spec is not modified.  For mbin = 32768 (nbin a power of two, d_spec
+ * 16-byte aligned, d_volt not overlapping d_spec) the library's own two-pass
+ * transform with the chirp applied on load; it agrees with chirp + cuFFT to
+ * FP32 rounding.  Other cases: chirp + cuFFT. */
 bfs_status bfs_chunk_voltages(bfs_chunk* chunk, const void* d_spec, double dm, void* d_volt,
                               void* stream);
 /* Power detection + roll + unpadding + frequency reversal + dedispersion shift
  * (Chunk_gpu.cu:296-321) into a rows x msamp plane.  Synchronises `stream`. */
 bfs_status bfs_chunk_detect(bfs_chunk* chunk, const void* d_volt, double dm, float* d_plane,
                             void* stream);
+/* bfs_chunk_voltages followed by bfs_chunk_detect without storing the
+ * voltages where the own sub-band transform applies (its second pass writes
+ * the detected plane): the same plane, bit for bit, as detecting the
+ * voltages bfs_chunk_voltages returns.  Synchronises `stream`. */
+bfs_status bfs_chunk_detect_spectrum(bfs_chunk* chunk, const void* d_spec, double dm, float* d_plane,
+                                     void* stream);
 /* CChunkB::process (L/CDMT/ChunkB.h:73-74): forward FFT of d_cplx (in place,
  * overwritten like the reference's), then per DM voltages, detection,
  * statistical preprocessing, FDMT of mask and data and fdmt_normalization into

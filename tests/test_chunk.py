@@ -191,3 +191,86 @@ def test_dispersed_pulse_recovered_at_its_dm(cuda):
         ch.detect(v, 0.0, plane)
         peaks.append(float(plane.max()))
     assert peaks[1] > 3 * peaks[0]
+
+
+# ---- the own sub-band transforms (mbin = 32768) --------------------------------
+# geometries whose sub-bands are 32768 bins: the two-pass chirp + inverse
+# transform (+ detection) of this library instead of chirp + cuFFT (+ gather)
+OWN_GEOS = {
+    "nbin65536": dict(fmin=1200.0, fmax=1264.0, npol=4, nchan=2, len_sft=2, nbin=65536, nfft=2, noverlap=512,
+                      tsamp=1.0 / 32.0 * 1e-6, max_dt=4),
+    "nbin2^20": dict(fmin=1200.0, fmax=1232.0, npol=2, nchan=1, len_sft=32, nbin=1 << 20, nfft=1,
+                     noverlap=8192, tsamp=1.0 / 32.0 * 1e-6, max_dt=32),
+}
+
+
+def _own(name, dms=(0.0, DM)):
+    g = OWN_GEOS[name]
+    ch = CChunk_gpu(g["fmin"], g["fmax"], g["npol"], g["nchan"], g["len_sft"], 0, 0, 0.0, 0.0, 1, 6.0, 1,
+                    g["nbin"], g["nfft"], g["noverlap"], g["tsamp"], max_dt=g["max_dt"], dms=list(dms))
+    return ch, co.Geometry(**g)
+
+
+def _own_spectrum(ch, g, cuda, seed=11):
+    raw = np.random.default_rng(seed).integers(-8, 8, size=(g.nchan, g.len_chunk, g.npol), dtype=np.int8)
+    d = ch.complex_buffer(cuda)
+    ch.unpack(torch.from_numpy(raw).to(cuda), d)
+    ch.forward_fft(d)
+    return raw, d
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(OWN_GEOS))
+def test_own_subband_voltages_within_1e5_of_fp64(cuda, name):
+    ch, g = _own(name)
+    raw, d = _own_spectrum(ch, g, cuda)
+    v = ch.complex_buffer(cuda)
+    ch.voltages(d, DM, v)     # separate buffers: the own transform
+    got = v.cpu().numpy().view(np.complex64).reshape(g.npol // 2, g.nfft, g.nchan, g.nbin)
+    want = co.voltages(g, co.forward_fft(co.unpack(g, raw)), DM)
+    err = np.abs(got - want).max() / np.abs(want).max()
+    print(f"own sub-band voltages {name}: max |err| / max |v| = {err:.2e}")
+    assert err < 1e-5
+    # the in-place call runs chirp + cuFFT: the same voltages to FP32 rounding
+    ref = d.clone()
+    ch.voltages(ref, DM, ref)
+    cu = ref.cpu().numpy().view(np.complex64).reshape(g.npol // 2, g.nfft, g.nchan, g.nbin)
+    assert np.abs(got - cu).max() / np.abs(cu).max() < 2e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(OWN_GEOS))
+def test_own_subband_detection_equals_detect_of_voltages(cuda, name):
+    """The second pass's detection (roll, unpadding, reversal, shift) gives
+    bit for bit the gather's plane of the voltages the same transform returns."""
+    ch, g = _own(name)
+    _, d = _own_spectrum(ch, g, cuda, seed=5)
+    for dm in (0.0, DM):
+        v = ch.complex_buffer(cuda)
+        ch.voltages(d, dm, v)
+        want = torch.full((g.rows, g.msamp), float("nan"), device=cuda)
+        ch.detect(v, dm, want)
+        got = torch.full((g.rows, g.msamp), float("nan"), device=cuda)
+        ch.detect_spectrum(d, dm, got)
+        assert torch.equal(got.view(torch.int32), want.view(torch.int32)), (name, dm)
+
+
+@pytest.mark.gpu
+def test_own_subband_process_chain_matches_oracle(cuda):
+    ch, g = _own("nbin65536")
+    raw = np.random.default_rng(21).integers(-8, 8, size=(g.nchan, g.len_chunk, g.npol), dtype=np.int8)
+    d = ch.complex_buffer(cuda)
+    ch.unpack(torch.from_numpy(raw).to(cuda), d)
+    planes = ch.process(d)
+    d2 = ch.complex_buffer(cuda)
+    ch.unpack(torch.from_numpy(raw).to(cuda), d2)
+    ch.forward_fft(d2)
+    for i, dm in enumerate([0.0, DM]):
+        plane = torch.empty((g.rows, g.msamp), device=cuda)
+        ch.detect_spectrum(d2, dm, plane)
+        x, mask, _ = pyoracle.calc_fdmt_inputs(plane.cpu().numpy())
+        fd = pyoracle.fdmt_f32(g.fmin, g.fmax, x, g.rows, g.msamp, g.max_dt)
+        nm = pyoracle.fdmt_f32(g.fmin, g.fmax, mask, g.rows, g.msamp, g.max_dt)
+        want = pyoracle.fdmt_normalize(fd, nm)
+        got = planes[i].cpu().numpy()
+        assert np.abs(got - want).max() <= 1e-5 * max(1.0, np.abs(want).max())
