@@ -736,16 +736,18 @@ template <int K, bool FAST>
 __device__ __forceinline__ void seg_chunks(float* __restrict__ sm, int rd, int wr, int4 q, int c0,
                                            int lane, int thr) {
     const int col = c0 * 32 + lane;
-    const int pa = rd + q.x + col, pb = rd + q.y + col, pw = wr + q.w + col;
+    const float* pa = sm + (rd + q.x + col);
+    const float* pb = sm + (rd + q.y + col);
+    float* pw = sm + (wr + q.w + col);
     float va[K], vb[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-        va[k] = sm[pa + 32 * k];
-        vb[k] = sm[pb + 32 * k];
+        va[k] = pa[32 * k];
+        vb[k] = pb[32 * k];
     }
 #pragma unroll
     for (int k = 0; k < K; ++k)
-        sm[pw + 32 * k] = (FAST || col + 32 * k >= thr) ? __fadd_rn(va[k], vb[k]) : va[k];
+        pw[32 * k] = (FAST || col + 32 * k >= thr) ? __fadd_rn(va[k], vb[k]) : va[k];
 }
 
 // Two rows of a level (fast tiles: every sample at or past every head
@@ -753,26 +755,30 @@ __device__ __forceinline__ void seg_chunks(float* __restrict__ sm, int rd, int w
 template <int K>
 __device__ __forceinline__ void seg_rows2(float* __restrict__ sm, int rd, int wr, int4 q0, int4 q1, bool two,
                                           int lane) {
-    const int pa0 = rd + q0.x + lane, pb0 = rd + q0.y + lane, pw0 = wr + q0.w + lane;
-    const int pa1 = rd + q1.x + lane, pb1 = rd + q1.y + lane, pw1 = wr + q1.w + lane;
+    const float* pa0 = sm + (rd + q0.x + lane);
+    const float* pb0 = sm + (rd + q0.y + lane);
+    float* pw0 = sm + (wr + q0.w + lane);
+    const float* pa1 = sm + (rd + q1.x + lane);
+    const float* pb1 = sm + (rd + q1.y + lane);
+    float* pw1 = sm + (wr + q1.w + lane);
     float a0[K], b0[K], a1[K], b1[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-        a0[k] = sm[pa0 + 32 * k];
-        b0[k] = sm[pb0 + 32 * k];
+        a0[k] = pa0[32 * k];
+        b0[k] = pb0[32 * k];
     }
     if (two) {
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            a1[k] = sm[pa1 + 32 * k];
-            b1[k] = sm[pb1 + 32 * k];
+            a1[k] = pa1[32 * k];
+            b1[k] = pb1[32 * k];
         }
     }
 #pragma unroll
-    for (int k = 0; k < K; ++k) sm[pw0 + 32 * k] = __fadd_rn(a0[k], b0[k]);
+    for (int k = 0; k < K; ++k) pw0[32 * k] = __fadd_rn(a0[k], b0[k]);
     if (two) {
 #pragma unroll
-        for (int k = 0; k < K; ++k) sm[pw1 + 32 * k] = __fadd_rn(a1[k], b1[k]);
+        for (int k = 0; k < K; ++k) pw1[32 * k] = __fadd_rn(a1[k], b1[k]);
     }
 }
 
@@ -981,22 +987,29 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 256 ? 2 : 1) k_fdmt_seg(co
         for (int i = 2; i <= kSegMaxLevels; ++i)
             if (i == a.nlev) nl = nlv[i];
         const int rd = (a.nlev & 1) ? xo : a.y0;
+        const bool clean = fast && t0 + kSegTile <= a.ncols;   // no shift test, no row end in this tile
         for (int r = cw; r < nl; r += ncw) {
             const int4 q = e[r];
             const int col = lane;
-            const int pa = rd + q.x + col, pb = rd + q.y + col;
+            const float* pa = sm + (rd + q.x + col);
+            const float* pb = sm + (rd + q.y + col);
             float va[kOutCPH], vb[kOutCPH];
 #pragma unroll
             for (int k = 0; k < kOutCPH; ++k) {
-                va[k] = sm[pa + 32 * k];
-                vb[k] = sm[pb + 32 * k];
+                va[k] = pa[32 * k];
+                vb[k] = pb[32 * k];
             }
             float* dst = a.out + static_cast<size_t>(q.w) * a.out_pitch + t0 + col;
-            const int thr = q.z - t0;
-            const int lim = a.ncols - t0 - col;  // samples of this row left from this lane's first
+            if (clean) {
 #pragma unroll
-            for (int k = 0; k < kOutCPH; ++k)
-                if (32 * k < lim) dst[32 * k] = (fast || col + 32 * k >= thr) ? __fadd_rn(va[k], vb[k]) : va[k];
+                for (int k = 0; k < kOutCPH; ++k) dst[32 * k] = __fadd_rn(va[k], vb[k]);
+            } else {
+                const int thr = q.z - t0;
+                const int lim = a.ncols - t0 - col;  // samples of this row left from this lane's first
+#pragma unroll
+                for (int k = 0; k < kOutCPH; ++k)
+                    if (32 * k < lim) dst[32 * k] = (fast || col + 32 * k >= thr) ? __fadd_rn(va[k], vb[k]) : va[k];
+            }
         }
         if (single && more) {  // every warp is done with the buffers: load the next tile
             __syncthreads();
@@ -1285,7 +1298,9 @@ static bfs_status plan_host_part(const bfs_fdmt_desc* desc, std::unique_ptr<bfs_
 static inline int bfs_fdmt_plan_depth_of(int d) { return d; }
 
 // ---------------------------------------------------------------------------
-// Autotuner: fusion depth and head tile measured on the plan's own shape.
+// Autotuner: head depth and tile, or the first segment forming level 0, then
+// segment length, rows per tile and input buffers per CTA, timed on the
+// plan's own shape.
 // ---------------------------------------------------------------------------
 namespace {
 struct TuneKey {
@@ -1297,7 +1312,7 @@ struct TuneKey {
                         o.fmin_bits, o.fmax_bits);
     }
 };
-struct TuneVal { int depth, tile, seg, rows; float ms; };
+struct TuneVal { int depth, tile, seg, rows, flags; float ms; };
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneVal> g_tune;
 
@@ -1320,24 +1335,29 @@ static bfs_status tune_fdmt(const bfs_fdmt_desc& base, TuneVal* best) {
         auto it = g_tune.find(tune_key(base));
         if (it != g_tune.end()) { *best = it->second; return BFS_OK; }
     }
-    struct Cand { int depth, tile, seg, rows; };
+    struct Cand { int depth, tile, seg, rows, flags; };
     std::vector<Cand> cands;
     // one merge pass per level: head depth x head tile
-    cands.push_back({0, 0, 1, 0});
+    cands.push_back({0, 0, 1, 0, 0});
     for (int k : {2, 3, 4, 5})
-        for (int tile : {256, 512}) cands.push_back({k, tile, 1, 0});
-    // fused merge segments of 2, 3 or 4 levels x 16 or 32 rows per tile (FP32)
+        for (int tile : {256, 512}) cands.push_back({k, tile, 1, 0, 0});
+    // fused merge segments of 2, 3 or 4 levels x 16 or 32 rows per tile (FP32):
+    // after a head, or forming level 0 in the first segment with one or two
+    // input buffers per CTA (one buffer: half the input staging, so two CTAs
+    // share an SM where two buffers allow one)
     if (base.precision == BFS_PREC_F32)
         for (int seg : {2, 3, 4})
-            for (int rows : {16, 32})
-                for (int k : {0, 2, 3, 4}) cands.push_back({k, k ? 256 : 0, seg, rows});
+            for (int rows : {16, 32}) {
+                for (int flags : {0, static_cast<int>(BFS_SEG_SINGLE_BUFFER)}) cands.push_back({0, 0, seg, rows, flags});
+                for (int k : {2, 3, 4}) cands.push_back({k, 256, seg, rows, 0});
+            }
     const size_t in_n = static_cast<size_t>(base.nchan) * base.ncols;
     const size_t out_n = static_cast<size_t>(base.max_dt) * base.ncols;
     float *d_in = nullptr, *d_out = nullptr;
     void* ws = nullptr;
     size_t ws_bytes = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    TuneVal win{0, 0, 1, 0, 1e30f};
+    TuneVal win{0, 0, 1, 0, 0, 1e30f};
     bfs_status st = BFS_OK;
     cudaStream_t s = nullptr;
     if (cudaMalloc(&d_in, in_n * sizeof(float)) != cudaSuccess ||
@@ -1353,6 +1373,8 @@ static bfs_status tune_fdmt(const bfs_fdmt_desc& base, TuneVal* best) {
         d.head_tile = c.tile;
         d.seg_levels = c.seg;
         d.seg_rows = c.rows;
+        d.seg_threads = 0;
+        d.seg_flags = c.flags;
         d.flags = BFS_FDMT_EXTERNAL_WS;
         bfs_fdmt_plan* p = nullptr;
         if (bfs_fdmt_plan_create(&d, &p) != BFS_OK) continue;  // depth/tile not usable here
@@ -1380,7 +1402,7 @@ static bfs_status tune_fdmt(const bfs_fdmt_desc& base, TuneVal* best) {
             ms = std::min(ms, t);
         }
         bfs_fdmt_plan_destroy(p);
-        if (ok && ms < win.ms) win = TuneVal{bfs_fdmt_plan_depth_of(c.depth), c.tile, c.seg, c.rows, ms};
+        if (ok && ms < win.ms) win = TuneVal{bfs_fdmt_plan_depth_of(c.depth), c.tile, c.seg, c.rows, c.flags, ms};
     }
     if (ws) cudaFree(ws);
     if (d_in) cudaFree(d_in);
@@ -1406,6 +1428,8 @@ extern "C" bfs_status bfs_fdmt_autotune_desc(const bfs_fdmt_desc* desc, bfs_fdmt
         tuned->head_tile = v.tile;
         tuned->seg_levels = v.seg;
         tuned->seg_rows = v.rows;
+        tuned->seg_threads = 0;
+        tuned->seg_flags = v.flags;
     }
     if (ms) *ms = v.ms;
     return BFS_OK;
@@ -1442,6 +1466,8 @@ extern "C" bfs_status bfs_fdmt_plan_create(const bfs_fdmt_desc* desc_in, bfs_fdm
         tuned.head_tile = v.tile;
         tuned.seg_levels = v.seg;
         tuned.seg_rows = v.rows;
+        tuned.seg_threads = 0;
+        tuned.seg_flags = v.flags;
     }
     const bfs_fdmt_desc* desc = &tuned;
     std::unique_ptr<bfs_fdmt_plan> p;

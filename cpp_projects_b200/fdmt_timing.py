@@ -45,6 +45,8 @@ def main(argv=None) -> int:
     ap.add_argument("--tile", type=int, default=0)
     ap.add_argument("--seg-levels", type=int, default=0, help="merge levels per fused pass (1: none)")
     ap.add_argument("--seg-rows", type=int, default=0, help="output rows per fused tile (0: auto)")
+    ap.add_argument("--seg-threads", type=int, default=0, help="threads per segment CTA (0: auto; 256/512/1024)")
+    ap.add_argument("--seg-flags", type=int, default=0, help="1: one input buffer per segment CTA")
     ap.add_argument("--precision", choices=sorted(PRECISIONS), default="f32")
     ap.add_argument("--adjoint", action="store_true")
     ap.add_argument("--reps", type=int, default=10)
@@ -62,11 +64,13 @@ def main(argv=None) -> int:
         from .fdmt import autotune_desc
         t, _ = autotune_desc(_capi.FdmtDesc(fmin=a.fmin, fmax=a.fmax, nchan=a.nchan, ncols=a.ncols,
                                             max_dt=max_dt, precision=PRECISIONS[a.precision]))
-        print(f"--fuse {t.fuse_depth} --tile {t.head_tile} --seg-levels {t.seg_levels} --seg-rows {t.seg_rows}")
+        print(f"--fuse {t.fuse_depth} --tile {t.head_tile} --seg-levels {t.seg_levels} --seg-rows {t.seg_rows} "
+              f"--seg-threads {t.seg_threads} --seg-flags {t.seg_flags}")
         return 0
     dev = torch.device("cuda", 0)
     f = CFdmtGpu(a.fmin, a.fmax, a.nchan, a.ncols, max_dt, fuse_depth=a.fuse, head_tile=a.tile,
-                 precision=PRECISIONS[a.precision], seg_levels=a.seg_levels, seg_rows=a.seg_rows)
+                 precision=PRECISIONS[a.precision], seg_levels=a.seg_levels, seg_rows=a.seg_rows,
+                 seg_threads=a.seg_threads, seg_flags=a.seg_flags)
     g = torch.Generator(device=dev).manual_seed(1)
     if a.adjoint:
         src = torch.randn((max_dt, a.ncols), device=dev, generator=g)
@@ -94,6 +98,7 @@ def main(argv=None) -> int:
     print(json.dumps({"passes": f.passes(),"nchan": a.nchan, "ncols": a.ncols, "max_dt": max_dt, "precision": a.precision,
                       "adjoint": a.adjoint, "fuse_depth": f.info.fuse_depth,
                       "hbm_passes": f.info.hbm_passes, "seg_levels": f.info.seg_levels, "ms": ms,
+                      "seg_threads": a.seg_threads, "seg_flags": a.seg_flags,
                       "sched_bytes": f.info.sched_bytes,
                       "alg_bytes": f.alg_bytes, "alg_gbs": f.alg_bytes / (ms / 1e3) / 1e9,
                       "reference_gflop_per_s": (REFERENCE_GFLOP[a.nchan] / (ms / 1e3)
