@@ -36,7 +36,7 @@
 namespace bfs {
 namespace {
 
-constexpr int kAdjThreads = 256;
+constexpr int kAdjThreads = 128;   // measured: 128 > 256 > 512 on 1024 x 65536
 constexpr int kAdjVecs = 2;       // float4 column groups per thread
 constexpr int kAdjInitThreads = 256;
 
@@ -175,6 +175,86 @@ k_fdmt_adj_init(const float* __restrict__ g0, float* __restrict__ gx, int ncols,
         }
     }
     if (q >= nv) return;
+    if (vec_out && u + 3 < ncols) {
+        reinterpret_cast<float4*>(o)[q] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (u + j < ncols) o[u + j] = acc[j];
+    }
+}
+
+// The last adjoint merge level (level 1 -> level 0) fused with the adjoint of
+// level 0 (Keith plans, R0C level-0 rows per channel): for each of channel
+// c's level-0 rows the CTA gathers the row's gradient over its samples into
+// shared memory (the k_fdmt_adj_level gather of one float4 per thread) and
+// folds it into gx at once (the k_fdmt_adj_init sum), so the level-0
+// gradient plane is never written or read back.  The sums and their order
+// are those of the two kernels, so the bits are too.  CTA b gathers quads
+// 255 b .. 255 b + 255 and writes gx for the first 255 of them (each quad's
+// window reaches into the next one).  gout: 16-byte aligned rows, pitch a
+// multiple of 4.  grid: (ceil(ceil(ncols / 4) / 255), nchan)
+template <int R0C>
+__global__ void __launch_bounds__(kAdjInitThreads)
+k_fdmt_adj_level0(const float* __restrict__ gout, float* __restrict__ gx, const int* __restrict__ off,
+                  const int2* __restrict__ ent, int ncols, int out_pitch, int vec_out) {
+    constexpr int kOut = kAdjInitThreads - 1;   // quads written per CTA
+    __shared__ float4 tile[kAdjInitThreads];
+    const int c = blockIdx.y;
+    const int nv = (ncols + 3) >> 2;
+    const int lane = threadIdx.x & 31;
+    const int q = blockIdx.x * kOut + threadIdx.x;
+    const int u = 4 * q;
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll 1
+    for (int rr = 0; rr < R0C; ++rr) {
+        const int i = c * R0C + rr;   // level-0 row (c, rr)
+        const int beg = __ldg(off + i), end = __ldg(off + i + 1);
+        float g[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        for (int e = beg; e < end; ++e) {  // uniform over the block
+            const int2 en = __ldg(ent + e);
+            const int s = en.y;
+            const float4* rv = reinterpret_cast<const float4*>(gout + static_cast<size_t>(en.x) * out_pitch);
+            const int sv = s >> 2, r = s & 3;
+            const int qa = q + sv;
+            float4 lo = (qa < nv) ? __ldg(rv + qa) : make_float4(0.f, 0.f, 0.f, 0.f);
+            if (r != 0) {
+                float4 hi;
+                hi.x = __shfl_down_sync(0xffffffffu, lo.x, 1);
+                hi.y = __shfl_down_sync(0xffffffffu, lo.y, 1);
+                hi.z = __shfl_down_sync(0xffffffffu, lo.z, 1);
+                hi.w = __shfl_down_sync(0xffffffffu, lo.w, 1);
+                if (lane == 31) hi = (qa + 1 < nv) ? __ldg(rv + qa + 1) : make_float4(0.f, 0.f, 0.f, 0.f);
+                const float w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+                lo = cut4(w, r);
+            }
+            const float v[4] = {lo.x, lo.y, lo.z, lo.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (u + j + s < ncols) g[j] = __fadd_rn(g[j], v[j]);
+        }
+        tile[threadIdx.x] = make_float4(g[0], g[1], g[2], g[3]);
+        __syncthreads();
+        if (threadIdx.x < kOut) {
+            const float4 a = tile[threadIdx.x], b = tile[threadIdx.x + 1];
+            const float e8[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+            const float rcp = __frcp_rn(static_cast<float>(rr + 1));
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                float w = 0.0f;
+#pragma unroll
+                for (int r = 0; r < R0C; ++r) {
+                    if (r > rr) break;
+                    const int t = u + j + r;
+                    if (t >= rr && t < ncols) w = __fadd_rn(w, e8[j + r]);
+                }
+                acc[j] = __fadd_rn(acc[j], __fmul_rn(w, rcp));
+            }
+        }
+        __syncthreads();   // the tile is rewritten for the next row
+    }
+    if (threadIdx.x >= kOut || q >= nv) return;
+    float* o = gx + static_cast<size_t>(c) * ncols;
     if (vec_out && u + 3 < ncols) {
         reinterpret_cast<float4*>(o)[q] = make_float4(acc[0], acc[1], acc[2], acc[3]);
     } else {
@@ -337,7 +417,15 @@ bfs_status adjoint_run(bfs_fdmt_plan* p, const float* d_gy, float* d_gx, float* 
     const int span = kAdjThreads * kAdjVecs;
     const int gy_blocks = ((T + 3) / 4 + span - 1) / span;
     BFS_ARG(gy_blocks <= 65535, "ncols too large for this build");
-    for (int l = h.niter; l >= 1; --l) {
+    // Keith plans: the last merge level runs fused with the level-0 adjoint
+    // when the level-1 gradient rows allow 16-byte reads
+    const int r0c = h.rows_per_chan0;
+    const float* src1 = (h.niter == 1) ? d_gy : bufs[1];
+    const int pitch1 = (h.niter == 1) ? T : P;
+    const bool fuse0 = h.kind == BFS_PLAN_KEITH && r0c >= 1 && r0c <= 5 && pitch1 % 4 == 0 &&
+                       (reinterpret_cast<uintptr_t>(src1) & 15) == 0 &&
+                       h.lv[0].total_rows() == h.nchan * r0c;
+    for (int l = h.niter; l >= (fuse0 ? 2 : 1); --l) {
         const float* src = (l == h.niter) ? d_gy : bufs[l & 1];
         float* dst = bufs[(l - 1) & 1];
         const int in_pitch = (l == h.niter) ? T : P;
@@ -359,9 +447,24 @@ bfs_status adjoint_run(bfs_fdmt_plan* p, const float* d_gy, float* d_gx, float* 
         BFS_LAUNCH_CHECK("k_fdmt_adj_init_grid");
         return BFS_OK;
     }
+    const int vec_out = (T % 4 == 0) && (reinterpret_cast<uintptr_t>(d_gx) & 15) == 0;
+    if (fuse0) {
+        const int* off = p->d_adj_off + p->adj.off_pos[1];
+        const int2* ent = p->d_adj_ent + p->adj.ent_pos[1];
+        dim3 g0(((T + 3) / 4 + kAdjInitThreads - 2) / (kAdjInitThreads - 1), h.nchan);
+        BFS_ARG(g0.y <= 65535, "nchan too large for this build");
+        switch (r0c) {
+            case 1: k_fdmt_adj_level0<1><<<g0, kAdjInitThreads, 0, s>>>(src1, d_gx, off, ent, T, pitch1, vec_out); break;
+            case 2: k_fdmt_adj_level0<2><<<g0, kAdjInitThreads, 0, s>>>(src1, d_gx, off, ent, T, pitch1, vec_out); break;
+            case 3: k_fdmt_adj_level0<3><<<g0, kAdjInitThreads, 0, s>>>(src1, d_gx, off, ent, T, pitch1, vec_out); break;
+            case 4: k_fdmt_adj_level0<4><<<g0, kAdjInitThreads, 0, s>>>(src1, d_gx, off, ent, T, pitch1, vec_out); break;
+            default: k_fdmt_adj_level0<5><<<g0, kAdjInitThreads, 0, s>>>(src1, d_gx, off, ent, T, pitch1, vec_out); break;
+        }
+        BFS_LAUNCH_CHECK("k_fdmt_adj_level0");
+        return BFS_OK;
+    }
     dim3 grid(((T + 3) / 4 + kAdjInitThreads - 1) / kAdjInitThreads, h.nchan);
     BFS_ARG(grid.y <= 65535, "nchan too large for this build");
-    const int vec_out = (T % 4 == 0) && (reinterpret_cast<uintptr_t>(d_gx) & 15) == 0;
     switch (h.rows_per_chan0) {
         case 1: k_fdmt_adj_init<1><<<grid, kAdjInitThreads, 0, s>>>(bufs[0], d_gx, T, P, 1, vec_out); break;
         case 2: k_fdmt_adj_init<2><<<grid, kAdjInitThreads, 0, s>>>(bufs[0], d_gx, T, P, 2, vec_out); break;

@@ -720,6 +720,10 @@ __device__ __forceinline__ void cp_async16(unsigned s, const void* gmem, int src
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes)
                  : "memory");
 }
+// 16 bytes, the whole piece read
+__device__ __forceinline__ void cp_async16_full(unsigned s, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 // 4-byte form (any 4-byte aligned addresses)
 __device__ __forceinline__ void cp_async4(unsigned s, const void* gmem, int src_bytes) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes)
@@ -878,28 +882,44 @@ __global__ void __launch_bounds__(THREADS, THREADS <= 256 ? 2 : 1) k_fdmt_seg(co
         const int t0 = tt * kSegTile;
         const int4* q4 = reinterpret_cast<const int4*>(sm + a.ent_base) + eb * a.max_ent;
         const unsigned x = sbase + 4u * (buf ? a.x1 : 0);
-        for (int r = warp; r < nin; r += inw) {
-            const int4 q = q4[r];
-            const int ts = t0 - q.y;  // the row's first sample
-            const float* src = a.in + static_cast<size_t>(q.x) * a.in_pitch;
-            const unsigned dst = x + 4u * q.w;
-            if (a.ones) {  // the all-ones image: 1 inside [0, ncols), 0 outside
+        if (a.ones) {  // the all-ones image: 1 inside [0, ncols), 0 outside
+            for (int r = warp; r < nin; r += inw) {
+                const int4 q = q4[r];
+                const int ts = t0 - q.y;
                 float* d = sm + (buf ? a.x1 : 0) + q.w;
                 for (int c = lane; c < 32 * NC; c += 32) d[c] = (ts + c >= 0 && ts + c < a.ncols) ? 1.0f : 0.0f;
-            } else if (!a.vec) {  // unaligned rows: 4-byte copies
+            }
+        } else if (!a.vec) {  // unaligned rows: 4-byte copies
+            for (int r = warp; r < nin; r += inw) {
+                const int4 q = q4[r];
+                const int ts = t0 - q.y;
+                const float* src = a.in + static_cast<size_t>(q.x) * a.in_pitch;
+                const unsigned dst = x + 4u * q.w;
                 for (int c = lane; c < 32 * NC; c += 32) {
                     const int t = ts + c;
                     const bool in = t >= 0 && t < a.ncols;
                     cp_async4(dst + 4u * c, in ? src + t : src, in ? 4 : 0);
                 }
-            } else if (ts >= 0 && ts + 4 * kPieces <= a.ncols) {  // the whole window lies in [0, ncols)
+            }
+        } else {
+            constexpr int kPerLane = (kPieces + 31) / 32;
+            for (int r = warp; r < nin; r += inw) {
+                const int4 q = q4[r];
+                const int ts = t0 - q.y;  // the row's first sample
+                const float* src = a.in + static_cast<size_t>(q.x) * a.in_pitch;
+                const unsigned dst = x + 4u * q.w;
+                if (ts >= 0 && ts + 4 * kPieces <= a.ncols) {  // the whole window lies in [0, ncols)
+                    const float* s0 = src + ts + 4 * lane;
+                    const unsigned d0 = dst + 16u * lane;
 #pragma unroll
-                for (int pc = lane; pc < kPieces; pc += 32) cp_async16(dst + 16u * pc, src + ts + 4 * pc, 16);
-            } else {
-                for (int pc = lane; pc < kPieces; pc += 32) {
-                    const int t = ts + 4 * pc;
-                    const int bytes = t < 0 ? 0 : 4 * max(0, min(4, a.ncols - t));
-                    cp_async16(dst + 16u * pc, bytes > 0 ? src + t : src, bytes);
+                    for (int k = 0; k < kPerLane; ++k)
+                        if (k < kPerLane - 1 || lane + 32 * k < kPieces) cp_async16_full(d0 + 512u * k, s0 + 128 * k);
+                } else {
+                    for (int pc = lane; pc < kPieces; pc += 32) {
+                        const int t = ts + 4 * pc;
+                        const int bytes = t < 0 ? 0 : 4 * max(0, min(4, a.ncols - t));
+                        cp_async16(dst + 16u * pc, bytes > 0 ? src + t : src, bytes);
+                    }
                 }
             }
         }

@@ -65,6 +65,32 @@ def test_noalloc_matches_allocating_entry_point_on_two_calls(cuda, shape):
         _capi.lib().bfs_fdmt_plan_destroy(plan)
 
 
+@pytest.mark.parametrize("shape", [
+    (1200.0, 1600.0, 512, 32768, 512),
+    (1100.0, 1500.0, 100, 3001, 77),
+])
+def test_noalloc_ones_mode_matches_allocating_entry_point_on_two_calls(cuda, shape):
+    """b_ones != 0 (the normalisation image, no input): the allocating entry
+    point may take its one-pass mask route; the allocation-free one runs the
+    level kernels on an all-ones image.  Both must give the same bits."""
+    fmin, fmax, nchan, ncols, max_dt = shape
+    plan = _host_plan(*shape)
+    try:
+        ref = CFdmtGpu(fmin, fmax, nchan, ncols, max_dt)
+        want = torch.empty((max_dt, ncols), device=cuda)
+        ref.process_image(None, want, True)
+        s = torch.cuda.current_stream()
+        for call in (1, 2):
+            got = torch.full((max_dt, ncols), float("nan"), device=cuda)
+            st = _capi.lib().bfs_fdmt_execute_noalloc(plan, None, ctypes.c_void_p(got.data_ptr()), 1,
+                                                      ctypes.c_void_p(s.cuda_stream))
+            _capi.check(st)
+            torch.cuda.synchronize()
+            assert torch.equal(got.view(torch.int32), want.view(torch.int32)), f"call {call}"
+    finally:
+        _capi.lib().bfs_fdmt_plan_destroy(plan)
+
+
 def test_noalloc_refuses_a_problem_larger_than_its_static_scratch(cuda):
     plan = _host_plan(1200.0, 1600.0, 4096, 131072, 4096)
     try:
