@@ -136,177 +136,13 @@ k_boxcar(const float* __restrict__ plane, int rows, int cols, const float* __res
     }
 }
 
-// Register-blocked boxcar for a width set fixed at compile time
-// (MODE 0: 1, 2, 4 .. WMAX; MODE 1: 1 .. WMAX).  The CTA's row tile (starts
-// t0 .. t0 + kRegTile - 1 plus the WMAX - 1 samples after them) is read once,
-// normalised once and kept in shared memory.  Each thread owns kRegStarts
-// adjacent starts and runs their running sums side by side (independent add
-// chains, each in the reference's sequential order); it reads its window as
-// float4s just before the width step that first needs them, so only about
-// kRegStarts + 4 window values are live at a time.  sqrtf(w) comes from the
-// host (IEEE there too).  The exact quotient sum / sqrtf(w) is
-// only evaluated for windows whose sum exceeds a per-width lower bound of the
-// sums that can pass (thr > 0; every window when thr <= 0).  Per width the
-// warp ORs the lanes' masks of such windows and visits only the start offsets
-// some lane has set.  Interior
-// tiles (every window inside the row) take a copy with no bounds tests.
-constexpr int kRegStarts = 8;
-constexpr int kRegThreads = 128;
-constexpr int kRegTile = kRegThreads * kRegStarts;
-
-constexpr int kRegMaxW = 128;  // widest window of the register-blocked kernel
+// Widest window of the compile-time width sets (pow2 up to 128, every width
+// up to 8) and sqrtf(w) for them, computed on the host (IEEE there too).
+constexpr int kRegMaxW = 128;
 
 struct WidthConsts {
     float sq[kRegMaxW + 1];  // sqrtf(w), w = 1..kRegMaxW (index w)
 };
-
-template <int MODE, int WMAX, bool INTERIOR>
-__device__ __forceinline__ void boxcar_starts(const float4* __restrict__ win4, int tb, int cols, int row,
-                                              float thr, float thr_lo, int snr_fast, const WidthConsts& wc,
-                                              bfs_cand* __restrict__ out, unsigned capacity,
-                                              unsigned* __restrict__ d_count, int tag, int* __restrict__ tags) {
-    constexpr int S = kRegStarts;
-    constexpr int kVec = (S + WMAX - 1 + 3) / 4;
-    const int lane = threadIdx.x & 31;
-    float win[4 * kVec];
-    float sum[S];
-#pragma unroll
-    for (int v = 0; v < S / 4; ++v) {
-        const float4 q = win4[v];
-        win[4 * v] = q.x; win[4 * v + 1] = q.y; win[4 * v + 2] = q.z; win[4 * v + 3] = q.w;
-    }
-#pragma unroll
-    for (int j = 0; j < S; ++j) sum[j] = 0.0f;
-#pragma unroll
-    for (int w = 1; w <= WMAX; ++w) {
-        // step w reads window values w - 1 .. w + S - 2: fetch the vector
-        // that starts at value w + S - 2 when the step first reaches it
-        constexpr int kFirst = S / 4;
-        if (((w + S - 2) & 3) == 0 && (w + S - 2) / 4 >= kFirst && (w + S - 2) / 4 < kVec) {
-            const float4 q = win4[(w + S - 2) / 4];
-            const int b = w + S - 2;
-            win[b] = q.x; win[b + 1] = q.y; win[b + 2] = q.z; win[b + 3] = q.w;
-        }
-#pragma unroll
-        for (int j = 0; j < S; ++j) sum[j] = __fadd_rn(sum[j], win[j + w - 1]);
-        if (MODE == 0 && (w & (w - 1)) != 0) continue;
-        // RN(sum / sq) > thr needs sum / sq > thr (1 - 2^-24), so for thr > 0
-        // every passing window has sum > RN(RN(thr sq) (1 - 1e-5)) (the two
-        // roundings add at most 2^-23 relative): one compare per window
-        const float sq = wc.sq[w];
-        const float lim = thr_lo > -INFINITY ? __fmul_rn(__fmul_rn(thr, sq), 0.99999f) : -INFINITY;
-        unsigned maybe = 0;
-#pragma unroll
-        for (int j = 0; j < S; ++j)
-            if (sum[j] > lim && (INTERIOR || tb + j + w - 1 < cols)) maybe |= 1u << j;
-        unsigned todo = __reduce_or_sync(0xffffffffu, maybe);
-        if (!todo) continue;
-        const int code = (MODE == 1) ? w : (31 - __clz(w));
-        while (todo) {  // warp-uniform: the start offsets some lane may emit
-            const int j = __ffs(todo) - 1;
-            todo &= todo - 1;
-            float sj = sum[0];
-#pragma unroll
-            for (int k = 1; k < S; ++k)
-                if (k == j) sj = sum[k];
-            float snr = 0.0f;
-            bool pass = false;
-            if ((maybe >> j) & 1u) {
-                snr = snr_fast ? __fdividef(sj, sq) : __fdiv_rn(sj, sq);
-                pass = snr > thr;
-            }
-            const unsigned ballot = __ballot_sync(0xffffffffu, pass);
-            if (ballot) {
-                const int leader = __ffs(ballot) - 1;
-                unsigned base = 0;
-                if (lane == leader) base = atomicAdd(d_count, static_cast<unsigned>(__popc(ballot)));
-                base = __shfl_sync(0xffffffffu, base, leader);
-                if (pass) {
-                    const unsigned idx = base + __popc(ballot & ((1u << lane) - 1u));
-                    if (idx < capacity) {
-                        bfs_cand c;
-                        c.mt = tb + j; c.mdt = row; c.mwidth = code; c.msnr = snr;
-                        out[idx] = c;
-                        if (tags) tags[idx] = tag;
-                    }
-                }
-            }
-        }
-    }
-}
-
-template <int MODE, int WMAX>
-__global__ void __launch_bounds__(kRegThreads)
-k_boxcar_reg(const float* __restrict__ plane, int rows, int cols, const float* __restrict__ stats,
-             const float* __restrict__ d_thr, float thr_host, float thr_lo_host, int snr_fast,
-             bfs_cand* __restrict__ out, unsigned capacity, unsigned* __restrict__ d_count,
-             const WidthConsts wc, int tag, int* __restrict__ tags) {
-    constexpr int kSpan = kRegTile + 4 * ((WMAX - 1 + 3) / 4);
-    __shared__ float4 tile4[kSpan / 4];
-    float* tile = reinterpret_cast<float*>(tile4);
-    const int row = blockIdx.y;
-    const int t0 = blockIdx.x * kRegTile;
-    const float* x = plane + static_cast<size_t>(row) * cols;
-    // interior tile: every window of every start lies inside the row
-    const bool interior = (t0 + kSpan) <= cols;
-    if (stats) {
-        const float m = stats[row], sd = stats[rows + row];
-        if (interior) {
-            // every load in flight before the first use
-            constexpr int kPer = (kSpan + kRegThreads - 1) / kRegThreads;
-            float v[kPer];
-#pragma unroll
-            for (int k = 0; k < kPer; ++k) {
-                const int i = threadIdx.x + k * kRegThreads;
-                v[k] = (k < kPer - 1 || i < kSpan) ? __ldg(x + t0 + i) : 0.0f;
-            }
-#pragma unroll
-            for (int k = 0; k < kPer; ++k) {
-                const int i = threadIdx.x + k * kRegThreads;
-                if (k < kPer - 1 || i < kSpan) tile[i] = norm_sample(v[k], m, sd);
-            }
-        } else {
-            for (int i = threadIdx.x; i < kSpan; i += kRegThreads) {
-                const int t = t0 + i;
-                tile[i] = t < cols ? norm_sample(__ldg(x + t), m, sd) : 0.0f;
-            }
-        }
-    } else {
-        if (interior) {
-            constexpr int kPer = (kSpan + kRegThreads - 1) / kRegThreads;
-            float v[kPer];
-#pragma unroll
-            for (int k = 0; k < kPer; ++k) {
-                const int i = threadIdx.x + k * kRegThreads;
-                v[k] = (k < kPer - 1 || i < kSpan) ? __ldg(x + t0 + i) : 0.0f;
-            }
-#pragma unroll
-            for (int k = 0; k < kPer; ++k) {
-                const int i = threadIdx.x + k * kRegThreads;
-                if (k < kPer - 1 || i < kSpan) tile[i] = v[k];
-            }
-        } else {
-            for (int i = threadIdx.x; i < kSpan; i += kRegThreads) {
-                const int t = t0 + i;
-                tile[i] = t < cols ? __ldg(x + t) : 0.0f;
-            }
-        }
-    }
-    __syncthreads();
-    float thr = thr_host, thr_lo = thr_lo_host;
-    if (d_thr) {
-        thr = __ldg(d_thr);
-        thr_lo = thr > 0.0f ? thr * 0.99999f : -INFINITY;
-    }
-    const float4* win4 = tile4 + threadIdx.x * (kRegStarts / 4);
-    const int tb = t0 + threadIdx.x * kRegStarts;
-    if (interior)
-        boxcar_starts<MODE, WMAX, true>(win4, tb, cols, row, thr, thr_lo, snr_fast, wc, out, capacity, d_count,
-                                        tag, tags);
-    else
-        boxcar_starts<MODE, WMAX, false>(win4, tb, cols, row, thr, thr_lo, snr_fast, wc, out, capacity,
-                                         d_count, tag, tags);
-}
 
 // ---- ordered boxcar over row pairs -------------------------------------------
 // The register-blocked boxcar for two rows at once, writing the candidates
@@ -801,48 +637,6 @@ bfs_status launch_boxcar(const float* d_plane, int rows, int cols, const float* 
         wmax = param;
     } else {
         return fail(BFS_ERR_ARG, "unknown widths_mode %d", mode);
-    }
-    {
-        // compile-time width sets: pow2 up to 128, every width up to 8
-        const float thr_lo = thr > 0.0f ? thr * 0.99999f : -INFINITY;
-        dim3 grid_r((cols + kRegTile - 1) / kRegTile, rows);
-        static_assert(kRegStarts % 4 == 0 && kRegStarts <= 32, "starts per thread: a multiple of 4, at most 32");
-        WidthConsts wc;
-        for (int w = 0; w <= kRegMaxW; ++w) wc.sq[w] = std::sqrt(static_cast<float>(w));  // IEEE-correct on the host
-        bool launched = true;
-#define BFS_BOX_REG(M, W) k_boxcar_reg<M, W><<<grid_r, kRegThreads, 0, s>>>(                  \
-            d_plane, rows, cols, d_stats, d_thr, thr, thr_lo, snr_fast, d_out, capacity, d_count, wc, \
-            tag, d_tags)
-        if (mode == BFS_WIDTHS_POW2) {
-            switch (wmax) {
-                case 1: BFS_BOX_REG(0, 1); break;
-                case 2: BFS_BOX_REG(0, 2); break;
-                case 4: BFS_BOX_REG(0, 4); break;
-                case 8: BFS_BOX_REG(0, 8); break;
-                case 16: BFS_BOX_REG(0, 16); break;
-                case 32: BFS_BOX_REG(0, 32); break;
-                case 64: BFS_BOX_REG(0, 64); break;
-                case 128: BFS_BOX_REG(0, 128); break;
-                default: launched = false;
-            }
-        } else {
-            switch (wmax) {
-                case 1: BFS_BOX_REG(1, 1); break;
-                case 2: BFS_BOX_REG(1, 2); break;
-                case 3: BFS_BOX_REG(1, 3); break;
-                case 4: BFS_BOX_REG(1, 4); break;
-                case 5: BFS_BOX_REG(1, 5); break;
-                case 6: BFS_BOX_REG(1, 6); break;
-                case 7: BFS_BOX_REG(1, 7); break;
-                case 8: BFS_BOX_REG(1, 8); break;
-                default: launched = false;
-            }
-        }
-#undef BFS_BOX_REG
-        if (launched) {
-            BFS_LAUNCH_CHECK("k_boxcar_reg");
-            return BFS_OK;
-        }
     }
     dim3 grid((cols + kBoxTile - 1) / kBoxTile, rows);
     const size_t smem = sizeof(float) * (kBoxTile + wmax - 1);

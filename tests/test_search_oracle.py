@@ -82,25 +82,34 @@ def test_oracle_boxcar_truncated_windows_and_edges():
 
 
 @pytest.mark.parametrize("wmax", [1, 2, 3, 4, 5, 6, 7, 8, 16, 32, 64, 128])
-def test_boxcar_sliding_window_schedule(wmax):
-    """k_boxcar_reg's register window: with S starts per thread, step w reads
-    window values w-1 .. w+S-2; the first S/4 float4s are loaded up front and
-    the vector starting at value w+S-2 at step w.  Every value must be loaded
-    before the step that first reads it, and every float4 read of the thread
-    with the highest start must stay inside the tile of kRegTile + 4 ceil((W-1)/4)
-    values."""
+def test_boxcar_pair_window_schedule(wmax):
+    """k_boxcar_pair's register window: a lane's S starts read positions
+    w-1 .. w+S-2 at width step w, each position a pair {row 0, row 1}, two
+    positions per float4.  The first kPre float4s are loaded up front and the
+    one starting at position w+S-2+kAhead at step w (kAhead steps early).
+    Every position must be loaded before the step that first reads it, and
+    the last lane's highest float4 must stay inside the warp's staged tile,
+    whose logical float4 f sits at f + f // 4 (one float4 of padding after
+    every four)."""
     src = (Path(__file__).resolve().parent.parent / "cpp_projects_b200" / "csrc" / "search.cu").read_text()
-    S = int(re.search(r"constexpr int kRegStarts = (\d+);", src).group(1))
-    threads = int(re.search(r"constexpr int kRegThreads = (\d+);", src).group(1))
-    vec = (S + wmax - 1 + 3) // 4
-    span = threads * S + 4 * ((wmax - 1 + 3) // 4)
-    loaded = set(range(S))
+    S = int(re.search(r"constexpr int kPairStarts = (\d+);", src).group(1))
+    ahead = int(re.search(r"constexpr int kAhead = (\d+);", src).group(1))
+    assert "constexpr int kPairWarpTile = 32 * kPairStarts;" in src
+    npos = S + wmax - 1
+    nvec = (npos + 1) // 2
+    npre = min((S + ahead + 1) // 2, nvec)
+    loaded = set()
+    for v in range(npre):
+        loaded |= {2 * v, 2 * v + 1}
+    highest = npre - 1
     for w in range(1, wmax + 1):
-        b = w + S - 2
-        if b % 4 == 0 and b // 4 >= S // 4 and b // 4 < vec:
-            loaded |= set(range(b, b + 4))
+        pn = w + S - 2 + ahead
+        if pn % 2 == 0 and npre <= pn // 2 < nvec:
+            loaded |= {pn, pn + 1}
+            highest = max(highest, pn // 2)
         assert set(range(w - 1, w + S - 1)) <= loaded, (w, sorted(loaded))
-    last_vec = max([S // 4 - 1] + [(w + S - 2) // 4 for w in range(1, wmax + 1)
-                                    if (w + S - 2) % 4 == 0 and (w + S - 2) // 4 < vec])
-    top = (threads - 1) * (S // 4) + last_vec       # float4 index of the highest read
-    assert 4 * top + 3 < span
+    span = (32 * S + wmax - 1 + 3) // 4 * 4          # staged positions of a warp
+    nf4 = span // 2
+    f_top = 31 * S // 2 + highest                      # the last lane's highest logical float4
+    assert f_top < nf4
+    assert f_top + f_top // 4 < nf4 + nf4 // 4         # inside the padded array
