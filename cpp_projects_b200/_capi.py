@@ -145,6 +145,8 @@ _SIGNATURES = {
     "bfs_batch_create": (_I, [ctypes.POINTER(BatchDesc), ctypes.POINTER(_P)]),
     "bfs_batch_destroy": (_I, [_P]),
     "bfs_batch_run": (_I, [_P, _P, _P]),
+    "bfs_batch_submit": (_I, [_P, _P, _P]),
+    "bfs_batch_collect": (_I, [_P, _P]),
     "bfs_batch_run_host": (_I, [_P, _P, _P, _P]),
     "bfs_batch_counts": (_I, [_P, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
     "bfs_batch_beam_results": (_I, [_P, _I, _P, _P, _I, ctypes.POINTER(_I), ctypes.POINTER(_U32)]),

@@ -84,6 +84,19 @@ struct bfs_batch {
     cudaGraphExec_t hexec = nullptr;
     std::vector<const void*> hgraph_ptrs;   // host then device pointers it was captured for
     std::vector<cudaEvent_t> events;
+    // the asynchronous form (bfs_batch_submit / bfs_batch_collect): two sets
+    // of stage-1 buffers; the fields above hold set `active`, these the other
+    bfs_cand* cands_alt = nullptr;
+    int* tags_alt = nullptr;
+    unsigned* rec_alt = nullptr;
+    unsigned* d_count_alt = nullptr;
+    cudaGraph_t graph_alt = nullptr;
+    cudaGraphExec_t exec_alt = nullptr;
+    std::vector<const float*> graph_inputs_alt;
+    int active = 0;
+    cudaStream_t s1 = nullptr;               // stage-1 stream of submitted runs
+    cudaEvent_t ev_in = nullptr, ev_done[2] = {nullptr, nullptr};
+    int queue[2] = {0, 0}, qhead = 0, inflight = 0, next_set = 0;
     // results of the last run
     unsigned n_cands = 0, n_groups = 0;
     std::vector<bfs_cand> h_delegates;
@@ -93,6 +106,14 @@ struct bfs_batch {
         if (graph) cudaGraphDestroy(graph);
         if (hexec) cudaGraphExecDestroy(hexec);
         if (hgraph) cudaGraphDestroy(hgraph);
+        if (exec_alt) cudaGraphExecDestroy(exec_alt);
+        if (graph_alt) cudaGraphDestroy(graph_alt);
+        for (cudaEvent_t e : {ev_in, ev_done[0], ev_done[1]})
+            if (e) cudaEventDestroy(e);
+        if (s1) cudaStreamDestroy(s1);
+        for (void* p : {static_cast<void*>(cands_alt), static_cast<void*>(tags_alt), static_cast<void*>(rec_alt),
+                        static_cast<void*>(d_count_alt)})
+            if (p) cudaFree(p);
         for (cudaEvent_t e : events) cudaEventDestroy(e);
         for (auto* p : plans) bfs_fdmt_plan_destroy(p);
         for (void* p : {ws, static_cast<void*>(plane), static_cast<void*>(stats), static_cast<void*>(cands),
@@ -261,14 +282,14 @@ static bfs_status enqueue_stage1(bfs_batch* b, const float* const* d_inputs, cud
 
 static bfs_status batch_stage2(bfs_batch* b, void* stream);
 
-extern "C" bfs_status bfs_batch_run(bfs_batch* b, const float* const* d_inputs, void* stream) {
-    BFS_ARG(b && d_inputs, "null argument");
-    cudaStream_t s = as_stream(stream);
+// Stage 1 of one run on s: replayed from the CUDA graph of the current
+// buffer set when its inputs are the ones it was captured for (the first run
+// is eager: kernel attributes are set then), else captured anew.
+static bfs_status launch_stage1(bfs_batch* b, const float* const* d_inputs, cudaStream_t s) {
     const int nb = static_cast<int>(b->beams.size());
     bool same_inputs = b->exec && b->graph_inputs.size() == static_cast<size_t>(nb);
     for (int i = 0; same_inputs && i < nb; ++i) same_inputs = b->graph_inputs[i] == d_inputs[i];
     if (b->use_graph && b->runs >= 1 && !same_inputs) {
-        // (re)capture: the first run was eager (kernel attributes are set then)
         if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
         if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
         cudaStream_t cs;
@@ -293,6 +314,72 @@ extern "C" bfs_status bfs_batch_run(bfs_batch* b, const float* const* d_inputs, 
         if (st != BFS_OK) return st;
     }
     ++b->runs;
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_batch_run(bfs_batch* b, const float* const* d_inputs, void* stream) {
+    BFS_ARG(b && d_inputs, "null argument");
+    BFS_ARG(b->inflight == 0, "runs submitted with bfs_batch_submit are not collected yet");
+    bfs_status st = launch_stage1(b, d_inputs, as_stream(stream));
+    if (st != BFS_OK) return st;
+    return batch_stage2(b, stream);
+}
+
+// ---- the asynchronous form --------------------------------------------------
+// Makes buffer set k the one in the batch's stage-1 fields.
+static void use_set(bfs_batch* b, int k) {
+    if (b->active == k) return;
+    std::swap(b->cands, b->cands_alt);
+    std::swap(b->tags, b->tags_alt);
+    std::swap(b->rec, b->rec_alt);
+    std::swap(b->d_count, b->d_count_alt);
+    std::swap(b->graph, b->graph_alt);
+    std::swap(b->exec, b->exec_alt);
+    std::swap(b->graph_inputs, b->graph_inputs_alt);
+    b->active = k;
+}
+
+// The second buffer set, the stage-1 stream and the events (first submit).
+static bfs_status ensure_async(bfs_batch* b) {
+    if (b->s1) return BFS_OK;
+    const size_t cap = b->capacity;
+    BFS_CUDA(cudaMalloc(&b->cands_alt, cap * sizeof(bfs_cand)));
+    if (!b->ordered) BFS_CUDA(cudaMalloc(&b->tags_alt, cap * sizeof(int)));
+    if (b->ordered) BFS_CUDA(cudaMalloc(&b->rec_alt, sizeof(unsigned) * 2 * b->nrec));
+    BFS_CUDA(cudaMalloc(&b->d_count_alt, sizeof(unsigned)));
+    BFS_CUDA(cudaEventCreateWithFlags(&b->ev_in, cudaEventDisableTiming));
+    for (auto& e : b->ev_done) BFS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    BFS_CUDA(cudaStreamCreateWithFlags(&b->s1, cudaStreamNonBlocking));
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_batch_submit(bfs_batch* b, const float* const* d_inputs, void* stream) {
+    BFS_ARG(b && d_inputs, "null argument");
+    BFS_ARG(b->inflight < 2, "two runs are in flight: collect one first");
+    bfs_status st = ensure_async(b);
+    if (st != BFS_OK) return st;
+    const int k = b->next_set;
+    use_set(b, k);
+    // the inputs are ready once the caller's stream reaches this point
+    BFS_CUDA(cudaEventRecord(b->ev_in, as_stream(stream)));
+    BFS_CUDA(cudaStreamWaitEvent(b->s1, b->ev_in, 0));
+    st = launch_stage1(b, d_inputs, b->s1);
+    if (st != BFS_OK) return st;
+    BFS_CUDA(cudaEventRecord(b->ev_done[k], b->s1));
+    b->queue[(b->qhead + b->inflight) % 2] = k;
+    ++b->inflight;
+    b->next_set ^= 1;
+    return BFS_OK;
+}
+
+extern "C" bfs_status bfs_batch_collect(bfs_batch* b, void* stream) {
+    BFS_ARG(b != nullptr, "null argument");
+    BFS_ARG(b->inflight > 0, "no submitted run to collect");
+    const int k = b->queue[b->qhead];
+    use_set(b, k);
+    BFS_CUDA(cudaStreamWaitEvent(as_stream(stream), b->ev_done[k], 0));
+    b->qhead ^= 1;
+    --b->inflight;
     return batch_stage2(b, stream);
 }
 
@@ -330,6 +417,7 @@ static bfs_status enqueue_host_stage1(bfs_batch* b, const float* const* h_inputs
 extern "C" bfs_status bfs_batch_run_host(bfs_batch* b, const float* const* h_inputs,
                                          float* const* d_inputs, void* stream) {
     BFS_ARG(b && h_inputs && d_inputs, "null argument");
+    BFS_ARG(b->inflight == 0, "runs submitted with bfs_batch_submit are not collected yet");
     cudaStream_t s = as_stream(stream);
     const int nb = static_cast<int>(b->beams.size());
     for (int i = 0; i < nb; ++i) BFS_ARG(h_inputs[i] && d_inputs[i], "beam %d: null input pointer", i);

@@ -11,6 +11,7 @@ the batch.
 """
 from __future__ import annotations
 
+import ctypes
 from dataclasses import dataclass
 
 import numpy as np
@@ -209,6 +210,26 @@ class BatchedSearch:
         for i, x in enumerate(inputs):
             self._ptrs[i] = dev_ptr(x, torch.float32, "input")
         self._capi.call("bfs_batch_run", self._h, self._ptrs, stream_handle(stream))
+        return self._results()
+
+    def submit(self, inputs: list[torch.Tensor], stream=None) -> None:
+        """Start one run (FDMT + statistics + boxcar of every beam) without
+        waiting; at most two runs in flight.  The tensors must stay unchanged
+        until the run is collected."""
+        from ._tensors import dev_ptr, stream_handle
+        if len(inputs) != len(self.shapes):
+            raise ValueError("one input per beam")
+        ptrs = (ctypes.c_void_p * len(inputs))()
+        for i, (x, sh) in enumerate(zip(inputs, self.shapes)):
+            if x.numel() != sh.nchan * sh.nsamp:
+                raise ValueError(f"beam {i}: input must hold {sh.nchan}x{sh.nsamp} floats")
+            ptrs[i] = dev_ptr(x, torch.float32, f"inputs[{i}]")
+        self._capi.call("bfs_batch_submit", self._h, ptrs, stream_handle(stream))
+
+    def collect(self, stream=None) -> list[BeamResult]:
+        """Finish the oldest submitted run (sort, clustering, delegates)."""
+        from ._tensors import stream_handle
+        self._capi.call("bfs_batch_collect", self._h, stream_handle(stream))
         return self._results()
 
     def run_host(self, host_inputs: list[torch.Tensor], dev_inputs: list[torch.Tensor],

@@ -358,6 +358,18 @@ bfs_status bfs_batch_run(bfs_batch* batch, const float* const* d_inputs, void* s
  * Synchronises `stream`. */
 bfs_status bfs_batch_run_host(bfs_batch* batch, const float* const* h_inputs,
                               float* const* d_inputs, void* stream);
+/* The asynchronous form (no reference counterpart): bfs_batch_submit
+ * enqueues one run's FDMT + statistics + boxcar of every beam on an internal
+ * stream (after the work already on `stream`, which makes the inputs ready)
+ * and returns; bfs_batch_collect waits for the oldest submitted run and does
+ * its sort, clustering and delegates on `stream`, leaving its results for
+ * bfs_batch_counts / bfs_batch_beam_results as bfs_batch_run does.  At most
+ * two runs are in flight (two candidate buffers), so submit(i + 1) before
+ * collect(i) overlaps run i's clustering with run i + 1's FDMT.  The inputs
+ * of a run must stay unchanged until it is collected.  bfs_batch_run and
+ * bfs_batch_run_host refuse to start while runs are in flight. */
+bfs_status bfs_batch_submit(bfs_batch* batch, const float* const* d_inputs, void* stream);
+bfs_status bfs_batch_collect(bfs_batch* batch, void* stream);
 bfs_status bfs_batch_counts(const bfs_batch* batch, uint32_t* n_cands, uint32_t* n_groups);
 /* Host copies of one beam's delegates (cap entries) and group sizes. */
 bfs_status bfs_batch_beam_results(const bfs_batch* batch, int beam, bfs_cand* delegates,

@@ -76,3 +76,38 @@ def test_explicit_schedules_equal_autotuned(cuda):
         assert np.array_equal(g.delegates.view(np.uint32).reshape(-1), w.delegates.view(np.uint32).reshape(-1))
     with pytest.raises(ValueError):
         SearchPipeline(shapes, device=cuda, schedules=scheds[:1])
+
+
+def test_submit_collect_equals_run(cuda):
+    """The asynchronous form (submit run i + 1 before collecting run i, two
+    candidate buffers) returns for every run exactly what bfs_batch_run
+    returns, with inputs alternating between two sets; a third run in flight
+    and a synchronous run while runs are in flight are refused."""
+    from cpp_projects_b200 import BfsError
+    beams = _beams()
+    shapes = [BeamShape(b.nchan, b.nsamp, b.fmin, b.fmax, b.max_dt) for b in beams]
+    ins = [[device_filterbank(b.nchan, b.nsamp, b.fmin, b.fmax, b.seed + 50 * k, b.pulses, cuda) for b in beams]
+           for k in range(2)]
+    batch = BatchedSearch(shapes, thr=6.0, capacity=1 << 22)
+    want = [batch.run(ins[0]), batch.run(ins[1])]
+    order = [0, 1, 0, 1, 0]
+    batch.submit(ins[order[0]])
+    for i, k in enumerate(order):
+        if i + 1 < len(order):
+            batch.submit(ins[order[i + 1]])
+        got = batch.collect()
+        for w, g in zip(want[k], got):
+            assert g.n_candidates == w.n_candidates, (i, k)
+            assert np.array_equal(g.delegates.view(np.uint32).reshape(-1), w.delegates.view(np.uint32).reshape(-1))
+            assert np.array_equal(g.group_sizes, w.group_sizes)
+    batch.submit(ins[0])
+    batch.submit(ins[1])
+    with pytest.raises(BfsError):
+        batch.submit(ins[0])
+    with pytest.raises(BfsError):
+        batch.run(ins[0])
+    for k in (0, 1):
+        got = batch.collect()
+        assert [g.n_candidates for g in got] == [w.n_candidates for w in want[k]]
+    with pytest.raises(BfsError):
+        batch.collect()
