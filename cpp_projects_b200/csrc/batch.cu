@@ -97,6 +97,16 @@ struct bfs_batch {
     cudaStream_t s1 = nullptr;               // stage-1 stream of submitted runs
     cudaEvent_t ev_in = nullptr, ev_done[2] = {nullptr, nullptr};
     int queue[2] = {0, 0}, qhead = 0, inflight = 0, next_set = 0;
+    // stage 1 in kLanes lanes (branches of the graph): lane l > 0 has its own
+    // plane, statistics and FDMT workspace (lane 0 uses the ones above);
+    // beam i runs in lane lane_of[i]
+    static constexpr int kLanes = 2;
+    float* lane_plane[kLanes] = {};
+    float* lane_stats[kLanes] = {};
+    void* lane_ws[kLanes] = {};
+    std::vector<int> lane_of;
+    cudaStream_t lane_s[kLanes] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[kLanes] = {};
     // results of the last run
     unsigned n_cands = 0, n_groups = 0;
     std::vector<bfs_cand> h_delegates;
@@ -111,6 +121,15 @@ struct bfs_batch {
         for (cudaEvent_t e : {ev_in, ev_done[0], ev_done[1]})
             if (e) cudaEventDestroy(e);
         if (s1) cudaStreamDestroy(s1);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        for (int l = 0; l < kLanes; ++l) {
+            if (ev_join[l]) cudaEventDestroy(ev_join[l]);
+            if (lane_s[l]) cudaStreamDestroy(lane_s[l]);
+            if (l > 0) {
+                for (void* p : {static_cast<void*>(lane_plane[l]), static_cast<void*>(lane_stats[l]), lane_ws[l]})
+                    if (p) cudaFree(p);
+            }
+        }
         for (void* p : {static_cast<void*>(cands_alt), static_cast<void*>(tags_alt), static_cast<void*>(rec_alt),
                         static_cast<void*>(d_count_alt)})
             if (p) cudaFree(p);
@@ -235,6 +254,31 @@ extern "C" bfs_status bfs_batch_create(const bfs_batch_desc* desc, bfs_batch** o
     BFS_CUDA(cudaMalloc(&b->ws, b->ws_bytes ? b->ws_bytes : 256));
     BFS_CUDA(cudaMalloc(&b->plane, plane * sizeof(float)));
     BFS_CUDA(cudaMalloc(&b->stats, 2 * static_cast<size_t>(b->max_rows) * sizeof(float)));
+    // lanes: beams in order, each to the lane with the least work so far
+    constexpr int L = bfs_batch::kLanes;
+    b->lane_of.assign(b->beams.size(), 0);
+    b->lane_plane[0] = b->plane;
+    b->lane_stats[0] = b->stats;
+    b->lane_ws[0] = b->ws;
+    if (b->beams.size() >= 2) {
+        double work[L] = {};
+        for (size_t i = 0; i < b->beams.size(); ++i) {
+            int l = 0;
+            for (int k = 1; k < L; ++k)
+                if (work[k] < work[l]) l = k;
+            b->lane_of[i] = l;
+            work[l] += static_cast<double>(b->beams[i].max_dt) * b->beams[i].ncols +
+                       static_cast<double>(b->beams[i].nchan) * b->beams[i].ncols;
+        }
+        for (int l = 1; l < L; ++l) {
+            BFS_CUDA(cudaMalloc(&b->lane_ws[l], b->ws_bytes ? b->ws_bytes : 256));
+            BFS_CUDA(cudaMalloc(&b->lane_plane[l], plane * sizeof(float)));
+            BFS_CUDA(cudaMalloc(&b->lane_stats[l], 2 * static_cast<size_t>(b->max_rows) * sizeof(float)));
+        }
+        for (auto& t : b->lane_s) BFS_CUDA(cudaStreamCreateWithFlags(&t, cudaStreamNonBlocking));
+        BFS_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+        for (auto& e : b->ev_join) BFS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
     const size_t cap = b->capacity;
     BFS_CUDA(cudaMalloc(&b->cands, cap * sizeof(bfs_cand)));
     if (!b->ordered) BFS_CUDA(cudaMalloc(&b->tags, cap * sizeof(int)));
@@ -255,27 +299,52 @@ extern "C" bfs_status bfs_batch_destroy(bfs_batch* b) {
 
 // Boxcar of beam i over the shared plane: ordered blocks + records, or
 // atomic appends tagged with the beam.
-static bfs_status beam_boxcar(bfs_batch* b, int i, cudaStream_t s) {
+static bfs_status beam_boxcar(bfs_batch* b, int i, const float* plane, const float* stats, cudaStream_t s) {
     const bfs_fdmt_desc& d = b->beams[i];
     if (b->ordered)
-        return launch_boxcar_ordered(b->plane, d.max_dt, d.ncols, b->stats, b->thr, nullptr, b->widths_mode,
+        return launch_boxcar_ordered(plane, d.max_dt, d.ncols, stats, b->thr, nullptr, b->widths_mode,
                                      b->param, 0, b->cands, b->capacity, b->d_count, b->rec + b->rec0[i],
                                      b->rec + b->nrec + b->rec0[i], s);
-    return launch_boxcar(b->plane, d.max_dt, d.ncols, b->stats, b->thr, nullptr, b->widths_mode, b->param, 0,
+    return launch_boxcar(plane, d.max_dt, d.ncols, stats, b->thr, nullptr, b->widths_mode, b->param, 0,
                          b->cands, b->capacity, b->d_count, s, i, b->tags);
 }
 
+// FDMT, row statistics and boxcar of beam i with one lane's plane,
+// statistics and workspace.
+static bfs_status beam_stage1(bfs_batch* b, int i, const float* d_in, float* plane, float* stats, void* ws,
+                              cudaStream_t s) {
+    const bfs_fdmt_desc& d = b->beams[i];
+    bfs_status st = bfs_fdmt_execute_ws(b->plans[i], d_in, plane, 0, ws, b->ws_bytes, s);
+    if (st != BFS_OK) return st;
+    st = launch_row_stats(plane, d.max_dt, d.ncols, stats, 0, s);
+    if (st != BFS_OK) return st;
+    return beam_boxcar(b, i, plane, stats, s);
+}
+
 // Stage 1 for every beam, enqueued on s (captured or eager).
+// With several lanes the beams fork from s into the lanes' streams (branches of
+// the captured graph) and join back; the candidates of both lanes go to the
+// one candidate array (their order is set by the records or the sort).
 static bfs_status enqueue_stage1(bfs_batch* b, const float* const* d_inputs, cudaStream_t s) {
     BFS_CUDA(cudaMemsetAsync(b->d_count, 0, sizeof(unsigned), s));
+    if (!b->lane_s[0]) {
+        for (size_t i = 0; i < b->beams.size(); ++i) {
+            bfs_status st = beam_stage1(b, static_cast<int>(i), d_inputs[i], b->plane, b->stats, b->ws, s);
+            if (st != BFS_OK) return st;
+        }
+        return BFS_OK;
+    }
+    BFS_CUDA(cudaEventRecord(b->ev_fork, s));
+    for (cudaStream_t t : b->lane_s) BFS_CUDA(cudaStreamWaitEvent(t, b->ev_fork, 0));
     for (size_t i = 0; i < b->beams.size(); ++i) {
-        const bfs_fdmt_desc& d = b->beams[i];
-        bfs_status st = bfs_fdmt_execute_ws(b->plans[i], d_inputs[i], b->plane, 0, b->ws, b->ws_bytes, s);
+        const int l = b->lane_of[i];
+        bfs_status st = beam_stage1(b, static_cast<int>(i), d_inputs[i], b->lane_plane[l], b->lane_stats[l],
+                                    b->lane_ws[l], b->lane_s[l]);
         if (st != BFS_OK) return st;
-        st = launch_row_stats(b->plane, d.max_dt, d.ncols, b->stats, 0, s);
-        if (st != BFS_OK) return st;
-        st = beam_boxcar(b, static_cast<int>(i), s);
-        if (st != BFS_OK) return st;
+    }
+    for (int l = 0; l < bfs_batch::kLanes; ++l) {
+        BFS_CUDA(cudaEventRecord(b->ev_join[l], b->lane_s[l]));
+        BFS_CUDA(cudaStreamWaitEvent(s, b->ev_join[l], 0));
     }
     return BFS_OK;
 }
@@ -401,11 +470,7 @@ static bfs_status enqueue_host_stage1(bfs_batch* b, const float* const* h_inputs
         BFS_CUDA(cudaMemcpyAsync(d_inputs[i], h_inputs[i], bytes, cudaMemcpyHostToDevice, cp));
         BFS_CUDA(cudaEventRecord(b->events[i], cp));
         BFS_CUDA(cudaStreamWaitEvent(cs, b->events[i], 0));
-        bfs_status st = bfs_fdmt_execute_ws(b->plans[i], d_inputs[i], b->plane, 0, b->ws, b->ws_bytes, cs);
-        if (st != BFS_OK) return st;
-        st = launch_row_stats(b->plane, d.max_dt, d.ncols, b->stats, 0, cs);
-        if (st != BFS_OK) return st;
-        st = beam_boxcar(b, i, cs);
+        bfs_status st = beam_stage1(b, i, d_inputs[i], b->plane, b->stats, b->ws, cs);
         if (st != BFS_OK) return st;
     }
     // the copy stream joins the compute stream (required to end a capture)
