@@ -250,19 +250,24 @@ __device__ __forceinline__ void pair_widths(const float4* __restrict__ win4, int
         const int code = (MODE == 1) ? w - 1 : 31 - __clz(w);
         // windows inside the row: starts j < inside
         const int inside = edge ? cols - (tb + w - 1) : S;
+        // windows over the bound: a bit each (one code path for all of them)
+        unsigned over = 0;
 #pragma unroll
-        for (int j = 0; j < S; ++j) {
-            if (!(hm[j] > lim) || j >= inside) continue;
+        for (int k = 0; k < 2 * S; ++k)
+            if (h[k] > lim && (k >> 1) < inside) over |= 1u << k;
+#pragma unroll 1
+        while (over) {
+            const int k = __ffs(over) - 1;
+            over &= over - 1;
+            float sj = h[0];
 #pragma unroll
-            for (int r = 0; r < 2; ++r) {
-                const float sj = h[2 * j + r];
-                if (sj > lim) {
-                    const float q = snr_fast ? __fdividef(sj, sq) : __fdiv_rn(sj, sq);
-                    if (q > thr) {
-                        pass[r] |= 1ull << (8 * j + code);
-                        snr[64 * r + 8 * j + code] = q;
-                    }
-                }
+            for (int i = 1; i < 2 * S; ++i)
+                if (i == k) sj = h[i];
+            const float q = snr_fast ? __fdividef(sj, sq) : __fdiv_rn(sj, sq);
+            if (q > thr) {
+                const int r = k & 1, bit = 8 * (k >> 1) + code;
+                pass[r] |= 1ull << bit;
+                snr[64 * r + bit] = q;
             }
         }
     }
