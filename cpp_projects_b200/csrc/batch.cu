@@ -112,6 +112,11 @@ struct bfs_batch {
     std::vector<bfs_cand> h_delegates;
     std::vector<int> h_delegate_beam, h_delegate_size, h_beam_first, h_beam_count, h_beam_cands;
     ~bfs_batch() {
+        // work still queued on the batch's own streams (a submitted run that
+        // was never collected) must finish before its buffers are freed
+        if (s1) cudaStreamSynchronize(s1);
+        for (cudaStream_t t : lane_s)
+            if (t) cudaStreamSynchronize(t);
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (hexec) cudaGraphExecDestroy(hexec);

@@ -111,3 +111,18 @@ def test_submit_collect_equals_run(cuda):
         assert [g.n_candidates for g in got] == [w.n_candidates for w in want[k]]
     with pytest.raises(BfsError):
         batch.collect()
+
+
+def test_destroy_with_a_run_in_flight(cuda):
+    """A batch destroyed with a submitted run never collected waits for that
+    run's kernels before freeing their buffers; the device stays usable."""
+    beams = _beams()[:2]
+    shapes = [BeamShape(b.nchan, b.nsamp, b.fmin, b.fmax, b.max_dt) for b in beams]
+    ins = [device_filterbank(b.nchan, b.nsamp, b.fmin, b.fmax, b.seed, b.pulses, cuda) for b in beams]
+    batch = BatchedSearch(shapes, thr=6.0, capacity=1 << 22)
+    want = batch.run(ins)
+    batch.submit(ins)
+    del batch
+    torch.cuda.synchronize()
+    again = BatchedSearch(shapes, thr=6.0, capacity=1 << 22).run(ins)
+    assert [g.n_candidates for g in again] == [w.n_candidates for w in want]
