@@ -516,9 +516,23 @@ def run_ours(args):
         wall = time.perf_counter() - t0
         barrier()
         e2e_ms = max_over_ranks(f0.elapsed_time(f1) / args.steps)
+        # the bound: the same host buffers copied to the device and nothing else
+        copy_ms = []
+        for _ in range(3):
+            f0.record()
+            for h, x in zip(host, inputs):
+                x.copy_(h, non_blocking=True)
+            f1.record()
+            torch.cuda.synchronize()
+            copy_ms.append(f0.elapsed_time(f1))
+        copy_ms = max_over_ranks(min(copy_ms[1:]))
         e2e = {"value": units / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h // args.steps, "ms_per_step": e2e_ms,
-               "wall_ms_per_step": 1e3 * wall / args.steps}
+               "wall_ms_per_step": 1e3 * wall / args.steps,
+               "h2d_gbs": h2d / e2e_ms / 1e6,
+               "copy_only": {"ms_per_step": copy_ms, "gbs": h2d / copy_ms / 1e6,
+                             "frac": copy_ms / e2e_ms,
+                             "what": "the step's host inputs copied to the device alone (pinned, one stream)"}}
         del host
 
     # ---- CPU baseline (rank 0, N=1 only) -------------------------------------
