@@ -1901,8 +1901,7 @@ extern "C" bfs_status bfs_fdmt_execute_row_mask(bfs_fdmt_plan* plan, const float
 //
 // In host code the array's name is only a host-side stand-in, not a device
 // address, so the device address is looked up with cudaGetSymbolAddress once
-// per device (with that device current) on the first call made on it; that
-// first call should therefore come before any stream capture.  All calls
+// per device (with that device current) on the first call made on it.  All calls
 // share the one array and it keeps the previous call's contents: every byte a
 // call reads is written by that call first (tables copied in, planes fully
 // overwritten), so nothing needs clearing, but calls whose executions

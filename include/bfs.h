@@ -195,9 +195,9 @@ bfs_status bfs_fdmt_execute_row_mask(bfs_fdmt_plan* plan, const float* d_mask, i
  * and both ping-pong planes live in one 256 MiB static device array built
  * into the library (held by every GPU that loads it, until exit); a problem
  * needing more returns BFS_ERR_ARG.  The first call on each device looks the
- * array's device address up (cudaGetSymbolAddress), so make it before any
- * stream capture.  That address is kept for the life of the process, so do
- * not call cudaDeviceReset after using this entry point.  Calls share the
+ * array's device address up (cudaGetSymbolAddress) and keeps it for the life
+ * of the process, so do not call cudaDeviceReset after using this entry
+ * point.  Calls share the
  * array: calls that overlap on the GPU race.  Same output as
  * bfs_fdmt_execute (with b_ones != 0 too, d_in may then be NULL). */
 bfs_status bfs_fdmt_execute_noalloc(const bfs_fdmt_plan* plan, const float* d_in, float* d_out,
