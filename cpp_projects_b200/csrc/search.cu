@@ -37,12 +37,13 @@ constexpr int kMaxPow2Q = 16;
 constexpr int kMaxAllW = 4096;
 
 // stats[r] = mean, stats[rows + r] = std (mode 0) or population variance (mode 1)
-__global__ void __cluster_dims__(kStatCluster, 1, 1) __launch_bounds__(kStatThreads)
+// launched with clusters of gridDim.x CTAs (one cluster per row)
+__global__ void __launch_bounds__(kStatThreads)
 k_row_stats(const float* __restrict__ plane, int rows, int cols, float* __restrict__ stats,
-            int mode) {
+            int mode, int vec) {
     const int row = blockIdx.y;
     double s, q;
-    cluster_row_moments(plane + static_cast<size_t>(row) * cols, cols, s, q);
+    cluster_row_moments(plane + static_cast<size_t>(row) * cols, row, cols, vec != 0, s, q);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         const double mean = s / cols;
         double var = q / cols - mean * mean;
@@ -620,9 +621,29 @@ bfs_status launch_row_stats(const float* d_in, int rows, int cols, float* d_stat
     BFS_ARG(d_in && d_stats, "null argument");
     BFS_ARG(rows >= 1 && cols >= 1, "bad shape %dx%d", rows, cols);
     BFS_ARG(rows <= 65535, "rows > 65535 not supported");
-    dim3 grid(kStatCluster, rows);
-    k_row_stats<<<grid, kStatThreads, 0, s>>>(d_in, rows, cols, d_stats, mode);
-    BFS_LAUNCH_CHECK("k_row_stats");
+    // CTAs per row: doubled while the grid is under two waves of 256-thread
+    // CTAs (8 per SM) and every thread still reads >= 32 samples
+    int dev = 0, sms = 0;
+    BFS_CUDA(cudaGetDevice(&dev));
+    BFS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    int split = 1;
+    while (split < kStatMaxCluster && static_cast<long long>(rows) * split < 16LL * sms &&
+           cols / (2 * split) >= 32 * kStatThreads)
+        split *= 2;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(split, rows);
+    cfg.blockDim = dim3(kStatThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = split;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const int vec = (reinterpret_cast<uintptr_t>(d_in) & 15) == 0 ? 1 : 0;
+    BFS_CUDA(cudaLaunchKernelEx(&cfg, k_row_stats, d_in, rows, cols, d_stats, mode, vec));
     return BFS_OK;
 }
 
