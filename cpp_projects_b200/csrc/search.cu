@@ -156,12 +156,13 @@ struct WidthConsts {
 // sequential sums bit for bit.  Per width the warp first asks whether any
 // of its sums exceeds the width's lower bound of passing sums (a
 // three-input max tree and one vote); only then are exact quotients
-// evaluated.  Pass 1 keeps the passing windows as bits (start j, width code
-// c) -> bit 8 j + c, which orders them by (start, width); a warp scan of the
-// lanes' counts and one atomicAdd give the warp its block (row 2y's
-// candidates, then row 2y + 1's).  Warps with candidates then run the width
-// loop again (pass 2, the same packed adds) and write each passing window
-// at its position in the block.  The warps never wait for one another.
+// evaluated.  The width loop keeps the passing windows as bits (start j,
+// width code c) -> bit 8 j + c, which orders them by (start, width), and
+// each one's S/N in a per-lane array indexed like its bit; a warp scan of
+// the lanes' counts and one atomicAdd give the warp its block (row 2y's
+// candidates, then row 2y + 1's), and each lane writes its windows at their
+// positions in the block from the bits.  The warps never wait for one
+// another.
 // Record (row, warp tile i) = {first index, count} of row `row`'s block in
 // warp tile i (index row * ceil(cols / kPairWarpTile) + i), so a scan of
 // the counts in record order gives every candidate its canonical position
