@@ -228,3 +228,24 @@ def test_config0_search_chain_finds_the_pulse(cuda):
     np.testing.assert_array_equal(cl.perm.cpu().numpy(), perm)
     np.testing.assert_array_equal(cl.offsets.cpu().numpy(), offs)
     np.testing.assert_array_equal(cl.delegates.cpu().numpy(), dl)
+
+
+@pytest.mark.parametrize("rows,cols", [(4096, 8192), (256, 131072), (1024, 16749), (33, 4099), (5, 3)])
+def test_row_stats_do_not_depend_on_the_planes_address(cuda, rows, cols):
+    """The row statistics' order of additions follows each row's plane index,
+    so a plane 4 bytes past a 16-byte boundary (scalar loads) gives the same
+    bits as its 16-byte aligned copy (16-byte loads), and both stay within
+    1 ulp of the oracle's FP64 sums."""
+    rng = np.random.default_rng(rows + cols)
+    x = (rng.standard_normal(rows * cols + 1) * 2.0 + 0.25).astype(np.float32)
+    flat = torch.from_numpy(x).to(cuda)
+    shifted = flat[1:].view(rows, cols)                # 4 bytes past the allocation's start
+    assert shifted.data_ptr() % 16 == 4
+    aligned = shifted.clone()
+    assert aligned.data_ptr() % 16 == 0
+    st_s = search.row_stats(shifted).cpu().numpy()
+    st_a = search.row_stats(aligned).cpu().numpy()
+    assert np.array_equal(st_s.view(np.int32), st_a.view(np.int32))
+    _, m, s = pyoracle.norm_rows(x[1:].reshape(rows, cols))
+    assert np.abs(st_a[:rows].view(np.int32) - m.view(np.int32)).max() <= 1
+    assert np.abs(st_a[rows:].view(np.int32) - s.view(np.int32)).max() <= 1

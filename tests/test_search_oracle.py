@@ -113,3 +113,50 @@ def test_boxcar_pair_window_schedule(wmax):
     f_top = 31 * S // 2 + highest                      # the last lane's highest logical float4
     assert f_top < nf4
     assert f_top + f_top // 4 < nf4 + nf4 // 4         # inside the padded array
+
+
+@pytest.mark.parametrize("rows,cols", [(4096, 32768), (256, 131072), (1024, 16749), (512, 24485), (3, 5),
+                                       (7, 1), (2, 8193), (65535, 3)])
+def test_row_stats_partition(rows, cols):
+    """k_row_stats' work split (emulated from the constants in its sources):
+    the cluster size per row (1..kStatMaxCluster, doubled while the grid is
+    under two waves of 8 CTAs per SM and each thread keeps >= 32 samples),
+    each CTA's range (a multiple of 4 samples), the scalars before the first
+    4-sample piece whose plane index is a multiple of 4, the pieces strided
+    over the threads and the tail scalars: every sample of a row is added
+    exactly once, and each piece starts on a 16-byte boundary of a 16-byte
+    aligned plane.  The assignment depends on the plane index only."""
+    root = Path(__file__).resolve().parent.parent / "cpp_projects_b200" / "csrc"
+    common = (root / "search_common.cuh").read_text()
+    T = int(re.search(r"constexpr int kStatThreads = (\d+);", common).group(1))
+    maxc = int(re.search(r"constexpr int kStatMaxCluster = (\d+);", common).group(1))
+    src = (root / "search.cu").read_text()
+    assert "static_cast<long long>(rows) * split < 16LL * sms" in src
+    assert "cols / (2 * split) >= 32 * kStatThreads" in src
+    sms = 148
+    split = 1
+    while split < maxc and rows * split < 16 * sms and cols // (2 * split) >= 32 * T:
+        split *= 2
+    assert split & (split - 1) == 0 and split <= 8   # a portable cluster size
+    for r in sorted({0, 1, 2, 3, rows - 1} & set(range(rows))):
+        seen = np.zeros(cols, np.int64)
+        per = ((cols + split - 1) // split + 3) & ~3
+        for rank in range(split):
+            beg = min(cols, rank * per)
+            end = min(cols, beg + per)
+            phase = (r * cols + beg) & 3
+            lead = min(end - beg, (4 - phase) & 3)
+            n4 = (end - beg - lead) >> 2
+            tail = end - beg - lead - 4 * n4
+            assert 0 <= lead < 4 and 0 <= tail < 4 and lead + 4 <= T
+            if n4:
+                assert (r * cols + beg + lead) % 4 == 0   # 16-byte aligned given an aligned plane
+                base = beg + lead + 4 * np.arange(n4)
+                for j in range(4):
+                    np.add.at(seen, base + j, 1)
+            for k in range(T):
+                if k < lead:
+                    seen[beg + k] += 1
+                elif 4 <= k < 4 + tail:
+                    seen[beg + lead + 4 * n4 + (k - 4)] += 1
+        assert (seen == 1).all(), (r, split)
