@@ -1361,15 +1361,18 @@ static bfs_status tune_fdmt(const bfs_fdmt_desc& base, TuneVal* best) {
     cands.push_back({0, 0, 1, 0, 0});
     for (int k : {2, 3, 4, 5})
         for (int tile : {256, 512}) cands.push_back({k, tile, 1, 0, 0});
-    // fused merge segments of 2, 3 or 4 levels x 16 or 32 rows per tile (FP32):
-    // after a head, or forming level 0 in the first segment with one or two
-    // input buffers per CTA (one buffer: half the input staging, so two CTAs
-    // share an SM where two buffers allow one)
+    // fused merge segments of 2, 3 or 4 levels x 16-32 rows per tile (FP32):
+    // after a head (16 or 32 rows), or forming level 0 in the first segment
+    // with one or two input buffers per CTA (one buffer: half the input
+    // staging, so two CTAs share an SM where two buffers allow one; 24 and 28
+    // rows bring a single-buffered input segment under half an SM's shared
+    // memory)
     if (base.precision == BFS_PREC_F32)
         for (int seg : {2, 3, 4})
-            for (int rows : {16, 32}) {
+            for (int rows : {16, 24, 28, 32}) {
                 for (int flags : {0, static_cast<int>(BFS_SEG_SINGLE_BUFFER)}) cands.push_back({0, 0, seg, rows, flags});
-                for (int k : {2, 3, 4}) cands.push_back({k, 256, seg, rows, 0});
+                if (rows == 16 || rows == 32)
+                    for (int k : {2, 3, 4}) cands.push_back({k, 256, seg, rows, 0});
             }
     const size_t in_n = static_cast<size_t>(base.nchan) * base.ncols;
     const size_t out_n = static_cast<size_t>(base.max_dt) * base.ncols;

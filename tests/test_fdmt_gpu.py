@@ -99,7 +99,7 @@ def test_autotune_returns_a_valid_choice(cuda):
     d = _capi.FdmtDesc(fmin=1200.0, fmax=1600.0, nchan=1024, ncols=65536, max_dt=1024)
     t, ms2 = autotune_desc(d)
     assert (t.fuse_depth, t.head_tile) == (depth, tile) and ms2 == ms
-    assert t.seg_levels in (1, 2, 3, 4) and t.seg_rows in ((0,) if t.seg_levels == 1 else (16, 32))
+    assert t.seg_levels in (1, 2, 3, 4) and t.seg_rows in ((0,) if t.seg_levels == 1 else (16, 24, 28, 32))
     # the tuned plan is the one the autotuning plan request builds, and bit-exact
     x = np.random.default_rng(7).standard_normal((1024, 4096)).astype(np.float32)
     f = CFdmtGpu(1200.0, 1600.0, 1024, 4096, 1024, fuse_depth=t.fuse_depth, head_tile=t.head_tile,

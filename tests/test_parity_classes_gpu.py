@@ -36,17 +36,15 @@ def _want4096(ncols):
     return pyoracle.fdmt_f32(*BAND, _x4096(ncols), 4096, ncols, 4096)
 
 
-# (fuse_depth, head_tile, seg_levels, seg_rows): the tuned choice, one pass per
-# level, fused segments of 2 / 3 / 4 levels with 16 or 32 rows per tile, with
-# and without a head, the wide head tile
 # (fuse_depth, head_tile, seg_levels, seg_rows, seg_threads, seg_flags): the
-# tuned choice, one pass per level, fused segments of 2 / 3 / 4 levels with 16
-# or 32 rows per tile, with and without a head (without: the first segment
-# forms level 0 from the channels), the wide head tile, CTAs of 256 / 512 /
-# 1024 threads, one input buffer per CTA
+# tuned choice, one pass per level, fused segments of 2 / 3 / 4 levels with
+# 16, 24, 28 or 32 rows per tile, with and without a head (without: the first
+# segment forms level 0 from the channels), the wide head tile, CTAs of 256 /
+# 512 / 1024 threads, one input buffer per CTA
 SCHEDULES = [(-2, 0, 0, 0, 0, 0), (3, 256, 1, 0, 0, 0), (3, 512, 3, 32, 0, 0), (3, 256, 4, 16, 0, 0),
              (0, 0, 3, 16, 0, 0), (4, 256, 2, 16, 0, 0), (2, 256, 3, 32, 0, 0), (0, 0, 4, 32, 1024, 0),
-             (0, 0, 3, 32, 256, 1), (3, 256, 3, 16, 512, 1)]
+             (0, 0, 3, 32, 256, 1), (3, 256, 3, 16, 512, 1), (0, 0, 3, 28, 0, 1), (0, 0, 4, 24, 0, 1),
+             (0, 0, 3, 28, 0, 0)]
 
 
 @pytest.mark.parametrize("ncols", [8192, 5003])

@@ -221,6 +221,8 @@ def test_segment_emulation_matches_oracle(case):
     (1100.0, 1500.0, 128, 513, 100, 0, 4, 0),
     (1200.0, 1600.0, 99, 531, 99, 0, 2, 8),      # odd channel count: a carried level-1 row
     (1200.0, 1328.0, 64, 1031, 200, 0, 3, 32),   # max delay > channels: 5 level-0 rows per channel
+    (1200.0, 1600.0, 128, 900, 128, 0, 3, 28),   # 28 rows per tile (a row tile count not a power of 2)
+    (1200.0, 1600.0, 96, 777, 96, 0, 4, 24),     # 24 rows per tile, 4 levels
 ])
 def test_input_segment_emulation_matches_oracle(case):
     """No head: the first segment stages the channels and forms level 0 in
