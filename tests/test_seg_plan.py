@@ -17,10 +17,10 @@ TILE_INTS = 8
 PASS_INTS = 13
 
 
-def plan_passes(fmin, fmax, nchan, ncols, max_dt, fuse, seg_levels=0, seg_rows=0):
+def plan_passes(fmin, fmax, nchan, ncols, max_dt, fuse, seg_levels=0, seg_rows=0, seg_flags=0):
     """(head depth, rows per level, passes): each pass is (params, tiles, ent)."""
     desc = _capi.FdmtDesc(fmin=fmin, fmax=fmax, nchan=nchan, ncols=ncols, max_dt=max_dt,
-                          fuse_depth=fuse, seg_levels=seg_levels, seg_rows=seg_rows)
+                          fuse_depth=fuse, seg_levels=seg_levels, seg_rows=seg_rows, seg_flags=seg_flags)
     plan = ctypes.c_void_p()
     _capi.call("bfs_fdmt_plan_create_host", ctypes.byref(desc), ctypes.byref(plan))
     try:
@@ -265,6 +265,56 @@ def test_segment_geometry_at_search_shapes():
                         seen[q[:, 3]] += 1
                     e = e[n[lev]:]
             assert np.all(seen == 1)
+
+
+@pytest.mark.parametrize("rows_per_tile", [24, 28])
+@pytest.mark.parametrize("levels", [3, 4])
+def test_input_segment_geometry_at_search_shapes(rows_per_tile, levels):
+    """Single-buffered input segments of 24 / 28 rows per tile (autotuner
+    candidates) at the batched search's channel counts: the shared memory
+    fits an SM (at 28 rows and 3 levels, half of one, so two CTAs share it),
+    the channels staged are inside the input, every level-0 row's look-back
+    of r samples and its 32 nc positions stay inside buffer X, its
+    destination inside buffer Y, every merge inside its buffers, and each
+    output row of the pass is written once."""
+    for nchan in (256, 512, 1024, 4096):
+        k, rows, passes = plan_passes(1200.0, 1600.0, nchan, 1 << 17, nchan, 0, levels, rows_per_tile,
+                                      _capi.BFS_SEG_SINGLE_BUFFER)
+        pr, tiles, ent = passes[0]
+        assert k == 0 and int(pr[12]) >= 1 and len(tiles)   # an input segment
+        l0, l1, G, TT, nc, pitch, rx, ry, max_ent = (int(v) for v in pr[:9])
+        assert l0 == 0 and G in (rows_per_tile, 16) and nc in (9, 10, 12)
+        smem = (((rx + 2) + ry + 2) * pitch) * 4 + max_ent * 16
+        assert smem <= 227 * 1024
+        if rows_per_tile == 28 and levels == 3:
+            assert smem <= 113 * 1024
+        m = l1 - l0
+        seen = np.zeros(int(rows[l1]), np.int64)
+        for tile in tiles:
+            e0, n = int(tile[0]), [int(v) for v in tile[1:2 + m + 1]]
+            e = ent[e0:]
+            inp = e[:n[0]]
+            assert inp[:, 0].min() >= 0 and inp[:, 0].max() < nchan
+            assert inp[:, 3].min() >= 0 and inp[:, 3].max() + 32 * nc <= (rx + 2) * pitch
+            e = e[n[0]:]
+            q = e[:n[1]]                                  # level-0 rows from the staged channels
+            r = (q[:, 3] >> 20) & 15
+            assert (q[:, 0] - r).min() >= 0 and q[:, 0].max() + 32 * nc <= (rx + 2) * pitch
+            assert (q[:, 3] & 0xFFFFF).max() + 32 * nc <= (ry + 2) * pitch
+            e = e[n[1]:]
+            for lev in range(2, m + 2):
+                q = e[:n[lev]]
+                last = lev == m + 1
+                span = TT if last else 32 * nc
+                below = ry if lev % 2 == 0 else rx
+                assert q[:, :2].min() >= 0 and q[:, :2].max() + span <= (below + 2) * pitch
+                if last:
+                    seen[q[:, 3]] += 1
+                else:
+                    above = rx if lev % 2 == 0 else ry
+                    assert q[:, 3].max() + span <= (above + 2) * pitch
+                e = e[n[lev]:]
+        assert np.all(seen == 1), nchan
 
 
 def test_segment_options_are_checked():
