@@ -89,7 +89,9 @@ typedef struct bfs_fdmt_desc {
     int seg_levels;    /* merge levels fused per HBM pass after the head (FP32 plans):
                           0: 3; 1: one pass per level; 2..6                              */
     int seg_rows;      /* output rows per tile of a fused pass (0: the most that keep
-                          two CTAs per SM, of 64 / 32 / 16)                              */
+                          two CTAs per SM, of 64 / 32 / 16; the autotuner also tries
+                          24 and 28, which fit a single-buffered input segment into
+                          half an SM's shared memory)                                    */
     int seg_threads;   /* threads per CTA of the fused passes: 256, 512, 1024 (0: 256
                           when two CTAs fit an SM, else 512)                             */
     int seg_flags;     /* BFS_SEG_SINGLE_BUFFER: one input buffer per CTA (the next
