@@ -327,3 +327,69 @@ def test_segment_options_are_checked():
         _capi.call("bfs_fdmt_plan_create_host", ctypes.byref(desc), ctypes.byref(plan))
     k, rows, passes = plan_passes(1200.0, 1600.0, 64, 500, 64, 2, seg_levels=1)
     assert all(len(t) == 0 for _, t, _ in passes) and len(passes) == rows.size - 1 - k
+
+
+def _check_pass_geometry(pr, tiles, ent, rows, nchan, single):
+    """The bounds k_fdmt_seg relies on, from one fused pass's tables: shared
+    memory within an SM, staged rows inside the input, every shared read and
+    write inside its buffer (level-0 rows of an input segment including their
+    look-back of r samples), each output row of the pass written once."""
+    l0, l1, G, TT, nc, pitch, rx, ry, max_ent = (int(v) for v in pr[:9])
+    r0c = int(pr[12])
+    xs = (rx + 2) * pitch                       # the X buffer in use (either of two, or the one)
+    smem = (((1 if single else 2) * (rx + 2) + ry + 2) * pitch) * 4 + (1 if single else 3) * max_ent * 16
+    assert smem <= 227 * 1024 and nc in (9, 10, 12)
+    m = l1 - l0 + (1 if r0c > 0 else 0)         # shared-memory levels + the one written to HBM
+    seen = np.zeros(int(rows[l1]), np.int64)
+    for tile in tiles:
+        e0, n = int(tile[0]), [int(v) for v in tile[1:2 + m]]
+        e = ent[e0:]
+        inp = e[:n[0]]
+        assert inp[:, 0].min() >= 0 and inp[:, 0].max() < (nchan if r0c > 0 else rows[l0])
+        assert inp[:, 3].min() >= 0 and inp[:, 3].max() + 32 * nc <= xs
+        e = e[n[0]:]
+        for lev in range(1, m + 1):
+            q = e[:n[lev]]
+            e = e[n[lev]:]
+            if len(q) == 0:
+                continue
+            below = rx if lev % 2 == 1 else ry
+            above = ry if lev % 2 == 1 else rx
+            if r0c > 0 and lev == 1:             # level 0 formed from the staged channels
+                r = (q[:, 3] >> 20) & 15
+                assert r.max() < r0c
+                assert (q[:, 0] - r).min() >= 0 and q[:, 0].max() + 32 * nc <= xs
+                assert (q[:, 3] & 0xFFFFF).max() + 32 * nc <= (ry + 2) * pitch
+                continue
+            span = TT if lev == m else 32 * nc
+            assert q[:, :2].min() >= 0 and q[:, :2].max() + span <= (below + 2) * pitch
+            if lev == m:
+                seen[q[:, 3]] += 1
+            else:
+                assert q[:, 3].min() >= 0 and q[:, 3].max() + span <= (above + 2) * pitch
+    assert np.all(seen == 1)
+
+
+@pytest.mark.parametrize("nchan,max_dt", [(256, 256), (512, 512), (1024, 1024), (4096, 4096), (96, 96),
+                                          (300, 150)])
+def test_every_tuner_schedule_has_sound_geometry(nchan, max_dt):
+    """Every schedule the autotuner may time (input segments of 2-4 levels x
+    16 / 24 / 28 / 32 rows x one or two input buffers; heads of depth 2-4 with
+    16 / 32 rows), at the search's channel counts and odd ones: the plan is
+    either refused or every fused pass keeps the kernel's bounds."""
+    built = 0
+    for ncols in (5003, 1 << 15):
+        for seg in (2, 3, 4):
+            cands = [(0, rows, flags) for rows in (16, 24, 28, 32) for flags in (0, 1)]
+            cands += [(k, rows, 0) for k in (2, 3, 4) for rows in (16, 32)]
+            for fuse, rows_per_tile, flags in cands:
+                try:
+                    k, rows, passes = plan_passes(1200.0, 1600.0, nchan, ncols, max_dt, fuse, seg, rows_per_tile,
+                                                  flags)
+                except _capi.BfsError:
+                    continue                     # not usable for this shape: the tuner skips it
+                for pr, tiles, ent in passes:
+                    if len(tiles):
+                        _check_pass_geometry(pr, tiles, ent, rows, nchan, flags == 1)
+                built += 1
+    assert built > 0
